@@ -1,0 +1,94 @@
+// Device-side helpers shared by the sm_100a kernels.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "tbg_internal.h"
+
+namespace tbg {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+__device__ __forceinline__ uint32_t radix_f(const RadixF &rf, uint32_t key) {
+    return ((key & rf.m1) << rf.b2) | ((key >> rf.b1) & rf.m2);
+}
+
+// streaming loads: data read once, keep it out of L1
+__device__ __forceinline__ uint4 ldg_stream(const uint4 *p) { return __ldcs(p); }
+__device__ __forceinline__ uint2 ldg_stream(const uint2 *p) { return __ldcs(p); }
+
+__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t *p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint64_t *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned warp_max_u32(unsigned v) {
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide exclusive scan of one uint64 per thread.  Every thread of the
+// block must call it.  scratch holds THREADS/32 + 1 words.
+template <int THREADS>
+__device__ __forceinline__ uint64_t block_excl_scan(uint64_t v, uint64_t *total, uint64_t *scratch) {
+    constexpr int NW = THREADS / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) scratch[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint64_t s = lane < NW ? scratch[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < NW) scratch[lane] = s;
+    }
+    __syncthreads();
+    uint64_t before = w ? scratch[w - 1] : 0;
+    *total = scratch[NW - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__device__ __forceinline__ uint32_t next_pow2(uint32_t v) {
+    if (v <= 1) return 1;
+    return 1u << (32 - __clz(v - 1));
+}
+
+// splitmix64 finaliser (Steele, Lea, Flood 2014): a row mixer for checksums
+// and a counter-based random source for the generators.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__host__ __device__ __forceinline__ uint64_t row_hash(uint32_t key, uint32_t rp, uint32_t sp) {
+    return mix64((((uint64_t)key << 32) | rp) ^ mix64((uint64_t)sp));
+}
+
+}  // namespace tbg

@@ -1,0 +1,136 @@
+// Internal declarations shared by the sm_100a kernels and the host runtime of
+// tee-bench-b200.  Host code includes this with a plain C++ compiler view
+// (no device code is defined here).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/tbg.h"
+
+namespace tbg {
+
+// 8-byte tuple, the layout of struct row_t (uint32 key, uint32 payload).
+struct Row {
+    uint32_t key;
+    uint32_t payload;
+};
+static_assert(sizeof(Row) == 8, "row layout");
+
+// One unit of join work: an R chunk (fits one CTA's shared memory) against a
+// run of S rows of the same partition.
+struct Item {
+    uint64_t r_off;
+    uint64_t s_off;
+    uint64_t s_len;
+    uint32_t r_len;
+    uint32_t part;
+};
+
+// Device-side control block, zeroed at the start of every join.
+struct Ctrl {
+    unsigned long long matches;   // equi-join cardinality
+    unsigned long long rows;      // rows reserved in the output
+    unsigned int error;           // first TBG_ERR_* raised on the device
+    unsigned int nitems;          // join work items written by the planner
+    unsigned int tiles[16];       // tile tickets, one slot per scatter launch
+    unsigned int item_ctr[4];     // work-item tickets, one slot per join launch
+    unsigned long long max_part_R, max_part_S;
+    unsigned long long nonempty;  // partitions with both sides non-empty
+    unsigned long long heavy_rows_S;
+    unsigned long long heavy_keys;
+    unsigned long long pad[4];
+};
+
+// Tile geometry of the stable partitioning scatter.
+constexpr int SCATTER_THREADS = 256;
+constexpr int SCATTER_ITEMS = 16;
+constexpr int SCATTER_TILE = SCATTER_THREADS * SCATTER_ITEMS;  // rows per tile
+constexpr int SCATTER_FMAX = 256;                              // digits per pass
+
+// Shared-memory table capacity of the build/probe kernels (rows of R_p).
+constexpr int JOIN_THREADS = 512;
+constexpr int JOIN_CAPR_DEFAULT = 8192;
+
+// Bounded device waits: iterations before a wait gives up with TBG_ERR_TIMEOUT.
+constexpr unsigned int SPIN_LIMIT = 1u << 21;
+
+// Radix digit of the final partition index f for a key, pass-major:
+// f = ((key & m1) << b2) | ((key >> b1) & m2).  With one pass, b2 = m2 = 0.
+struct RadixF {
+    uint32_t m1, b1, m2, b2;
+};
+
+// Per-relation partition plan written by the planner kernel.
+struct RelPlan {
+    uint32_t *hist;       // [P]   final partition sizes
+    uint64_t *base;       // [P+1] exclusive prefix, base[P] = n
+    uint64_t *seg_start;  // [F1+1] pass-1 partition starts (== pass-1 digit bases)
+    uint32_t *seg_tile;   // [F1+1] pass-2 tile prefix per pass-1 partition
+};
+
+struct ScatterArgs {
+    const Row *in;
+    Row *out;
+    uint64_t out_n;            // rows in `out` (bounds guard)
+    const uint64_t *seg_start; // null: one flat segment [0, flat_n)
+    const uint32_t *seg_tile;
+    uint32_t nseg;
+    uint64_t flat_n;
+    const uint64_t *bases;     // destination of digit d of segment s: bases[(s << dbits) | d]
+    uint64_t *status;          // decoupled look-back words, tiles x F
+    unsigned int *tile_ctr;
+    unsigned int *err;
+    uint32_t epoch;
+    uint32_t dshift, dbits;    // digit = (f(key) >> dshift) & ((1 << dbits) - 1)
+    RadixF rf;
+};
+
+struct JoinArgs {
+    const Row *R;
+    const Row *S;
+    const Item *items;
+    const unsigned int *nitems;
+    unsigned int *item_ctr;
+    int capR;
+    int hash_shift;
+    int layout;                // 0 bucket chain, 1 histogram (RHT)
+    unsigned long long *matches;
+    unsigned long long *rows_ctr;
+    tbg_row_out *out;
+    uint64_t cap;
+    unsigned int *err;
+};
+
+struct PlanArgs {
+    RelPlan r, s;
+    uint64_t nR, nS;
+    int P_log2, b1, b2, passes;
+    int capR;
+    uint64_t capS;            // S rows per work item when splitting (0: no split)
+    Item *items;
+    uint64_t item_cap;
+    Ctrl *ctrl;
+};
+
+// ---- launchers (partition.cu, join.cu, gen.cu) ----
+cudaError_t launch_hist(const Row *in, uint64_t n, uint32_t *hist, int P_log2, RadixF rf,
+                        bool aggregate, int nsm, cudaStream_t st);
+cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st);
+cudaError_t launch_scatter(const ScatterArgs &a, uint64_t max_tiles, cudaStream_t st);
+size_t scatter_smem_bytes();
+cudaError_t launch_join(const JoinArgs &a, bool materialize, int grid, cudaStream_t st);
+size_t join_smem_bytes(int capR);
+int join_ctas_per_sm(int capR);
+
+cudaError_t launch_gen_pk(Row *d, uint64_t n, uint64_t seed, cudaStream_t st);
+cudaError_t launch_gen_fk(Row *d, uint64_t n, uint64_t maxid, uint64_t seed, cudaStream_t st);
+cudaError_t launch_gen_zipf(Row *d, uint64_t n, uint64_t alphabet, double z, int scatter,
+                            uint64_t seed, cudaStream_t st);
+cudaError_t launch_checksum(const tbg_row_out *rows, uint64_t n, unsigned long long *out,
+                            cudaStream_t st);
+
+// Counts kernel launches made by this library (reported by tbg_kernel_launches).
+void count_launch(unsigned n = 1);
+
+}  // namespace tbg

@@ -1,0 +1,70 @@
+// Host-side runtime structures of tee-bench-b200 (workspace cache, join run
+// record) shared by the C ABI and the per-algorithm pipelines.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "tbg_internal.h"
+
+namespace tbg {
+
+// A device buffer that only grows.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    bool fresh = false;  // set when (re)allocated; consumers that need zeroed memory clear it
+    cudaError_t ensure(size_t bytes);
+    void release();
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// Scratch of one (device, stream): reused by consecutive joins on that stream.
+struct Workspace {
+    int device = 0;
+    int nsm = 148;
+    DevBuf ctrl, histR, histS, baseR, baseS, segStartR, segStartS, segTileR, segTileS;
+    DevBuf status, tmpR, tmpS, partR, partS, items, misc;
+    DevBuf inR, inS, rows;      // drop-in layer: device copies of host inputs and output rows
+    DevBuf aux[8];              // algorithm-specific scratch (sort, learned model)
+    uint32_t epoch = 0;         // last look-back epoch used on `status`
+    Ctrl *host_ctrl = nullptr;  // pinned mirror of the control block
+    cudaEvent_t ev[8];
+    uint32_t next_epoch(cudaStream_t st);
+};
+
+// What one join call did (for stats).
+struct JoinRun {
+    int B = 0, passes = 0;
+    uint64_t P = 0;
+    bool timed = false;
+    int used_fallback = 0;
+    double predicted_imbalance = 0;
+    int train_steps = 0;
+    float train_loss = 0;
+    float ms_learn = 0;
+    uint64_t launches = 0;
+};
+
+Workspace *workspace_for(cudaStream_t st);
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+void choose_radix(const tbg_config &cfg, uint64_t nR, int capR, int *B, int *passes);
+
+int join_device_impl(const tbg_config *cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                     tbg_row_out *d_rows, uint64_t rows_cap, cudaStream_t st, JoinRun *run,
+                     Workspace **wout);
+int finish_join(const tbg_config &cfg, Workspace &w, cudaStream_t st, const JoinRun &run,
+                uint64_t nR, uint64_t nS, uint64_t cap, uint64_t *matches, tbg_stats *stats);
+
+int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                   tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
+int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                       tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
+int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                 tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
+int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                     tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
+
+}  // namespace tbg

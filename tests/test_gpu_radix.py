@@ -1,0 +1,179 @@
+"""GPU parity of the radix joins (RHO, RHT) against the oracle and the
+reference's golden vectors, through the C ABI.  Integer work: bit-exact."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import gen_relation
+from gpu_util import dev_relation, dev_to_host_rows, run_join
+
+pytestmark = pytest.mark.gpu
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("algo", ["RHO", "RHT"])
+@pytest.mark.parametrize("idx", range(8))
+def test_golden_cases(tbg, oracle, golden, cuda, algo, idx):
+    j = golden["joins"][idx]
+    R = gen_relation(oracle, j["R"], j["seedR"], 0)
+    S = gen_relation(oracle, j["S"], j["seedS"], 1)
+    assert sha(R["key"]) == j["R_keys_sha256"] and sha(S["key"]) == j["S_keys_sha256"]
+    m, _, st = run_join(tbg, cuda, algo, R, S)
+    assert m == j["RHO_n1"]
+    m2, rows, _ = run_join(tbg, cuda, algo, R, S, materialize=True)
+    assert m2 == j["RHO_mat_count"] == len(rows)
+    assert sha(oracle.sort_rows(rows)) == j["RHO_mat_sorted_sha256"]
+
+
+@pytest.mark.parametrize("algo", ["RHO", "RHT"])
+def test_dropin_matches_reference_default_config(tbg, oracle, golden, cuda, algo):
+    """RHO(&R, &S, nthreads) on the reference's default inputs (native.cpp:59-127)."""
+    j = golden["joins"][0]
+    R = gen_relation(oracle, j["R"], j["seedR"], 0)
+    S = gen_relation(oracle, j["S"], j["seedS"], 1)
+    assert tbg.find(algo).join(R, S, 2) == 2097152
+    c, rows = tbg.find(algo).join(R, S, 3, materialize=True)
+    assert c == 2097152 and len(rows) == c
+    assert sha(oracle.sort_rows(rows)) == j["RHO_mat_sorted_sha256"]
+
+
+@pytest.mark.parametrize("bits,passes", [(1, 1), (4, 1), (8, 1), (9, 2), (12, 2), (14, 2), (15, 2)])
+def test_radix_geometry(tbg, oracle, cuda, bits, passes):
+    rng = np.random.default_rng(bits * 10 + passes)
+    R = np.zeros(30011, dtype=oracle.ROW)
+    S = np.zeros(100003, dtype=oracle.ROW)
+    R["key"] = rng.integers(0, 1 << 20, len(R))
+    S["key"] = rng.integers(0, 1 << 20, len(S))
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    m, rows, st = run_join(tbg, cuda, "RHO", R, S, materialize=True, radix_bits=bits, passes=passes)
+    assert (st.radix_bits, st.passes) == (bits, passes)
+    assert m == ref
+    assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+
+
+def test_partition_sizes_match_oracle(tbg, oracle, cuda):
+    R = gen_relation(oracle, ("pk", 1 << 18, 0, 0.0), 1, 0)
+    S = gen_relation(oracle, ("zipf", 1 << 20, 1 << 18, 1.0), 2, 1)
+    m, _, st = run_join(tbg, cuda, "RHO", R, S, radix_bits=10, passes=2)
+    hR = oracle.radix_hist(R, 10, 2)
+    hS = oracle.radix_hist(S, 10, 2)
+    assert st.max_part_R == hR.max() and st.max_part_S == hS.max()
+    assert m == oracle.rho(R, S)
+
+
+@pytest.mark.parametrize("case", ["emptyR", "emptyS", "one", "dupes", "allsame", "highbits",
+                                  "misaligned", "nomatch"])
+def test_edge_cases(tbg, oracle, cuda, case):
+    rng = np.random.default_rng(5)
+    nR, nS = 1000, 5000
+    R = np.zeros(nR, dtype=oracle.ROW)
+    S = np.zeros(nS, dtype=oracle.ROW)
+    R["key"] = rng.permutation(nR) + 1
+    S["key"] = rng.integers(1, nR + 1, nS)
+    off = 0
+    if case == "emptyR":
+        R = R[:0]
+    elif case == "emptyS":
+        S = S[:0]
+    elif case == "one":
+        R, S = R[:1].copy(), R[:1].copy()
+    elif case == "dupes":
+        R["key"] = rng.integers(1, 50, nR)
+    elif case == "allsame":
+        R = R[:40].copy()
+        R["key"] = 7
+        S["key"] = 7
+    elif case == "highbits":
+        R["key"] = (rng.permutation(nR).astype(np.uint64) * 4294967 + 0xFFFF0000) & 0xFFFFFFFF
+        S["key"] = R["key"][rng.integers(0, nR, nS)]
+        R["key"][0] = 0xFFFFFFFF
+        R["key"][1] = 0
+    elif case == "misaligned":
+        off = 1
+    elif case == "nomatch":
+        S["key"] += 1 << 20
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True) if len(R) and len(S) else (0, np.zeros((0, 3), np.uint32))
+    for algo in ("RHO", "RHT"):
+        m, rows, _ = run_join(tbg, cuda, algo, R, S, materialize=True, offset=off)
+        assert m == ref
+        assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+
+
+def test_capacity_overflow_reports_exact_count(tbg, oracle, cuda):
+    R = gen_relation(oracle, ("pk", 5000, 0, 0.0), 1, 0)
+    S = gen_relation(oracle, ("fk", 20000, 5000, 0.0), 2, 1)
+    with pytest.raises(tbg.TbgError) as e:
+        run_join(tbg, cuda, "RHO", R, S, materialize=True, cap=1000)
+    assert e.value.code == tbg.ERR_CAPACITY
+    from gpu_util import to_dev, out_rows
+    tR, pR = to_dev(cuda, R)
+    tS, pS = to_dev(cuda, S)
+    tO, pO = out_rows(cuda, 1000)
+    rc, m, _ = tbg.join_device(tbg.config("RHO", materialize=1), pR, len(R), pS, len(S), pO, 1000,
+                               check=False)
+    assert rc == tbg.ERR_CAPACITY and m == 20000
+
+
+def test_async_api_and_launch_count(tbg, oracle, cuda):
+    R = gen_relation(oracle, ("pk", 1 << 16, 0, 0.0), 1, 0)
+    S = gen_relation(oracle, ("fk", 1 << 18, 1 << 16, 0.0), 2, 1)
+    from gpu_util import to_dev
+    tR, pR = to_dev(cuda, R)
+    tS, pS = to_dev(cuda, S)
+    out = cuda.zeros(4, dtype=cuda.int64, device="cuda")
+    n0 = tbg.kernel_launches()
+    s = cuda.cuda.current_stream().cuda_stream
+    for k in range(3):
+        tbg.join_device_async(tbg.config("RHO"), pR, len(R), pS, len(S), out.data_ptr() + 8 * k, stream=s)
+    assert tbg.lib().tbg_sync_status(s) == 0
+    assert out[:3].tolist() == [1 << 18] * 3
+    assert tbg.kernel_launches() - n0 >= 3 * 4
+
+
+@pytest.mark.parametrize("sel", [100, 50])
+def test_full_size_headline_config(tbg, cuda, sel):
+    """|R| = 2^27, |S| = 2^30 from the GPU generators: a permutation of
+    1..|R| against |S|/maxid permuted copies of 1..maxid (maxid = |R| at 100%
+    selectivity, 2|R| at 50%).  Known answer: |S| * |R| / maxid matches."""
+    nR, nS = 1 << 27, 1 << 30
+    maxid = nR * 100 // sel
+    tR, pR = dev_relation(cuda, nR)
+    tS, pS = dev_relation(cuda, nS)
+    tbg.gen_pk(pR, nR, 11111)
+    tbg.gen_fk(pS, nS, maxid, 22222)
+    cuda.cuda.synchronize()
+    rc, m, st = tbg.join_device(tbg.config("RHO"), pR, nR, pS, nS)
+    assert m == nS * nR // maxid
+    # the generators' contract: R is a permutation of 1..|R|
+    keys = tR.view(cuda.int32)[0::2]
+    assert int(keys.min()) == 1 and int(keys.max()) == nR
+    assert int(cuda.bincount(keys.long(), minlength=nR + 1)[1:].max()) == 1
+
+
+def test_generators_contract(tbg, cuda):
+    n, maxid = 3_000_001, 1_000_000
+    t, p = dev_relation(cuda, n)
+    tbg.gen_fk(p, n, maxid, 9)
+    keys = t[:n].view(cuda.int32)[0::2].long().cpu().numpy()
+    for c in range(3):
+        blk = keys[c * maxid:(c + 1) * maxid]
+        assert np.array_equal(np.sort(blk), np.arange(1, maxid + 1))
+    assert np.array_equal(np.sort(keys[3 * maxid:]), np.arange(1, 2))
+    tz, pz = dev_relation(cuda, 1 << 22)
+    tbg.gen_zipf(pz, 1 << 22, 1 << 16, 1.0, 0, 5)
+    kz = tz.view(cuda.int32)[0::2].long().cpu().numpy()
+    assert kz.min() >= 1 and kz.max() <= 1 << 16
+    freq = np.bincount(kz, minlength=(1 << 16) + 1)[1:] / len(kz)
+    H = np.sum(1.0 / np.arange(1, (1 << 16) + 1))
+    expect = 1.0 / (np.arange(1, 9) * H)
+    assert np.allclose(freq[:8], expect, rtol=0.02)
