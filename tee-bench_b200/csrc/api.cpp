@@ -140,15 +140,14 @@ static void mark(Workspace &w, bool timing, int i, cudaStream_t st) {
     if (timing) cudaEventRecord(w.ev[i], st);
 }
 
-// The radix-partitioned join: RHO (layout 0) and RHT (layout 1).
-int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
-                   tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
-                   JoinRun *run) {
+// Chunked radix partitioning of R and S into 2^B final partitions (shared by
+// RHO, RHT and RSM).  Output: partR / partS and the plan (bases, work items).
+int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                    int capR, Workspace &w, cudaStream_t st, JoinRun *run, int *join_grid_out) {
     const bool timing = cfg.timing != 0;
-    const int capR = JOIN_CAPR_DEFAULT;
     int B, passes;
     choose_radix(cfg, nR, capR, &B, &passes);
-    const int b1 = B / passes, b2 = B - b1;
+    const int b1 = passes == 2 ? B / 2 : B, b2 = B - b1;
     const uint64_t P = 1ull << B;
     const uint64_t F1 = 1ull << b1;
     run->B = B;
@@ -157,30 +156,39 @@ int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row 
 
     const int join_per_sm = join_ctas_per_sm(capR);
     const int join_grid = w.nsm * join_per_sm;
+    *join_grid_out = join_grid;
     uint64_t capS = 0;
     if (cfg.skew_split) {
         capS = nS / ((uint64_t)join_grid * 4);
         if (capS < 65536) capS = 65536;
     }
     const uint64_t item_cap = nR / capR + (capS ? nS / capS : 0) + 2 * P + 16;
-    const uint64_t tiles_max = (std::max(nR, nS) + SCATTER_TILE - 1) / SCATTER_TILE + F1 + 1;
+    // four chunks per SM (two resident partitioning CTAs each), at least
+    // 32K rows per chunk
+    auto chunks = [&](uint64_t n) {
+        uint64_t g = std::min<uint64_t>((uint64_t)w.nsm * 4, (n + 32767) / 32768);
+        return (int)std::max<uint64_t>(g, 1);
+    };
+    const int GR = chunks(nR), GS = chunks(nS);
+    const uint64_t chR = ((nR + GR - 1) / GR + 1) & ~1ull, chS = ((nS + GS - 1) / GS + 1) & ~1ull;
 
     cudaError_t e;
-#define ENSURE(buf, bytes)                                      \
-    do {                                                        \
-        e = (buf).ensure(bytes);                                \
+#define ENSURE(buf, bytes)                                        \
+    do {                                                          \
+        e = (buf).ensure(bytes);                                  \
         if (e != cudaSuccess) return cuda_error(e, "cudaMalloc"); \
     } while (0)
     ENSURE(w.ctrl, sizeof(Ctrl));
-    ENSURE(w.histR, P * 4);
-    ENSURE(w.histS, P * 4);
+    ENSURE(w.histR, (uint64_t)GR * P * 4);
+    ENSURE(w.histS, (uint64_t)GS * P * 4);
+    ENSURE(w.totR, P * 4);
+    ENSURE(w.totS, P * 4);
     ENSURE(w.baseR, (P + 1) * 8);
     ENSURE(w.baseS, (P + 1) * 8);
-    ENSURE(w.segStartR, (F1 + 1) * 8);
-    ENSURE(w.segStartS, (F1 + 1) * 8);
-    ENSURE(w.segTileR, (F1 + 1) * 4);
-    ENSURE(w.segTileS, (F1 + 1) * 4);
-    ENSURE(w.status, tiles_max * SCATTER_FMAX * 8);
+    ENSURE(w.off1R, (uint64_t)GR * F1 * 4);
+    ENSURE(w.off1S, (uint64_t)GS * F1 * 4);
+    ENSURE(w.cnt1R, (uint64_t)GR * F1 * 4);
+    ENSURE(w.cnt1S, (uint64_t)GS * F1 * 4);
     ENSURE(w.partR, std::max<uint64_t>(nR, 1) * 8);
     ENSURE(w.partS, std::max<uint64_t>(nS, 1) * 8);
     if (passes == 2) {
@@ -193,26 +201,22 @@ int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row 
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
     mark(w, timing, 0, st);
     if ((e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st)) != cudaSuccess) return cuda_error(e, "memset");
-    if ((e = cudaMemsetAsync(w.histR.p, 0, P * 4, st)) != cudaSuccess) return cuda_error(e, "memset");
-    if ((e = cudaMemsetAsync(w.histS.p, 0, P * 4, st)) != cudaSuccess) return cuda_error(e, "memset");
 
-    RadixF rf;
-    if (passes == 1) {
-        rf = RadixF{(uint32_t)(P - 1), 0, 0, 0};
-    } else {
-        rf = RadixF{(uint32_t)(F1 - 1), (uint32_t)b1, (uint32_t)((1u << b2) - 1), (uint32_t)b2};
-    }
-    const bool agg = true;
-    if ((e = launch_hist(dR, nR, w.histR.as<uint32_t>(), B, rf, agg, w.nsm, st)) != cudaSuccess)
+    const RadixF rf = passes == 1 ? RadixF{(uint32_t)(P - 1), 0, 0, 0}
+                                  : RadixF{(uint32_t)(F1 - 1), (uint32_t)b1,
+                                           (uint32_t)((1u << b2) - 1), (uint32_t)b2};
+    if ((e = launch_hist_chunks(dR, nR, chR, GR, w.histR.as<uint32_t>(), B, rf, st)) != cudaSuccess)
         return cuda_error(e, "hist R");
-    if ((e = launch_hist(dS, nS, w.histS.as<uint32_t>(), B, rf, agg, w.nsm, st)) != cudaSuccess)
+    if ((e = launch_hist_chunks(dS, nS, chS, GS, w.histS.as<uint32_t>(), B, rf, st)) != cudaSuccess)
         return cuda_error(e, "hist S");
+    if ((e = launch_colscan(w.histR.as<uint32_t>(), GR, (int)P, w.totR.as<uint32_t>(), st)) != cudaSuccess)
+        return cuda_error(e, "colscan R");
+    if ((e = launch_colscan(w.histS.as<uint32_t>(), GS, (int)P, w.totS.as<uint32_t>(), st)) != cudaSuccess)
+        return cuda_error(e, "colscan S");
 
     PlanArgs pa;
-    pa.r = RelPlan{w.histR.as<uint32_t>(), w.baseR.as<uint64_t>(), w.segStartR.as<uint64_t>(),
-                   w.segTileR.as<uint32_t>()};
-    pa.s = RelPlan{w.histS.as<uint32_t>(), w.baseS.as<uint64_t>(), w.segStartS.as<uint64_t>(),
-                   w.segTileS.as<uint32_t>()};
+    pa.r = RelPlan{w.totR.as<uint32_t>(), w.baseR.as<uint64_t>()};
+    pa.s = RelPlan{w.totS.as<uint32_t>(), w.baseS.as<uint64_t>()};
     pa.nR = nR;
     pa.nS = nS;
     pa.P_log2 = B;
@@ -227,79 +231,74 @@ int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row 
     if ((e = launch_plan(pa, st)) != cudaSuccess) return cuda_error(e, "plan");
     mark(w, timing, 1, st);
 
-    // pass 1 (and pass 2)
-    auto scatter = [&](const Row *in, Row *out, uint64_t n, int slot, bool second,
-                       const RelPlan &rp) -> cudaError_t {
-        ScatterArgs a;
+    auto args = [&](const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, DevBuf &hist,
+                    DevBuf &tot, DevBuf &base, DevBuf &off1, DevBuf &cnt1) {
+        PartArgs a;
         a.in = in;
         a.out = out;
-        a.out_n = n;
-        a.tile_ctr = &ctrl->tiles[slot];
-        a.err = &ctrl->error;
-        a.status = w.status.as<uint64_t>();
-        a.epoch = w.next_epoch(st);
+        a.n = n;
+        a.chunk = chunk;
+        a.G = G;
+        // pass-2 units of about 64K rows: group consecutive chunks of a segment
+        const uint64_t per_unit = std::max<uint64_t>(n / ((uint64_t)G * F1), 1);
+        a.group = (int)std::min<uint64_t>((uint64_t)G, std::max<uint64_t>(1, 65536 / per_unit));
+        a.b1 = b1;
+        a.b2 = b2;
         a.rf = rf;
-        a.flat_n = n;
-        uint64_t max_tiles = (n + SCATTER_TILE - 1) / SCATTER_TILE;
-        if (passes == 1) {
-            a.seg_start = nullptr;
-            a.seg_tile = nullptr;
-            a.nseg = 0;
-            a.bases = rp.base;
-            a.dshift = 0;
-            a.dbits = B;
-        } else if (!second) {
-            a.seg_start = nullptr;
-            a.seg_tile = nullptr;
-            a.nseg = 0;
-            a.bases = rp.seg_start;
-            a.dshift = b2;
-            a.dbits = b1;
-        } else {
-            a.seg_start = rp.seg_start;
-            a.seg_tile = rp.seg_tile;
-            a.nseg = (uint32_t)F1;
-            a.bases = rp.base;
-            a.dshift = 0;
-            a.dbits = b2;
-            max_tiles += F1;
-        }
-        return launch_scatter(a, n ? max_tiles : 0, st);
+        a.pre = hist.as<uint32_t>();
+        a.totals = tot.as<uint32_t>();
+        a.base = base.as<uint64_t>();
+        a.off1 = passes == 2 ? off1.as<uint32_t>() : nullptr;
+        a.cnt1 = passes == 2 ? cnt1.as<uint32_t>() : nullptr;
+        a.err = &ctrl->error;
+        return a;
     };
     Row *outR = w.partR.as<Row>(), *outS = w.partS.as<Row>();
-    if (passes == 1) {
-        if ((e = scatter(dR, outR, nR, 0, false, pa.r)) != cudaSuccess) return cuda_error(e, "scatter R");
-        if ((e = scatter(dS, outS, nS, 1, false, pa.s)) != cudaSuccess) return cuda_error(e, "scatter S");
-        mark(w, timing, 2, st);
-        mark(w, timing, 3, st);
-    } else {
-        Row *tR = w.tmpR.as<Row>(), *tS = w.tmpS.as<Row>();
-        if ((e = scatter(dR, tR, nR, 0, false, pa.r)) != cudaSuccess) return cuda_error(e, "scatter R1");
-        if ((e = scatter(dS, tS, nS, 1, false, pa.s)) != cudaSuccess) return cuda_error(e, "scatter S1");
-        mark(w, timing, 2, st);
-        if ((e = scatter(tR, outR, nR, 2, true, pa.r)) != cudaSuccess) return cuda_error(e, "scatter R2");
-        if ((e = scatter(tS, outS, nS, 3, true, pa.s)) != cudaSuccess) return cuda_error(e, "scatter S2");
-        mark(w, timing, 3, st);
+    Row *p1R = passes == 2 ? w.tmpR.as<Row>() : outR, *p1S = passes == 2 ? w.tmpS.as<Row>() : outS;
+    PartArgs aR = args(dR, p1R, nR, chR, GR, w.histR, w.totR, w.baseR, w.off1R, w.cnt1R);
+    PartArgs aS = args(dS, p1S, nS, chS, GS, w.histS, w.totS, w.baseS, w.off1S, w.cnt1S);
+    if ((e = launch_part_pass1(aR, st)) != cudaSuccess) return cuda_error(e, "pass 1 R");
+    if ((e = launch_part_pass1(aS, st)) != cudaSuccess) return cuda_error(e, "pass 1 S");
+    mark(w, timing, 2, st);
+    if (passes == 2) {
+        aR.in = p1R;
+        aR.out = outR;
+        aS.in = p1S;
+        aS.out = outS;
+        if ((e = launch_part_pass2(aR, st)) != cudaSuccess) return cuda_error(e, "pass 2 R");
+        if ((e = launch_part_pass2(aS, st)) != cudaSuccess) return cuda_error(e, "pass 2 S");
     }
+    mark(w, timing, 3, st);
+    return TBG_OK;
+}
 
+// The radix-partitioned join: RHO (layout 0) and RHT (layout 1).
+int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                   tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
+                   JoinRun *run) {
+    const int capR = JOIN_CAPR_DEFAULT;
+    int join_grid = 0;
+    int rc = radix_partition(cfg, dR, nR, dS, nS, capR, w, st, run, &join_grid);
+    if (rc) return rc;
+    Ctrl *ctrl = w.ctrl.as<Ctrl>();
     JoinArgs ja;
-    ja.R = outR;
-    ja.S = outS;
+    ja.R = w.partR.as<Row>();
+    ja.S = w.partS.as<Row>();
     ja.items = w.items.as<Item>();
     ja.nitems = &ctrl->nitems;
     ja.item_ctr = &ctrl->item_ctr[0];
     ja.capR = capR;
-    ja.hash_shift = B;
+    ja.hash_shift = run->B;
     ja.layout = cfg.algo == TBG_RHT ? 1 : 0;
     ja.matches = &ctrl->matches;
     ja.rows_ctr = &ctrl->rows;
     ja.out = d_rows;
     ja.cap = d_rows ? cap : 0;
     ja.err = &ctrl->error;
-    if ((e = launch_join(ja, cfg.materialize != 0, join_grid, st)) != cudaSuccess)
-        return cuda_error(e, "join");
-    mark(w, timing, 4, st);
-    run->timed = timing;
+    cudaError_t e = launch_join(ja, cfg.materialize != 0, join_grid, st);
+    if (e != cudaSuccess) return cuda_error(e, "join");
+    mark(w, cfg.timing != 0, 4, st);
+    run->timed = cfg.timing != 0;
     return TBG_OK;
 }
 
@@ -359,7 +358,7 @@ static int validate(const tbg_config *cfg, const void *dR, uint64_t nR, const vo
     if (cfg->algo < TBG_RHO || cfg->algo > TBG_LRN) return set_error(TBG_ERR_ARG, "unknown algo %d", cfg->algo);
     if ((reinterpret_cast<uintptr_t>(dR) | reinterpret_cast<uintptr_t>(dS)) & 7)
         return set_error(TBG_ERR_ARG, "relations must be 8-byte aligned");
-    if (nR > 0xFFFFFFFFull || nS > (1ull << 40)) return set_error(TBG_ERR_ARG, "relation too large");
+    if (nR > 0xFFFFFFFFull || nS > 0xFFFFFFFFull) return set_error(TBG_ERR_ARG, "relations hold at most 2^32 - 1 rows");
     return TBG_OK;
 }
 

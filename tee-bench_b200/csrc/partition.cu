@@ -1,95 +1,157 @@
-// Radix partitioning for sm_100a: histogram, planner, and a stable one-sweep
-// scatter with decoupled look-back.
+// Radix partitioning for sm_100a without inter-CTA waits.
 //
-// Replaces the reference's partitioning passes (Joins/radix_join.c:630-703
+// Replaces the reference's two partitioning passes (Joins/radix_join.c:630-703
 // parallel_radix_partition, :525-562 radix_cluster, :573-619
 // serial_radix_partition, the SWWC variant :734-827) and the task queues that
-// feed them (Include/task_queue.h).  One histogram read gives the sizes of all
-// final partitions of both passes; each pass is then one read and one write.
+// feed them (Include/task_queue.h).  The reference's own structure -- every
+// thread histograms a contiguous chunk, a prefix over (thread, digit) gives
+// each thread exact write cursors, then each thread scatters its chunk -- is
+// kept, with a CTA in the role of a thread:
+//
+//   K1 hist   CTA c histograms chunk c over all final partitions f (2^bits
+//             bins in shared memory) -> hist[c][f];
+//   K2 scan   column prefix over chunks -> pre[c][f], totals[f];
+//   K3 plan   exclusive scan of totals -> base[f], join work items;
+//   K4 pass 1 CTA c scatters chunk c by the pass-1 digit d1 = f >> b2 to
+//             cursor[d1] = base[d1 << b2] + sum_{d2} pre[c][(d1 << b2) | d2];
+//   K5 pass 2 unit (c, s) = the rows chunk c wrote to pass-1 partition s;
+//             scattered by d2 to cursor[d2] = base[(s << b2) | d2] + pre[c][...].
+//
+// One histogram read gives every cursor of both passes, so the traffic is
+// 8 (hist) + 16 (pass 1) + 16 (pass 2) bytes per row, and no CTA ever waits
+// for another.  Each pass stages a tile digit-sorted in shared memory and
+// writes runs with consecutive threads on consecutive addresses (coalesced).
 #include "tbg_device.cuh"
 
 namespace tbg {
 
 // ---------------------------------------------------------------------------
-// K1 histogram of the final partition index f over all rows.
-// Per-CTA shared-memory histogram; lanes holding the same bin are merged with
-// __match_any_sync so a hot key costs one shared atomic per warp, not 32.
+// shared helpers
 // ---------------------------------------------------------------------------
-template <bool AGG>
-__device__ __forceinline__ void hist_add(uint32_t *h, uint32_t f) {
-    if (AGG) {
-        unsigned mask = __activemask();
-        unsigned peers = __match_any_sync(mask, f);
-        if ((peers & lanemask_lt()) == 0) atomicAdd(&h[f], (uint32_t)__popc(peers));
+
+// True when neighbouring lanes of the warp hold the same digit: a sign of
+// skew, for which ranks are aggregated with __match_any_sync.
+__device__ __forceinline__ bool warp_has_dups(uint32_t d, bool valid) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t key = valid ? d : 0xFFFFFFFFu;
+    const uint32_t up = __shfl_up_sync(0xffffffffu, key, 1);
+    return __any_sync(0xffffffffu, valid && lane > 0 && up == key);
+}
+
+// Adds one row's bin to a shared histogram; every lane of the warp calls it
+// (valid = false for lanes without a row).  With `dup` (the warp showed
+// repeated bins: skew), lanes sharing a bin are merged by __match_any_sync
+// into one atomic; otherwise each row pays one shared atomic.
+__device__ __forceinline__ void hist_add_warp(uint32_t *h, uint32_t f, bool valid, bool dup) {
+    if (!dup) {
+        if (valid) atomicAdd(&h[f], 1u);
     } else {
-        atomicAdd(&h[f], 1u);
+        const unsigned peers = __match_any_sync(0xffffffffu, valid ? f : 0xFFFFFFFFu);
+        if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&h[f], (uint32_t)__popc(peers));
     }
 }
 
-template <bool AGG>
-__global__ void __launch_bounds__(512) k_hist(const Row *__restrict__ in, uint64_t n,
-                                              uint32_t *__restrict__ ghist, int nbins,
-                                              RadixF rf) {
-    extern __shared__ uint32_t sh_hist[];
-    for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh_hist[i] = 0;
-    __syncthreads();
-    const uint64_t head = (reinterpret_cast<uintptr_t>(in) & 15) ? 1 : 0;
-    if (head && n && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&sh_hist[radix_f(rf, in[0].key)], 1u);
-    const uint64_t body = n > head ? n - head : 0;
-    const uint4 *v = reinterpret_cast<const uint4 *>(in + head);
-    const uint64_t nv = body / 2;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (; i + 3 * stride < nv; i += 4 * stride) {
-        uint4 a = ldg_stream(v + i), b = ldg_stream(v + i + stride);
-        uint4 c = ldg_stream(v + i + 2 * stride), d = ldg_stream(v + i + 3 * stride);
-        hist_add<AGG>(sh_hist, radix_f(rf, a.x));
-        hist_add<AGG>(sh_hist, radix_f(rf, a.z));
-        hist_add<AGG>(sh_hist, radix_f(rf, b.x));
-        hist_add<AGG>(sh_hist, radix_f(rf, b.z));
-        hist_add<AGG>(sh_hist, radix_f(rf, c.x));
-        hist_add<AGG>(sh_hist, radix_f(rf, c.z));
-        hist_add<AGG>(sh_hist, radix_f(rf, d.x));
-        hist_add<AGG>(sh_hist, radix_f(rf, d.z));
+// Rank of a row within its warp's digit counter (returns the old count).
+// Correct either way; `dup` only picks the faster path.
+__device__ __forceinline__ uint32_t rank_warp(uint32_t *cnt, uint32_t d, bool valid, bool dup) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t key = valid ? d : 0xFFFFFFFFu;
+    uint32_t r = 0;
+    if (!dup) {
+        if (valid) r = atomicAdd(&cnt[d], 1u);
+    } else {
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (valid && lane == leader) b = atomicAdd(&cnt[d], (uint32_t)__popc(peers));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        r = b + __popc(peers & lanemask_lt());
     }
-    for (; i < nv; i += stride) {
-        uint4 a = ldg_stream(v + i);
-        hist_add<AGG>(sh_hist, radix_f(rf, a.x));
-        hist_add<AGG>(sh_hist, radix_f(rf, a.z));
-    }
-    if ((body & 1) && blockIdx.x == 0 && threadIdx.x == 0)
-        atomicAdd(&sh_hist[radix_f(rf, in[n - 1].key)], 1u);
-    __syncthreads();
-    for (int j = threadIdx.x; j < nbins; j += blockDim.x)
-        if (sh_hist[j]) atomicAdd(&ghist[j], sh_hist[j]);
-}
-
-cudaError_t launch_hist(const Row *in, uint64_t n, uint32_t *hist, int P_log2, RadixF rf,
-                        bool aggregate, int nsm, cudaStream_t st) {
-    if (n == 0) return cudaSuccess;
-    const int nbins = 1 << P_log2;
-    const size_t smem = (size_t)nbins * sizeof(uint32_t);
-    // enough CTAs to cover the GPU, but at least ~16K rows each so the
-    // per-CTA histogram flush stays small next to the streaming read
-    uint64_t want = (n + 16383) / 16384;
-    int per_sm = smem <= 48 * 1024 ? 4 : (smem <= 96 * 1024 ? 2 : 1);
-    uint64_t grid = umin64(want, (uint64_t)nsm * per_sm);
-    if (grid < 1) grid = 1;
-    auto kern = aggregate ? k_hist<true> : k_hist<false>;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    kern<<<(unsigned)grid, 512, smem, st>>>(in, n, hist, nbins, rf);
-    count_launch();
-    return cudaGetLastError();
+    return r;
 }
 
 // ---------------------------------------------------------------------------
-// K2 planner (one CTA): exclusive scans of both histograms into partition
-// bases, pass-2 segment/tile tables, and the join work items.  Replaces the
+// K1 per-chunk histogram over the final partition index f
+// ---------------------------------------------------------------------------
+constexpr int HIST_THREADS = 1024;
+
+__global__ void __launch_bounds__(HIST_THREADS) k_hist_chunks(const Row *__restrict__ in, uint64_t n,
+                                                             uint64_t chunk, uint32_t *__restrict__ hist,
+                                                             int nbins, RadixF rf) {
+    extern __shared__ uint32_t sh[];
+    for (int i = threadIdx.x; i < nbins; i += HIST_THREADS) sh[i] = 0;
+    __syncthreads();
+    const uint64_t lo = (uint64_t)blockIdx.x * chunk;
+    const uint64_t hi = umin64(n, lo + chunk);
+    if (lo < hi) {
+        const uint64_t head = ((reinterpret_cast<uintptr_t>(in + lo) & 15) != 0) ? 1 : 0;
+        const uint64_t body = hi - lo - head;
+        const uint64_t nv = body / 2;
+        const uint4 *v = reinterpret_cast<const uint4 *>(in + lo + head);
+        // warp-uniform trip count: every lane reaches the shuffles
+        const uint64_t per = (uint64_t)HIST_THREADS * 4;
+        for (uint64_t base = 0; base < nv; base += per) {
+            uint4 x[4];
+            bool ok[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                uint64_t i = base + (uint64_t)u * HIST_THREADS + threadIdx.x;
+                ok[u] = i < nv;
+                if (ok[u]) x[u] = ldg_stream(v + i);
+            }
+            uint32_t f[8];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                f[2 * u] = ok[u] ? radix_f(rf, x[u].x) : 0;
+                f[2 * u + 1] = ok[u] ? radix_f(rf, x[u].z) : 0;
+            }
+            const bool dup = warp_has_dups(f[0], ok[0]);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                hist_add_warp(sh, f[2 * u], ok[u], dup);
+                hist_add_warp(sh, f[2 * u + 1], ok[u], dup);
+            }
+        }
+        if (threadIdx.x == 0) {
+            if (head) atomicAdd(&sh[radix_f(rf, in[lo].key)], 1u);
+            if (body & 1) atomicAdd(&sh[radix_f(rf, in[hi - 1].key)], 1u);
+        }
+    }
+    __syncthreads();
+    uint32_t *dst = hist + (uint64_t)blockIdx.x * nbins;
+    for (int i = threadIdx.x; i < nbins; i += HIST_THREADS) dst[i] = sh[i];
+}
+
+// ---------------------------------------------------------------------------
+// K2 column prefix over chunks (in place) and per-partition totals
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_colscan(uint32_t *__restrict__ hist, int G, int P,
+                                                 uint32_t *__restrict__ totals) {
+    const int f = blockIdx.x * 256 + threadIdx.x;
+    if (f >= P) return;
+    uint32_t run = 0;
+    int c = 0;
+    for (; c + 4 <= G; c += 4) {
+        uint32_t a = hist[(uint64_t)c * P + f], b = hist[(uint64_t)(c + 1) * P + f];
+        uint32_t d = hist[(uint64_t)(c + 2) * P + f], e = hist[(uint64_t)(c + 3) * P + f];
+        hist[(uint64_t)c * P + f] = run;
+        hist[(uint64_t)(c + 1) * P + f] = run + a;
+        hist[(uint64_t)(c + 2) * P + f] = run + a + b;
+        hist[(uint64_t)(c + 3) * P + f] = run + a + b + d;
+        run += a + b + d + e;
+    }
+    for (; c < G; c++) {
+        uint32_t a = hist[(uint64_t)c * P + f];
+        hist[(uint64_t)c * P + f] = run;
+        run += a;
+    }
+    totals[f] = run;
+}
+
+// ---------------------------------------------------------------------------
+// K3 planner (one CTA): partition bases and join work items.  Replaces the
 // task creation of Joins/radix_join.c:946-1000 and :609-617 (pairs with both
-// sides non-empty), with oversized S sides split into several items.
+// sides non-empty); oversized S sides are split into several items.
 // ---------------------------------------------------------------------------
 constexpr int PLAN_THREADS = 1024;
 
@@ -119,36 +181,8 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
     const int P = 1 << a.P_log2;
     plan_bases(a.r.hist, a.r.base, a.nR, P, &a.ctrl->max_part_R, scratch);
     plan_bases(a.s.hist, a.s.base, a.nS, P, &a.ctrl->max_part_S, scratch);
-    __syncthreads();  // bases visible block-wide
+    __syncthreads();
 
-    // pass-2 segments: pass-1 partition p1 = final partitions [p1 << b2, (p1+1) << b2)
-    if (a.passes == 2) {
-        const int F1 = 1 << a.b1;
-        for (int rel = 0; rel < 2; rel++) {
-            const RelPlan &rp = rel ? a.s : a.r;
-            const uint64_t n = rel ? a.nS : a.nR;
-            uint32_t tiles = 0;
-            const int p1 = threadIdx.x;
-            uint64_t st = 0;
-            if (p1 < F1) {
-                st = rp.base[(uint64_t)p1 << a.b2];
-                uint64_t en = rp.base[(uint64_t)(p1 + 1) << a.b2];
-                tiles = (uint32_t)((en - st + SCATTER_TILE - 1) / SCATTER_TILE);
-            }
-            uint64_t total;
-            uint64_t ex = block_excl_scan<PLAN_THREADS>(tiles, &total, scratch);
-            if (p1 < F1) {
-                rp.seg_start[p1] = st;
-                rp.seg_tile[p1] = (uint32_t)ex;
-            }
-            if (threadIdx.x == 0) {
-                rp.seg_start[F1] = n;
-                rp.seg_tile[F1] = (uint32_t)total;
-            }
-        }
-    }
-
-    // join work items
     const int C = (P + PLAN_THREADS - 1) / PLAN_THREADS;
     const int lo = min(P, (int)threadIdx.x * C), hi = min(P, lo + C);
     uint64_t cnt = 0, nonempty = 0;
@@ -192,205 +226,298 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
     if (threadIdx.x == 0) a.ctrl->nitems = (unsigned)total;
 }
 
+// ---------------------------------------------------------------------------
+// tile scatter shared by both passes
+// ---------------------------------------------------------------------------
+template <int THREADS>
+struct PartSmem {
+    static constexpr int NW = THREADS / 32;
+    static constexpr int T = THREADS * PART_ITEMS;
+    static constexpr int CW = NW + 1;           // padded (digit, warp) row: spreads banks
+    Row buf[2][T + 2];                          // input tile (bulk copy), then the same tile digit-sorted
+    uint32_t spos[T];                           // output row of staged row j
+    uint32_t cnt[2][SCATTER_FMAX * CW];         // per (digit, warp) counts, double-buffered
+    uint32_t cursor[SCATTER_FMAX];              // next output row of each digit
+    uint32_t delta[SCATTER_FMAX];               // cursor - tile offset of the digit
+    uint64_t scan[NW + 1];
+    uint64_t mbar[2];
+};
+
+// Digit of a pass: a bit field of the key (pass 1: bits [0, b1); pass 2:
+// bits [b1, b1 + b2); one pass: bits [0, B)).
+struct DigitOp {
+    uint32_t shift, mask;
+    __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return (key >> shift) & mask; }
+};
+
+// Where tile rows [t, t + cnt) sit in a shared buffer: the bulk copy moves
+// the 16-byte aligned rows [a_lo, a_hi); row r is at buffer index r + off so
+// the copy's destination is 16-byte aligned too; edge rows outside the copy
+// (at most one at each end) are read from global memory.
+struct TileGeo {
+    uint64_t t;
+    uint32_t cnt, a_lo, a_hi, off;
+};
+
+__device__ __forceinline__ TileGeo tile_geo(const Row *in, uint64_t t, uint32_t cnt) {
+    TileGeo g;
+    g.t = t;
+    g.cnt = cnt;
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(in + t);
+    g.a_lo = (addr & 15) ? 1u : 0u;
+    g.a_hi = ((addr + (uintptr_t)cnt * 8) & 15) ? cnt - 1 : cnt;
+    if (g.a_hi < g.a_lo) g.a_hi = g.a_lo;  // a single misaligned row: no copy
+    g.off = g.a_lo;
+    return g;
+}
+
+__device__ __forceinline__ void issue_tile(const Row *in, const TileGeo &g, Row *buf, uint64_t *bar) {
+    const uint32_t bytes = (g.a_hi - g.a_lo) * 8;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, bytes);
+    if (bytes) bulk_g2s(buf + g.a_lo + g.off, in + g.t + g.a_lo, bytes, bar);
+}
+
+// One tile: rows are read from the landed buffer, ranked inside their warp,
+// the (digit, warp) counts are prefixed (column scan per digit + one block
+// scan over digits), then the tile is staged digit-sorted into the same
+// buffer with each row's output position and written out in slot order,
+// so consecutive threads store consecutive rows of each digit's run.
+template <int THREADS, bool FULL>
+__device__ __forceinline__ void part_tile(const Row *__restrict__ in, const TileGeo &g, int k, int ntiles,
+                                          const TileGeo &gnext, uint2 *__restrict__ out, uint32_t out_n,
+                                          DigitOp dop, int F, PartSmem<THREADS> &sm, unsigned *err) {
+    constexpr int NW = THREADS / 32, CW = NW + 1;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int b = k & 1;
+    const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
+    const uint32_t cnt = g.cnt;
+    uint32_t *c = sm.cnt[b];
+    if (!mbar_wait(&sm.mbar[b], (uint32_t)(k >> 1) & 1, SPIN_LIMIT * 16)) atomicCAS(err, 0u, (unsigned)TBG_ERR_TIMEOUT);
+    uint2 v[PART_ITEMS];
+#pragma unroll
+    for (int i = 0; i < PART_ITEMS; i++) {
+        const uint32_t r = wbase + i * 32 + lane;
+        if (FULL || r < cnt) {
+            if (r >= g.a_lo && r < g.a_hi) {
+                const Row x = sm.buf[b][r + g.off];
+                v[i] = make_uint2(x.key, x.payload);
+            } else {
+                v[i] = reinterpret_cast<const uint2 *>(in)[g.t + r];
+            }
+        }
+    }
+    for (int i = tid; i < F * CW; i += THREADS) sm.cnt[b ^ 1][i] = 0;
+    uint32_t rank[PART_ITEMS];
+    const bool dup = warp_has_dups(dop(v[0].x), FULL || wbase + lane < cnt);
+#pragma unroll
+    for (int i = 0; i < PART_ITEMS; i++) {
+        const bool valid = FULL || wbase + i * 32 + lane < cnt;
+        rank[i] = rank_warp(c + w, valid ? dop(v[i].x) * CW : 0, valid, dup);
+    }
+    __syncthreads();
+    // the other buffer is free (its tile was written out before this barrier)
+    if (tid == 0 && k + 1 < ntiles) issue_tile(in, gnext, sm.buf[b ^ 1], &sm.mbar[b ^ 1]);
+    uint32_t tot = 0;
+    if (tid < F) {
+#pragma unroll
+        for (int ww = 0; ww < NW; ww++) tot += c[tid * CW + ww];
+    }
+    uint64_t dummy;
+    const uint32_t toff = (uint32_t)block_excl_scan<THREADS, false>(tid < F ? tot : 0, &dummy, sm.scan);
+    if (tid < F) {
+        uint32_t run = toff;
+#pragma unroll
+        for (int ww = 0; ww < NW; ww++) {
+            const uint32_t x = c[tid * CW + ww];
+            c[tid * CW + ww] = run;
+            run += x;
+        }
+        sm.delta[tid] = sm.cursor[tid] - toff;
+        sm.cursor[tid] += tot;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PART_ITEMS; i++) {
+        if (FULL || wbase + i * 32 + lane < cnt) {
+            const uint32_t d = dop(v[i].x);
+            const uint32_t j = c[d * CW + w] + rank[i];
+            sm.buf[b][j] = Row{v[i].x, v[i].y};
+            sm.spos[j] = sm.delta[d] + j;
+        }
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < PART_ITEMS; kk++) {
+        const uint32_t j = kk * THREADS + tid;
+        if (FULL || j < cnt) {
+            const Row x = sm.buf[b][j];
+            const uint32_t pos = sm.spos[j];
+            if (pos < out_n) out[pos] = make_uint2(x.key, x.payload);
+            else atomicCAS(err, 0u, (unsigned)TBG_ERR_ARG);
+        }
+    }
+}
+
+// Scatters rows [lo, hi) of `in`, digit by digit, to out[sm.cursor[d]...];
+// the caller initialises sm.cursor[0..F) and synchronises.  Tile k + 1 is
+// bulk-copied into the second buffer while tile k is processed.
+template <int THREADS>
+__device__ void part_range(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
+                           uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm, unsigned *err) {
+    constexpr int T = THREADS * PART_ITEMS, CW = THREADS / 32 + 1;
+    uint2 *o = reinterpret_cast<uint2 *>(out);
+    const int ntiles = (int)((hi - lo + T - 1) / T);
+    for (int i = threadIdx.x; i < F * CW; i += THREADS) sm.cnt[0][i] = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&sm.mbar[0], 1);
+        mbar_init(&sm.mbar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (ntiles == 0) return;
+    TileGeo g = tile_geo(in, lo, (uint32_t)umin64(T, hi - lo));
+    if (threadIdx.x == 0) issue_tile(in, g, sm.buf[0], &sm.mbar[0]);
+    for (int k = 0; k < ntiles; k++) {
+        const uint64_t t1 = g.t + T;
+        const TileGeo gn = k + 1 < ntiles ? tile_geo(in, t1, (uint32_t)umin64(T, hi - t1)) : g;
+        if (g.cnt == T) part_tile<THREADS, true>(in, g, k, ntiles, gn, o, out_n, dop, F, sm, err);
+        else part_tile<THREADS, false>(in, g, k, ntiles, gn, o, out_n, dop, F, sm, err);
+        g = gn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K4 pass 1: CTA c scatters chunk c by d1.  With one pass, d1 is f itself.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto &sm = *reinterpret_cast<PartSmem<PART_THREADS> *>(smem_raw);
+    const int c = blockIdx.x, tid = threadIdx.x;
+    const int P = 1 << (a.b1 + a.b2);
+    const int F = 1 << a.b1;
+    const uint32_t *pre = a.pre + (uint64_t)c * P;
+    const uint32_t *nxt = c + 1 < a.G ? a.pre + (uint64_t)(c + 1) * P : a.totals;
+    // cursors: sum the chunk's prefix over each pass-1 digit's final partitions
+    for (int i = tid; i < F; i += PART_THREADS) {
+        sm.cursor[i] = 0;
+        sm.delta[i] = 0;
+    }
+    __syncthreads();
+    {
+        // each thread sums a contiguous run of f (one pass-1 digit per flush)
+        const int per = P >= PART_THREADS ? P / PART_THREADS : 1;
+        const int f0 = tid * per;
+        uint32_t acc_c = 0, acc_t = 0;
+        int cur_s = -1;
+        for (int f = f0; f < f0 + per && f < P; f++) {
+            const int s = f >> a.b2;
+            if (s != cur_s) {
+                if (cur_s >= 0) {
+                    atomicAdd(&sm.cursor[cur_s], acc_c);
+                    atomicAdd(&sm.delta[cur_s], acc_t);
+                }
+                cur_s = s;
+                acc_c = acc_t = 0;
+            }
+            acc_c += pre[f];
+            acc_t += nxt[f] - pre[f];
+        }
+        if (cur_s >= 0) {
+            atomicAdd(&sm.cursor[cur_s], acc_c);
+            atomicAdd(&sm.delta[cur_s], acc_t);
+        }
+    }
+    __syncthreads();
+    for (int s = tid; s < F; s += PART_THREADS) {
+        const uint32_t cur = (uint32_t)a.base[(uint64_t)s << a.b2] + sm.cursor[s];
+        sm.cursor[s] = cur;
+        if (a.off1) {
+            a.off1[(uint64_t)c * F + s] = cur;
+            a.cnt1[(uint64_t)c * F + s] = sm.delta[s];
+        }
+    }
+    __syncthreads();
+    const uint64_t lo = (uint64_t)c * a.chunk, hi = umin64(a.n, lo + a.chunk);
+    DigitOp dop{0u, (uint32_t)F - 1};
+    part_range<PART_THREADS>(a.in, lo, hi, a.out, (uint32_t)a.n, dop, F, sm, a.err);
+}
+
+// ---------------------------------------------------------------------------
+// K5 pass 2: unit (c, s), s-major, scatters by d2 within pass-1 partition s.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass2(PartArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto &sm = *reinterpret_cast<PartSmem<PART_THREADS> *>(smem_raw);
+    const int F1 = 1 << a.b1, F2 = 1 << a.b2;
+    const int P = F1 * F2;
+    const int ngroups = (a.G + a.group - 1) / a.group;
+    const uint64_t unit = blockIdx.x;
+    const int s = (int)(unit / ngroups), g = (int)(unit % ngroups);
+    const int c0 = g * a.group, c1 = min(a.G, c0 + a.group) - 1;
+    // chunk c's rows of partition s follow chunk c-1's in the pass-1 output,
+    // so a group of chunks is one contiguous range with one cursor per digit
+    const uint64_t lo = a.off1[(uint64_t)c0 * F1 + s];
+    const uint64_t hi = (uint64_t)a.off1[(uint64_t)c1 * F1 + s] + a.cnt1[(uint64_t)c1 * F1 + s];
+    if (lo >= hi) return;
+    for (int d = threadIdx.x; d < F2; d += PART_THREADS) {
+        const uint64_t f = ((uint64_t)s << a.b2) | d;
+        sm.cursor[d] = (uint32_t)a.base[f] + a.pre[(uint64_t)c0 * P + f];
+    }
+    __syncthreads();
+    DigitOp dop{(uint32_t)a.b1, (uint32_t)F2 - 1};
+    part_range<PART_THREADS>(a.in, lo, hi, a.out, (uint32_t)a.n, dop, F2, sm, a.err);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+int hist_ctas_per_sm(int P_log2) {
+    const size_t smem = ((size_t)1 << P_log2) * 4;
+    int n = 0;
+    cudaFuncSetAttribute(k_hist_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_hist_chunks, HIST_THREADS, smem);
+    return n < 1 ? 1 : n;
+}
+
+cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G, uint32_t *hist,
+                               int P_log2, RadixF rf, cudaStream_t st) {
+    const int nbins = 1 << P_log2;
+    const size_t smem = (size_t)nbins * 4;
+    cudaError_t e = cudaFuncSetAttribute(k_hist_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_hist_chunks<<<G, HIST_THREADS, smem, st>>>(in, n, chunk, hist, nbins, rf);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_colscan(uint32_t *hist, int G, int P, uint32_t *totals, cudaStream_t st) {
+    k_colscan<<<(P + 255) / 256, 256, 0, st>>>(hist, G, P, totals);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st) {
     k_plan<<<1, PLAN_THREADS, 0, st>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// K3 stable scatter, one tile of SCATTER_TILE rows per CTA ticket.
-//
-//  1. rows are loaded warp-striped: warp w owns a contiguous sub-tile, so the
-//     order (warp, item, lane) is the input order (needed for stability);
-//  2. each row is ranked inside its warp with __match_any_sync against a
-//     warp-private digit counter; a column scan over warps and a scan over
-//     digits give every row its slot in the digit-sorted tile;
-//  3. the tile publishes its digit counts and looks back over predecessor
-//     tiles of the same segment (decoupled look-back, epoch-tagged words,
-//     bounded waits) for its global offsets;
-//  4. rows are staged digit-sorted in shared memory and written out with
-//     consecutive threads on consecutive addresses of each digit run, so the
-//     stores coalesce (the software write-combining of radix_join.c:734-827).
-// ---------------------------------------------------------------------------
-constexpr uint64_t LB_AGG = 1ull << 62;
-constexpr uint64_t LB_PRE = 2ull << 62;
-constexpr uint64_t LB_VAL = (1ull << 54) - 1;
-
-__device__ __forceinline__ uint64_t lb_pack(uint64_t flag, uint32_t epoch, uint64_t v) {
-    return flag | ((uint64_t)(epoch & 0xFF) << 54) | (v & LB_VAL);
+cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st) {
+    const size_t smem = sizeof(PartSmem<PART_THREADS>);
+    cudaError_t e = cudaFuncSetAttribute(k_part_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_part_pass1<<<a.G, PART_THREADS, smem, st>>>(a);
+    count_launch();
+    return cudaGetLastError();
 }
 
-size_t scatter_smem_bytes() {
-    constexpr int NW = SCATTER_THREADS / 32;
-    return (size_t)SCATTER_TILE * sizeof(Row)              // stage
-           + (size_t)NW * SCATTER_FMAX * sizeof(uint32_t)  // warp digit counters
-           + (size_t)SCATTER_FMAX * sizeof(uint32_t)       // tile digit offsets
-           + (size_t)SCATTER_FMAX * sizeof(uint64_t)       // global digit positions
-           + (size_t)SCATTER_TILE;                         // staged digits
-}
-
-__global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(ScatterArgs a) {
-    constexpr int NW = SCATTER_THREADS / 32;
-    constexpr int T = SCATTER_TILE;
-    extern __shared__ __align__(16) unsigned char smem[];
-    Row *stage = reinterpret_cast<Row *>(smem);
-    uint32_t *wcnt = reinterpret_cast<uint32_t *>(stage + T);
-    uint32_t *toff = wcnt + NW * SCATTER_FMAX;
-    uint64_t *gpos = reinterpret_cast<uint64_t *>(toff + SCATTER_FMAX);
-    uint8_t *dig = reinterpret_cast<uint8_t *>(gpos + SCATTER_FMAX);
-    __shared__ uint64_t s_row0, s_rowend;
-    __shared__ uint32_t s_tile, s_seg;
-    __shared__ int s_first, s_valid, s_abort;
-    __shared__ uint64_t scan_scratch[NW + 1];
-
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int F = 1 << a.dbits;
-    const uint32_t dmask = (uint32_t)F - 1;
-
-    if (tid == 0) {
-        uint32_t t = atomicAdd(a.tile_ctr, 1u);
-        s_tile = t;
-        s_abort = 0;
-        if (a.seg_start == nullptr) {
-            uint64_t ntiles = (a.flat_n + T - 1) / T;
-            s_valid = t < ntiles;
-            s_seg = 0;
-            s_first = (t == 0);
-            s_row0 = (uint64_t)t * T;
-            s_rowend = umin64(a.flat_n, s_row0 + T);
-        } else {
-            uint32_t total = a.seg_tile[a.nseg];
-            s_valid = t < total;
-            if (t < total) {
-                // last segment whose first tile is <= t (empty segments share starts)
-                uint32_t lo = 0, hi = a.nseg;  // invariant: seg_tile[lo] <= t < seg_tile[hi]
-                while (hi - lo > 1) {
-                    uint32_t mid = (lo + hi) >> 1;
-                    if (a.seg_tile[mid] <= t) lo = mid;
-                    else hi = mid;
-                }
-                uint32_t j = t - a.seg_tile[lo];
-                s_seg = lo;
-                s_first = (j == 0);
-                s_row0 = a.seg_start[lo] + (uint64_t)j * T;
-                s_rowend = umin64(a.seg_start[lo + 1], s_row0 + T);
-            }
-        }
-    }
-    for (int i = tid; i < NW * F; i += SCATTER_THREADS) wcnt[(i / F) * SCATTER_FMAX + (i % F)] = 0;
-    __syncthreads();
-    if (!s_valid) return;
-    const uint64_t row0 = s_row0, rowend = s_rowend;
-
-    // 1. load (warp-striped within a per-warp contiguous sub-tile)
-    uint32_t key[SCATTER_ITEMS], pay[SCATTER_ITEMS], d[SCATTER_ITEMS], rank[SCATTER_ITEMS];
-    const uint64_t wbase = row0 + (uint64_t)w * 32 * SCATTER_ITEMS;
-#pragma unroll
-    for (int i = 0; i < SCATTER_ITEMS; i++) {
-        uint64_t r = wbase + (uint64_t)i * 32 + lane;
-        if (r < rowend) {
-            uint2 x = ldg_stream(reinterpret_cast<const uint2 *>(a.in) + r);
-            key[i] = x.x;
-            pay[i] = x.y;
-            d[i] = (radix_f(a.rf, x.x) >> a.dshift) & dmask;
-        } else {
-            key[i] = pay[i] = 0;
-            d[i] = SCATTER_FMAX;  // sentinel: not a row
-        }
-    }
-    // 2. stable rank within the warp
-    uint32_t *myc = wcnt + w * SCATTER_FMAX;
-#pragma unroll
-    for (int i = 0; i < SCATTER_ITEMS; i++) {
-        unsigned peers = __match_any_sync(0xffffffffu, d[i]);
-        unsigned lt = peers & lanemask_lt();
-        uint32_t c = d[i] < SCATTER_FMAX ? myc[d[i]] : 0;
-        rank[i] = c + __popc(lt);
-        __syncwarp();
-        if (d[i] < SCATTER_FMAX && lt == 0) myc[d[i]] = c + __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-    // column scan over warps (thread = digit), then scan over digits
-    uint32_t tot = 0;
-    if (tid < F) {
-        for (int ww = 0; ww < NW; ww++) {
-            uint32_t c = wcnt[ww * SCATTER_FMAX + tid];
-            wcnt[ww * SCATTER_FMAX + tid] = tot;
-            tot += c;
-        }
-    }
-    uint64_t dummy;
-    uint32_t ex = (uint32_t)block_excl_scan<SCATTER_THREADS>(tid < F ? tot : 0, &dummy, scan_scratch);
-    if (tid < F) toff[tid] = ex;
-
-    // 3. decoupled look-back within the segment
-    if (tid < F) {
-        uint64_t *st = a.status + (uint64_t)s_tile * F;
-        uint64_t prefix = 0;
-        if (s_first) {
-            st_relaxed(st + tid, lb_pack(LB_PRE, a.epoch, tot));
-        } else {
-            st_relaxed(st + tid, lb_pack(LB_AGG, a.epoch, tot));
-            int64_t p = (int64_t)s_tile - 1;
-            while (p >= 0) {
-                const uint64_t *src = a.status + (uint64_t)p * F + tid;
-                uint64_t v = ld_relaxed(src);
-                unsigned spins = 0;
-                while (((v >> 62) == 0) || (((v >> 54) & 0xFF) != (a.epoch & 0xFF))) {
-                    if (++spins > SPIN_LIMIT) {
-                        atomicCAS(a.err, 0u, (unsigned)TBG_ERR_TIMEOUT);
-                        s_abort = 1;
-                        v = LB_PRE;  // stop looking back
-                        break;
-                    }
-                    if (spins > 16) __nanosleep(64);
-                    v = ld_relaxed(src);
-                }
-                prefix += v & LB_VAL;
-                if ((v >> 62) == 2) break;
-                p--;
-            }
-            st_relaxed(st + tid, lb_pack(LB_PRE, a.epoch, prefix + tot));
-        }
-        gpos[tid] = a.bases[((uint64_t)s_seg << a.dbits) | tid] + prefix;
-    }
-    __syncthreads();
-
-    // 4. stage digit-sorted, then coalesced write-out
-#pragma unroll
-    for (int i = 0; i < SCATTER_ITEMS; i++) {
-        if (d[i] < SCATTER_FMAX) {
-            uint32_t pos = toff[d[i]] + wcnt[w * SCATTER_FMAX + d[i]] + rank[i];
-            stage[pos] = Row{key[i], pay[i]};
-            dig[pos] = (uint8_t)d[i];
-        }
-    }
-    __syncthreads();
-    if (s_abort) return;
-    const int cnt = (int)(rowend - row0);
-    for (int j = tid; j < cnt; j += SCATTER_THREADS) {
-        uint32_t dd = dig[j];
-        uint64_t pos = gpos[dd] + (uint64_t)(j - (int)toff[dd]);
-        if (pos < a.out_n) {
-            reinterpret_cast<uint2 *>(a.out)[pos] = make_uint2(stage[j].key, stage[j].payload);
-        } else {
-            atomicCAS(a.err, 0u, (unsigned)TBG_ERR_TIMEOUT);
-        }
-    }
-}
-
-cudaError_t launch_scatter(const ScatterArgs &a, uint64_t max_tiles, cudaStream_t st) {
-    if (max_tiles == 0) return cudaSuccess;
-    static bool attr_done = false;
-    const size_t smem = scatter_smem_bytes();
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_done = true;
-    }
-    k_scatter<<<(unsigned)max_tiles, SCATTER_THREADS, smem, st>>>(a);
+cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st) {
+    const size_t smem = sizeof(PartSmem<PART_THREADS>);
+    cudaError_t e = cudaFuncSetAttribute(k_part_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint64_t units = (uint64_t)((a.G + a.group - 1) / a.group) << a.b1;
+    k_part_pass2<<<(unsigned)units, PART_THREADS, smem, st>>>(a);
     count_launch();
     return cudaGetLastError();
 }

@@ -45,7 +45,7 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 
 // Block-wide exclusive scan of one uint64 per thread.  Every thread of the
 // block must call it.  scratch holds THREADS/32 + 1 words.
-template <int THREADS>
+template <int THREADS, bool TAIL_SYNC = true>
 __device__ __forceinline__ uint64_t block_excl_scan(uint64_t v, uint64_t *total, uint64_t *scratch) {
     constexpr int NW = THREADS / 32;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -69,7 +69,7 @@ __device__ __forceinline__ uint64_t block_excl_scan(uint64_t v, uint64_t *total,
     __syncthreads();
     uint64_t before = w ? scratch[w - 1] : 0;
     *total = scratch[NW - 1];
-    __syncthreads();
+    if (TAIL_SYNC) __syncthreads();  // without it the caller syncs before reusing scratch
     return before + x - v;
 }
 
@@ -89,6 +89,53 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 
 __host__ __device__ __forceinline__ uint64_t row_hash(uint32_t key, uint32_t rp, uint32_t sp) {
     return mix64((((uint64_t)key << 32) | rp) ^ mix64((uint64_t)sp));
+}
+
+}  // namespace tbg
+
+namespace tbg {
+
+// ---- bulk-copy (TMA) and mbarrier helpers --------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Orders this thread's (and, after a barrier, the CTA's) generic-proxy shared
+// memory accesses before later async-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global memory into this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// Bounded wait for phase `parity` of `bar`; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+    const uint32_t a = smem_addr(bar);
+    for (uint32_t it = 0; it < limit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
 }
 
 }  // namespace tbg

@@ -48,6 +48,10 @@ constexpr int SCATTER_ITEMS = 16;
 constexpr int SCATTER_TILE = SCATTER_THREADS * SCATTER_ITEMS;  // rows per tile
 constexpr int SCATTER_FMAX = 256;                              // digits per pass
 
+// Rows per thread per tile of the chunked partitioning passes.
+constexpr int PART_THREADS = 256;
+constexpr int PART_ITEMS = 16;
+
 // Shared-memory table capacity of the build/probe kernels (rows of R_p).
 constexpr int JOIN_THREADS = 512;
 constexpr int JOIN_CAPR_DEFAULT = 8192;
@@ -65,8 +69,24 @@ struct RadixF {
 struct RelPlan {
     uint32_t *hist;       // [P]   final partition sizes
     uint64_t *base;       // [P+1] exclusive prefix, base[P] = n
-    uint64_t *seg_start;  // [F1+1] pass-1 partition starts (== pass-1 digit bases)
-    uint32_t *seg_tile;   // [F1+1] pass-2 tile prefix per pass-1 partition
+};
+
+// Arguments of the chunked partitioning passes (partition.cu).
+struct PartArgs {
+    const Row *in;
+    Row *out;
+    uint64_t n;               // rows (< 2^32)
+    uint64_t chunk;           // rows per pass-1 chunk
+    int G;                    // chunks
+    int group;                // pass 2: consecutive chunks per unit
+    int b1, b2;               // digit bits of pass 1 and pass 2 (b2 = 0: one pass)
+    RadixF rf;
+    const uint32_t *pre;      // [G][P] rows of partition f in chunks before c
+    const uint32_t *totals;   // [P]
+    const uint64_t *base;     // [P+1]
+    uint32_t *off1;           // [G][F1] start of unit (c, s) in the pass-1 output
+    uint32_t *cnt1;           // [G][F1] rows of unit (c, s)
+    unsigned *err;
 };
 
 struct ScatterArgs {
@@ -113,10 +133,13 @@ struct PlanArgs {
     Ctrl *ctrl;
 };
 
-// ---- launchers (partition.cu, join.cu, gen.cu) ----
-cudaError_t launch_hist(const Row *in, uint64_t n, uint32_t *hist, int P_log2, RadixF rf,
-                        bool aggregate, int nsm, cudaStream_t st);
+// ---- launchers (partition.cu, sweep.cu, join.cu, gen.cu) ----
+cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G, uint32_t *hist,
+                               int P_log2, RadixF rf, cudaStream_t st);
+cudaError_t launch_colscan(uint32_t *hist, int G, int P, uint32_t *totals, cudaStream_t st);
 cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st);
+cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st);
+cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st);
 cudaError_t launch_scatter(const ScatterArgs &a, uint64_t max_tiles, cudaStream_t st);
 size_t scatter_smem_bytes();
 cudaError_t launch_join(const JoinArgs &a, bool materialize, int grid, cudaStream_t st);

@@ -24,7 +24,7 @@ struct DevBuf {
 struct Workspace {
     int device = 0;
     int nsm = 148;
-    DevBuf ctrl, histR, histS, baseR, baseS, segStartR, segStartS, segTileR, segTileS;
+    DevBuf ctrl, histR, histS, totR, totS, baseR, baseS, off1R, off1S, cnt1R, cnt1S;
     DevBuf status, tmpR, tmpS, partR, partS, items, misc;
     DevBuf inR, inS, rows;      // drop-in layer: device copies of host inputs and output rows
     DevBuf aux[8];              // algorithm-specific scratch (sort, learned model)
@@ -58,6 +58,8 @@ int join_device_impl(const tbg_config *cfg, const Row *dR, uint64_t nR, const Ro
 int finish_join(const tbg_config &cfg, Workspace &w, cudaStream_t st, const JoinRun &run,
                 uint64_t nR, uint64_t nS, uint64_t cap, uint64_t *matches, tbg_stats *stats);
 
+int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                    int capR, Workspace &w, cudaStream_t st, JoinRun *run, int *join_grid_out);
 int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                    tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
 int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
