@@ -235,7 +235,6 @@ struct PartSmem {
     static constexpr int T = THREADS * PART_ITEMS;
     static constexpr int CW = NW + 1;           // padded (digit, warp) row: spreads banks
     Row buf[2][T + 2];                          // input tile (bulk copy), then the same tile digit-sorted
-    uint32_t spos[T];                           // output row of staged row j
     uint32_t cnt[2][SCATTER_FMAX * CW];         // per (digit, warp) counts, double-buffered
     uint32_t cursor[SCATTER_FMAX];              // next output row of each digit
     uint32_t delta[SCATTER_FMAX];               // cursor - tile offset of the digit
@@ -343,7 +342,6 @@ __device__ __forceinline__ void part_tile(const Row *__restrict__ in, const Tile
             const uint32_t d = dop(v[i].x);
             const uint32_t j = c[d * CW + w] + rank[i];
             sm.buf[b][j] = Row{v[i].x, v[i].y};
-            sm.spos[j] = sm.delta[d] + j;
         }
     }
     __syncthreads();
@@ -352,7 +350,7 @@ __device__ __forceinline__ void part_tile(const Row *__restrict__ in, const Tile
         const uint32_t j = kk * THREADS + tid;
         if (FULL || j < cnt) {
             const Row x = sm.buf[b][j];
-            const uint32_t pos = sm.spos[j];
+            const uint32_t pos = sm.delta[dop(x.key)] + j;
             if (pos < out_n) out[pos] = make_uint2(x.key, x.payload);
             else atomicCAS(err, 0u, (unsigned)TBG_ERR_ARG);
         }

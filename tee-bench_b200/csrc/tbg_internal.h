@@ -49,8 +49,8 @@ constexpr int SCATTER_TILE = SCATTER_THREADS * SCATTER_ITEMS;  // rows per tile
 constexpr int SCATTER_FMAX = 256;                              // digits per pass
 
 // Rows per thread per tile of the chunked partitioning passes.
-constexpr int PART_THREADS = 256;
-constexpr int PART_ITEMS = 16;
+constexpr int PART_THREADS = 512;
+constexpr int PART_ITEMS = 8;
 
 // Shared-memory table capacity of the build/probe kernels (rows of R_p).
 constexpr int JOIN_THREADS = 512;
