@@ -2,14 +2,6 @@
 #include "tbg_runtime.h"
 
 namespace tbg {
-int run_sortmerge_join(const tbg_config &, const Row *, uint64_t, const Row *, uint64_t,
-                       tbg_row_out *, uint64_t, Workspace &, cudaStream_t, JoinRun *) {
-    return set_error(TBG_ERR_UNKNOWN_ALGO, "RSM is not built yet");
-}
-int run_psm_join(const tbg_config &, const Row *, uint64_t, const Row *, uint64_t,
-                 tbg_row_out *, uint64_t, Workspace &, cudaStream_t, JoinRun *) {
-    return set_error(TBG_ERR_UNKNOWN_ALGO, "PSM is not built yet");
-}
 int run_learned_join(const tbg_config &, const Row *, uint64_t, const Row *, uint64_t,
                      tbg_row_out *, uint64_t, Workspace &, cudaStream_t, JoinRun *) {
     return set_error(TBG_ERR_UNKNOWN_ALGO, "LRN is not built yet");

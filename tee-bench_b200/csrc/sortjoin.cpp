@@ -1,0 +1,150 @@
+// Host pipelines of the sort-merge joins RSM and PSM.
+//
+// RSM (Joins/radix_sortmerge_join.c:102-105) shares RHO's radix partitioning
+// and swaps the build/probe kernel for a per-partition sort + merge-path join.
+// PSM (Joins/psm/parallel_sortmerge_join.h:61-111) sorts both relations by key
+// (LSD radix sort, 8-bit digits, stable one-sweep scatter; a pass whose digit
+// is the same for every row is skipped) and merges them.
+#include <algorithm>
+#include <cstring>
+
+#include "tbg_internal.h"
+#include "tbg_runtime.h"
+
+namespace tbg {
+
+cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaStream_t st);
+int rsm_ctas_per_sm(int capR);
+cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_t *bases, int nsm,
+                              cudaStream_t st);
+cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t ns, uint64_t *splits,
+                              unsigned long long *matches, unsigned long long *rows_ctr, tbg_row_out *out,
+                              uint64_t cap, bool mat, cudaStream_t st);
+uint64_t merge_ctas(uint64_t nr, uint64_t ns);
+
+static void mark_ev(Workspace &w, bool timing, int i, cudaStream_t st) {
+    if (timing) cudaEventRecord(w.ev[i], st);
+}
+
+int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                       tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run) {
+    const int capR = JOIN_CAPR_DEFAULT;
+    int join_grid = 0;
+    int rc = radix_partition(cfg, dR, nR, dS, nS, capR, w, st, run, &join_grid);
+    if (rc) return rc;
+    Ctrl *ctrl = w.ctrl.as<Ctrl>();
+    JoinArgs ja;
+    memset(&ja, 0, sizeof ja);
+    ja.R = w.partR.as<Row>();
+    ja.S = w.partS.as<Row>();
+    ja.items = w.items.as<Item>();
+    ja.nitems = &ctrl->nitems;
+    ja.item_ctr = &ctrl->item_ctr[0];
+    ja.capR = capR;
+    ja.hash_shift = run->B;
+    ja.matches = &ctrl->matches;
+    ja.rows_ctr = &ctrl->rows;
+    ja.out = d_rows;
+    ja.cap = d_rows ? cap : 0;
+    ja.err = &ctrl->error;
+    cudaError_t e = launch_join_rsm(ja, cfg.materialize != 0, w.nsm * rsm_ctas_per_sm(capR), st);
+    if (e != cudaSuccess) return cuda_error(e, "rsm join");
+    mark_ev(w, cfg.timing != 0, 4, st);
+    run->timed = cfg.timing != 0;
+    return TBG_OK;
+}
+
+// LSD sort of n rows by key; returns the buffer holding the sorted rows.
+static int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist,
+                    const uint64_t *dbases, int slot0, Workspace &w, cudaStream_t st, const Row **out,
+                    int *passes) {
+    const Row *src = in;
+    Row *bufs[2] = {a.as<Row>(), b.as<Row>()};
+    int which = 0;
+    *passes = 0;
+    for (int p = 0; p < 4; p++) {
+        bool trivial = false;
+        for (int d = 0; d < 256; d++)
+            if (hhist[p * 256 + d] == n) trivial = true;
+        if (trivial || n <= 1) continue;
+        ScatterArgs s;
+        memset(&s, 0, sizeof s);
+        s.in = src;
+        s.out = bufs[which];
+        s.out_n = n;
+        s.seg_start = nullptr;
+        s.seg_tile = nullptr;
+        s.nseg = 0;
+        s.flat_n = n;
+        s.bases = dbases + p * 256;
+        s.status = w.status.as<uint64_t>();
+        s.tile_ctr = &w.ctrl.as<Ctrl>()->tiles[slot0 + p];
+        s.err = &w.ctrl.as<Ctrl>()->error;
+        s.epoch = w.next_epoch(st);
+        s.dshift = 8 * p;
+        s.dbits = 8;
+        s.rf = RadixF{0xFFFFFFFFu, 0, 0, 0};
+        cudaError_t e = launch_scatter(s, (n + SCATTER_TILE - 1) / SCATTER_TILE, st);
+        if (e != cudaSuccess) return cuda_error(e, "sort pass");
+        src = bufs[which];
+        which ^= 1;
+        (*passes)++;
+    }
+    *out = src;
+    return TBG_OK;
+}
+
+int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                 tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run) {
+    const bool timing = cfg.timing != 0;
+    cudaError_t e;
+    const uint64_t tiles = (std::max(nR, nS) + SCATTER_TILE - 1) / SCATTER_TILE + 1;
+#define ENSURE(buf, bytes)                                        \
+    do {                                                          \
+        e = (buf).ensure(bytes);                                  \
+        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc"); \
+    } while (0)
+    ENSURE(w.ctrl, sizeof(Ctrl));
+    ENSURE(w.aux[0], nR * 8);
+    ENSURE(w.aux[1], nR * 8);
+    ENSURE(w.aux[2], nS * 8);
+    ENSURE(w.aux[3], nS * 8);
+    ENSURE(w.aux[4], 2 * 4 * 256 * 4);
+    ENSURE(w.aux[5], 2 * 4 * 256 * 8);
+    ENSURE(w.aux[6], (merge_ctas(nR, nS) + 2) * 8);
+    ENSURE(w.status, tiles * SCATTER_FMAX * 8);
+#undef ENSURE
+    Ctrl *ctrl = w.ctrl.as<Ctrl>();
+    uint32_t *hist = w.aux[4].as<uint32_t>();
+    uint64_t *bases = w.aux[5].as<uint64_t>();
+    mark_ev(w, timing, 0, st);
+    if ((e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st)) != cudaSuccess) return cuda_error(e, "memset");
+    if ((e = launch_digit_hist(dR, nR, hist, bases, w.nsm, st)) != cudaSuccess) return cuda_error(e, "digits R");
+    if ((e = launch_digit_hist(dS, nS, hist + 1024, bases + 1024, w.nsm, st)) != cudaSuccess)
+        return cuda_error(e, "digits S");
+    // which digit passes are needed decides the buffer chain: read the counts back
+    uint32_t hh[2048];
+    if ((e = cudaMemcpyAsync(hh, hist, sizeof hh, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_error(e, "digits");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "digits");
+    mark_ev(w, timing, 1, st);
+    const Row *sR = nullptr, *sS = nullptr;
+    int pr = 0, ps = 0;
+    int rc = lsd_sort(dR, nR, w.aux[0], w.aux[1], hh, bases, 0, w, st, &sR, &pr);
+    if (rc) return rc;
+    mark_ev(w, timing, 2, st);
+    rc = lsd_sort(dS, nS, w.aux[2], w.aux[3], hh + 1024, bases + 1024, 4, w, st, &sS, &ps);
+    if (rc) return rc;
+    mark_ev(w, timing, 3, st);
+    e = launch_merge_join(sR, nR, sS, nS, w.aux[6].as<uint64_t>(), &ctrl->matches, &ctrl->rows, d_rows,
+                          d_rows ? cap : 0, cfg.materialize != 0, st);
+    if (e != cudaSuccess) return cuda_error(e, "merge join");
+    mark_ev(w, timing, 4, st);
+    run->B = 8;
+    run->passes = std::max(pr, ps);
+    run->P = 0;
+    run->timed = timing;
+    return TBG_OK;
+}
+
+}  // namespace tbg

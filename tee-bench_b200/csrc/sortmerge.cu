@@ -1,0 +1,355 @@
+// Sort-merge joins for sm_100a.
+//
+// RSM (Joins/radix_sortmerge_join.c:74-100): the radix partitions of RHO,
+// then per partition pair both sides are sorted in shared memory (bitonic
+// network on packed (key, payload) words) and merged.  PSM
+// (Joins/psm/parallel_sortmerge_join.h:61-111): R and S are sorted globally
+// (LSD radix sort with the one-sweep scatter of sweep.cu) and merged.
+//
+// The merge is a merge path (Green, McColl, Bader 2012): the merged order
+// takes R[i] before S[j] iff R[i].key < S[j].key, so when S[j] is taken every
+// R row with a smaller key is behind and its matches are the run of equal
+// keys starting at the current R position.  Diagonals split the path evenly
+// over threads (and, for PSM, over CTAs).  The reference's merge()
+// (Joins/radix_sortmerge_join.c:40-71, parallel_sortmerge_join.h:18-51) has
+// unbounded inner loops and a stale S cursor that miscount duplicates and
+// misses; this merge counts exactly the equi-join.
+#include "tbg_device.cuh"
+
+namespace tbg {
+
+__device__ __forceinline__ uint64_t pack_row(uint32_t k, uint32_t p) { return ((uint64_t)k << 32) | p; }
+__device__ __forceinline__ uint32_t row_key(uint64_t x) { return (uint32_t)(x >> 32); }
+__device__ __forceinline__ uint32_t row_pay(uint64_t x) { return (uint32_t)x; }
+
+// Bitonic sort of s[0..N) (N a power of two) by the packed value.
+template <int THREADS>
+__device__ void bitonic_sort(uint64_t *s, uint32_t N) {
+    for (uint32_t k = 2; k <= N; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < N / 2; i += THREADS) {
+                const uint32_t lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+                const uint32_t hi = lo | j;
+                const bool asc = (lo & k) == 0;
+                const uint64_t a = s[lo], b = s[hi];
+                if ((a > b) == asc) {
+                    s[lo] = b;
+                    s[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Loads rows [off, off + n) into s[0..N) packed, pads with the maximum
+// value, and sorts.  N = next power of two >= n.
+template <int THREADS>
+__device__ uint32_t load_sorted(const Row *__restrict__ src, uint64_t off, uint32_t n, uint64_t *s) {
+    const uint32_t N = next_pow2(n < 2 ? 2 : n);
+    for (uint32_t i = threadIdx.x; i < N; i += THREADS) {
+        uint64_t v = ~0ull;
+        if (i < n) {
+            const uint2 x = reinterpret_cast<const uint2 *>(src)[off + i];
+            v = pack_row(x.x, x.y);
+        }
+        s[i] = v;
+    }
+    __syncthreads();
+    bitonic_sort<THREADS>(s, N);
+    return N;
+}
+
+// Merge-path split of diagonal d over sorted arrays A (na) and B (nb):
+// the number of A elements among the first d of the merged order, where A[i]
+// precedes B[j] iff key(A[i]) < key(B[j]).
+template <class GetA, class GetB>
+__device__ __forceinline__ uint64_t merge_split(uint64_t d, uint64_t na, uint64_t nb, GetA ka, GetB kb) {
+    uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (ka(mid) < kb(d - mid - 1)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// RSM: per work item, sorted R chunk in shared memory against sorted S tiles.
+// ---------------------------------------------------------------------------
+constexpr int RSM_THREADS = 512;
+constexpr int RSM_STILE = 4096;
+
+size_t rsm_smem_bytes(int capR) { return ((size_t)capR + RSM_STILE) * 8; }
+
+template <bool MAT>
+__global__ void __launch_bounds__(RSM_THREADS) k_join_rsm(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t *Rs = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *Ss = Rs + a.capR;
+    __shared__ uint32_t s_item;
+    __shared__ unsigned long long s_base;
+    __shared__ uint64_t scan_scratch[RSM_THREADS / 32 + 1];
+    const int tid = threadIdx.x;
+    const unsigned nitems = *a.nitems;
+    unsigned long long local = 0;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(a.item_ctr, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= nitems) break;
+        const Item m = a.items[it];
+        const uint32_t nr = m.r_len;
+        load_sorted<RSM_THREADS>(a.R, m.r_off, nr, Rs);
+        for (uint64_t s0 = 0; s0 < m.s_len; s0 += RSM_STILE) {
+            const uint32_t ns = (uint32_t)umin64(RSM_STILE, m.s_len - s0);
+            load_sorted<RSM_THREADS>(a.S, m.s_off + s0, ns, Ss);
+            // each thread walks an equal share of the merge path of R[0..nr) and S[0..ns)
+            const uint32_t L = nr + ns;
+            const uint32_t per = (L + RSM_THREADS - 1) / RSM_THREADS;
+            const uint32_t d0 = min(L, tid * per), d1 = min(L, d0 + per);
+            auto kr = [&](uint64_t i) { return row_key(Rs[i]); };
+            auto ks = [&](uint64_t j) { return row_key(Ss[j]); };
+            uint32_t i = (uint32_t)merge_split(d0, nr, ns, kr, ks);
+            uint32_t j = d0 - i;
+            // pass 1: count this thread's matches
+            uint32_t cnt = 0;
+            {
+                uint32_t ii = i, jj = j;
+                uint32_t last_key = 0, last_cnt = 0;
+                bool have = false;
+                for (uint32_t d = d0; d < d1; d++) {
+                    if (ii < nr && (jj >= ns || row_key(Rs[ii]) < row_key(Ss[jj]))) {
+                        ii++;
+                    } else {
+                        const uint32_t k = row_key(Ss[jj]);
+                        if (!have || k != last_key) {
+                            last_cnt = 0;
+                            for (uint32_t q = ii; q < nr && row_key(Rs[q]) == k; q++) last_cnt++;
+                            last_key = k;
+                            have = true;
+                        }
+                        cnt += last_cnt;
+                        jj++;
+                    }
+                }
+            }
+            local += cnt;
+            if (MAT) {
+                uint64_t tot;
+                const uint64_t off = block_excl_scan<RSM_THREADS>(cnt, &tot, scan_scratch);
+                if (tid == 0) s_base = tot ? atomicAdd(a.rows_ctr, (unsigned long long)tot) : 0;
+                __syncthreads();
+                uint64_t pos = s_base + off;
+                for (uint32_t d = d0; d < d1; d++) {
+                    if (i < nr && (j >= ns || row_key(Rs[i]) < row_key(Ss[j]))) {
+                        i++;
+                    } else {
+                        const uint32_t k = row_key(Ss[j]);
+                        for (uint32_t q = i; q < nr && row_key(Rs[q]) == k; q++) {
+                            if (pos < a.cap) {
+                                tbg_row_out o;
+                                o.key = k;
+                                o.Rpayload = row_pay(Rs[q]);
+                                o.Spayload = row_pay(Ss[j]);
+                                a.out[pos] = o;
+                            }
+                            pos++;
+                        }
+                        j++;
+                    }
+                }
+            }
+            __syncthreads();  // S tile reused
+        }
+    }
+    const unsigned long long ws = warp_sum_u64(local);
+    if ((tid & 31) == 0 && ws) atomicAdd(a.matches, ws);
+}
+
+int rsm_ctas_per_sm(int capR) {
+    int n = 0;
+    const size_t smem = rsm_smem_bytes(capR);
+    cudaFuncSetAttribute(k_join_rsm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_join_rsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join_rsm<false>, RSM_THREADS, smem);
+    return n < 1 ? 1 : n;
+}
+
+cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaStream_t st) {
+    const size_t smem = rsm_smem_bytes(a.capR);
+    auto kern = materialize ? k_join_rsm<true> : k_join_rsm<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, RSM_THREADS, smem, st>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// PSM: digit histograms of all LSD passes in one read, then the merge join
+// of the globally sorted relations.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_digit_hist(const Row *__restrict__ in, uint64_t n,
+                                                    uint32_t *__restrict__ hist /* [4][256] */) {
+    __shared__ uint32_t h[4][256];
+    for (int i = threadIdx.x; i < 4 * 256; i += 512) (&h[0][0])[i] = 0;
+    __syncthreads();
+    for (uint64_t i = (uint64_t)blockIdx.x * 512 + threadIdx.x; i < n; i += (uint64_t)gridDim.x * 512) {
+        const uint32_t k = in[i].key;
+        atomicAdd(&h[0][k & 255], 1u);
+        atomicAdd(&h[1][(k >> 8) & 255], 1u);
+        atomicAdd(&h[2][(k >> 16) & 255], 1u);
+        atomicAdd(&h[3][k >> 24], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * 256; i += 512)
+        if ((&h[0][0])[i]) atomicAdd(&hist[i], (&h[0][0])[i]);
+}
+
+// bases[p][d] = exclusive prefix of hist[p][.] (one block, 4 warps x 256 digits)
+__global__ void k_digit_bases(const uint32_t *__restrict__ hist, uint64_t *__restrict__ bases) {
+    const int p = threadIdx.x;  // 4 threads
+    if (p >= 4) return;
+    uint64_t run = 0;
+    for (int d = 0; d < 256; d++) {
+        bases[p * 256 + d] = run;
+        run += hist[p * 256 + d];
+    }
+}
+
+cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_t *bases, int nsm,
+                              cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(hist, 0, 4 * 256 * 4, st);
+    if (e != cudaSuccess) return e;
+    if (n) {
+        const uint64_t g = umin64((n + 511) / 512, (uint64_t)nsm * 4);
+        k_digit_hist<<<(unsigned)g, 512, 0, st>>>(in, n, hist);
+        count_launch();
+    }
+    k_digit_bases<<<1, 32, 0, st>>>(hist, bases);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Merge join of sorted R (nr) and sorted S (ns).  k_merge_splits finds, for
+// every CTA boundary c * D, the merge-path split (one thread per boundary);
+// CTA c then loads R[i_c, i_c+1) and S[j_c, j_c+1) (D rows together) into
+// shared memory, splits its D diagonals evenly over threads and walks them.
+// A run of equal R keys that continues past the tile is finished in global
+// memory.
+constexpr int MERGE_THREADS = 256;
+constexpr int MERGE_PER_THREAD = 8;
+constexpr int MERGE_TILE = MERGE_THREADS * MERGE_PER_THREAD;
+
+__global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row *__restrict__ S, uint64_t ns,
+                               uint64_t *__restrict__ splits, uint64_t nsplits) {
+    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nsplits) return;
+    const uint64_t d = umin64(nr + ns, c * MERGE_TILE);
+    auto kr = [&](uint64_t i) { return R[i].key; };
+    auto ks = [&](uint64_t j) { return S[j].key; };
+    splits[c] = merge_split(d, nr, ns, kr, ks);
+}
+
+template <bool MAT>
+__global__ void __launch_bounds__(MERGE_THREADS) k_merge_join(const Row *__restrict__ R, uint64_t nr,
+                                                               const Row *__restrict__ S, uint64_t ns,
+                                                               const uint64_t *__restrict__ splits,
+                                                               unsigned long long *matches,
+                                                               unsigned long long *rows_ctr, tbg_row_out *out,
+                                                               uint64_t cap) {
+    __shared__ uint64_t Rt[MERGE_TILE], St[MERGE_TILE];
+    __shared__ unsigned long long s_base;
+    __shared__ uint64_t scan_scratch[MERGE_THREADS / 32 + 1];
+    const uint64_t L = nr + ns;
+    const uint64_t c = blockIdx.x;
+    const uint64_t dc0 = c * MERGE_TILE, dc1 = umin64(L, dc0 + MERGE_TILE);
+    const uint64_t ic0 = splits[c], ic1 = splits[c + 1];
+    const uint64_t jc0 = dc0 - ic0, jc1 = dc1 - ic1;
+    const uint32_t nrt = (uint32_t)(ic1 - ic0), nst = (uint32_t)(jc1 - jc0);
+    for (uint32_t t = threadIdx.x; t < nrt; t += MERGE_THREADS) {
+        const uint2 x = reinterpret_cast<const uint2 *>(R)[ic0 + t];
+        Rt[t] = pack_row(x.x, x.y);
+    }
+    for (uint32_t t = threadIdx.x; t < nst; t += MERGE_THREADS) {
+        const uint2 x = reinterpret_cast<const uint2 *>(S)[jc0 + t];
+        St[t] = pack_row(x.x, x.y);
+    }
+    __syncthreads();
+    const uint32_t Lt = nrt + nst;
+    const uint32_t d0 = min(Lt, threadIdx.x * MERGE_PER_THREAD), d1 = min(Lt, d0 + MERGE_PER_THREAD);
+    auto kr = [&](uint64_t i) { return row_key(Rt[i]); };
+    auto ks = [&](uint64_t j) { return row_key(St[j]); };
+    const uint32_t i0 = (uint32_t)merge_split(d0, nrt, nst, kr, ks);
+    const uint32_t j0 = d0 - i0;
+    // matches of S row with key k taken at tile R position i: the run of k
+    auto run_len = [&](uint32_t i, uint32_t k) {
+        uint32_t n = 0;
+        uint32_t q = i;
+        for (; q < nrt && row_key(Rt[q]) == k; q++) n++;
+        if (q == nrt)
+            for (uint64_t g = ic0 + q; g < nr && R[g].key == k; g++) n++;
+        return n;
+    };
+    uint32_t i = i0, j = j0, cnt = 0, last_key = 0, last_cnt = 0;
+    bool have = false;
+    for (uint32_t d = d0; d < d1; d++) {
+        if (i < nrt && (j >= nst || row_key(Rt[i]) < row_key(St[j]))) {
+            i++;
+        } else {
+            const uint32_t k = row_key(St[j]);
+            if (!have || k != last_key) {
+                last_cnt = run_len(i, k);
+                last_key = k;
+                have = true;
+            }
+            cnt += last_cnt;
+            j++;
+        }
+    }
+    if (MAT) {
+        uint64_t tot;
+        const uint64_t off = block_excl_scan<MERGE_THREADS>(cnt, &tot, scan_scratch);
+        if (threadIdx.x == 0) s_base = tot ? atomicAdd(rows_ctr, (unsigned long long)tot) : 0;
+        __syncthreads();
+        uint64_t pos = s_base + off;
+        i = i0;
+        j = j0;
+        for (uint32_t d = d0; d < d1; d++) {
+            if (i < nrt && (j >= nst || row_key(Rt[i]) < row_key(St[j]))) {
+                i++;
+            } else {
+                const uint32_t k = row_key(St[j]), sp = row_pay(St[j]);
+                uint32_t q = i;
+                for (; q < nrt && row_key(Rt[q]) == k; q++, pos++)
+                    if (pos < cap) out[pos] = tbg_row_out{k, row_pay(Rt[q]), sp};
+                if (q == nrt)
+                    for (uint64_t g = ic0 + q; g < nr && R[g].key == k; g++, pos++)
+                        if (pos < cap) out[pos] = tbg_row_out{k, R[g].payload, sp};
+                j++;
+            }
+        }
+    }
+    const unsigned long long ws = warp_sum_u64(cnt);
+    if ((threadIdx.x & 31) == 0 && ws) atomicAdd(matches, ws);
+}
+
+uint64_t merge_ctas(uint64_t nr, uint64_t ns) { return (nr + ns + MERGE_TILE - 1) / MERGE_TILE; }
+
+cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t ns, uint64_t *splits,
+                              unsigned long long *matches, unsigned long long *rows_ctr, tbg_row_out *out,
+                              uint64_t cap, bool mat, cudaStream_t st) {
+    const uint64_t grid = merge_ctas(nr, ns);
+    if (!grid) return cudaSuccess;
+    const uint64_t nsplits = grid + 1;
+    k_merge_splits<<<(unsigned)((nsplits + 255) / 256), 256, 0, st>>>(R, nr, S, ns, splits, nsplits);
+    if (mat)
+        k_merge_join<true><<<(unsigned)grid, MERGE_THREADS, 0, st>>>(R, nr, S, ns, splits, matches, rows_ctr, out, cap);
+    else
+        k_merge_join<false><<<(unsigned)grid, MERGE_THREADS, 0, st>>>(R, nr, S, ns, splits, matches, rows_ctr, out, cap);
+    count_launch(2);
+    return cudaGetLastError();
+}
+
+}  // namespace tbg
