@@ -217,6 +217,22 @@ TBG_API int tbg_sync_status(void *stream);
 /* Number of kernels this library launched since load (all entry points). */
 TBG_API uint64_t tbg_kernel_launches(void);
 
+/* ---- learned partitioner model (LRN) --------------------------------------
+ * The FP32 MLP 1->32->32->1 (tanh) that LRN trains per join, exposed for
+ * inspection and tests.  params: W1[32], b1[32], W2[32][32], b2[32], W3[32],
+ * b3 (host arrays of tbg_mlp_param_count() floats); x is the key feature
+ * tbg_mlp_feature(key), y the target CDF value. */
+TBG_API int tbg_mlp_param_count(void);
+TBG_API float tbg_mlp_feature(uint32_t key);
+/* seeded initialisation, as LRN uses before training */
+TBG_API int tbg_mlp_init(float *params, uint64_t seed);
+/* mean squared error over n points and its gradient (the GPU backward pass) */
+TBG_API int tbg_mlp_grad(const float *params, const float *x, const float *y, uint64_t n,
+                         float *grad, float *loss);
+/* `steps` Adam steps on the GPU trainer (batches drawn from the n points) */
+TBG_API int tbg_mlp_train(float *params, const float *x, const float *y, uint64_t n, int steps,
+                          float lr, uint64_t seed);
+
 /* ---- on-GPU seeded generators (App/Lib/generator.cpp semantics) ----------- */
 /* pk: keys a seeded permutation of 1..n, payload = row index.               */
 TBG_API int tbg_gen_pk(struct row_t *d, uint64_t n, uint64_t seed, void *stream);

@@ -156,6 +156,15 @@ def lib():
         L.tbg_batch_run.restype = I
         L.tbg_batch_destroy.argtypes = [P]
     L.tbg_last_transfer_bytes.argtypes = [C.POINTER(U64), C.POINTER(U64)]
+    L.tbg_mlp_param_count.restype = I
+    L.tbg_mlp_feature.argtypes = [C.c_uint32]
+    L.tbg_mlp_feature.restype = C.c_float
+    L.tbg_mlp_init.argtypes = [P, U64]
+    L.tbg_mlp_init.restype = I
+    L.tbg_mlp_grad.argtypes = [P, P, P, U64, P, P]
+    L.tbg_mlp_grad.restype = I
+    L.tbg_mlp_train.argtypes = [P, P, P, U64, I, C.c_float, U64]
+    L.tbg_mlp_train.restype = I
     L.tbg_set_error_mode(ERRMODE_RETURN)  # Python callers get exceptions, not exit()
     _lib = L
     return L
@@ -282,6 +291,41 @@ def last_transfer_bytes():
     h, d = C.c_uint64(), C.c_uint64()
     lib().tbg_last_transfer_bytes(C.byref(h), C.byref(d))
     return int(h.value), int(d.value)
+
+
+# ------------------------------------------------------------------ model
+def mlp_init(seed: int) -> np.ndarray:
+    L = lib()
+    p = np.zeros(L.tbg_mlp_param_count(), dtype=np.float32)
+    _check(L.tbg_mlp_init(p.ctypes.data, seed))
+    return p
+
+
+def mlp_grad(params, x, y):
+    """(loss, grad) of the MSE over the points, computed by the GPU kernels."""
+    L = lib()
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    g = np.zeros_like(params)
+    loss = C.c_float()
+    _check(L.tbg_mlp_grad(params.ctypes.data, x.ctypes.data, y.ctypes.data, len(x), g.ctypes.data,
+                          C.addressof(loss)))
+    return float(loss.value), g
+
+
+def mlp_train(params, x, y, steps, lr=0.01, seed=1):
+    L = lib()
+    p = np.ascontiguousarray(params, dtype=np.float32).copy()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    _check(L.tbg_mlp_train(p.ctypes.data, x.ctypes.data, y.ctypes.data, len(x), steps, lr, seed))
+    return p
+
+
+def mlp_feature(keys) -> np.ndarray:
+    """Model input of keys: log2(key + 1) / 16 - 1 (what LRN feeds the MLP)."""
+    return (np.log2(np.asarray(keys, dtype=np.float64) + 1.0) / 16.0 - 1.0).astype(np.float32)
 
 
 def kernel_launches() -> int:

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "tbg_internal.h"
+#include "tbg_learned.h"
 #include "tbg_runtime.h"
 
 namespace tbg {
@@ -136,138 +137,200 @@ void choose_radix(const tbg_config &cfg, uint64_t nR, int capR, int *B, int *pas
 }
 
 // Records a timing event when cfg.timing is on.
-static void mark(Workspace &w, bool timing, int i, cudaStream_t st) {
+void mark(Workspace &w, bool timing, int i, cudaStream_t st) {
     if (timing) cudaEventRecord(w.ev[i], st);
 }
 
-// Chunked radix partitioning of R and S into 2^B final partitions (shared by
-// RHO, RHT and RSM).  Output: partR / partS and the plan (bases, work items).
-int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
-                    int capR, Workspace &w, cudaStream_t st, JoinRun *run, int *join_grid_out) {
-    const bool timing = cfg.timing != 0;
-    int B, passes;
-    choose_radix(cfg, nR, capR, &B, &passes);
-    const int b1 = passes == 2 ? B / 2 : B, b2 = B - b1;
-    const uint64_t P = 1ull << B;
-    const uint64_t F1 = 1ull << b1;
-    run->B = B;
-    run->passes = passes;
-    run->P = P;
-
-    const int join_per_sm = join_ctas_per_sm(capR);
-    const int join_grid = w.nsm * join_per_sm;
-    *join_grid_out = join_grid;
-    uint64_t capS = 0;
+// Geometry of the chunked radix partitioning of R and S into 2^B final
+// partitions (shared by RHO, RHT, RSM and LRN).
+RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int capR, Workspace &w) {
+    RadixGeom g;
+    choose_radix(cfg, nR, capR, &g.B, &g.passes);
+    g.b1 = g.passes == 2 ? g.B / 2 : g.B;
+    g.b2 = g.B - g.b1;
+    g.P = 1ull << g.B;
+    g.F1 = 1ull << g.b1;
+    g.capR = capR;
+    g.join_grid = w.nsm * join_ctas_per_sm(capR);
+    g.capS = 0;
     if (cfg.skew_split) {
-        capS = nS / ((uint64_t)join_grid * 4);
-        if (capS < 65536) capS = 65536;
+        g.capS = nS / ((uint64_t)g.join_grid * 4);
+        if (g.capS < 65536) g.capS = 65536;
     }
-    const uint64_t item_cap = nR / capR + (capS ? nS / capS : 0) + 2 * P + 16;
-    // four chunks per SM (two resident partitioning CTAs each), at least
-    // 32K rows per chunk
+    g.item_cap = nR / capR + (g.capS ? nS / g.capS : 0) + 2 * g.P + 16;
+    // four chunks per SM (two resident partitioning CTAs each), >= 32K rows each
     auto chunks = [&](uint64_t n) {
-        uint64_t g = std::min<uint64_t>((uint64_t)w.nsm * 4, (n + 32767) / 32768);
-        return (int)std::max<uint64_t>(g, 1);
+        uint64_t c = std::min<uint64_t>((uint64_t)w.nsm * 4, (n + 32767) / 32768);
+        return (int)std::max<uint64_t>(c, 1);
     };
-    const int GR = chunks(nR), GS = chunks(nS);
-    const uint64_t chR = ((nR + GR - 1) / GR + 1) & ~1ull, chS = ((nS + GS - 1) / GS + 1) & ~1ull;
+    g.G[0] = chunks(nR);
+    g.G[1] = chunks(nS);
+    g.ch[0] = ((nR + g.G[0] - 1) / g.G[0] + 1) & ~1ull;
+    g.ch[1] = ((nS + g.G[1] - 1) / g.G[1] + 1) & ~1ull;
+    g.n[0] = nR;
+    g.n[1] = nS;
+    g.rf = g.passes == 1 ? RadixF{(uint32_t)(g.P - 1), 0, 0, 0}
+                         : RadixF{(uint32_t)(g.F1 - 1), (uint32_t)g.b1, (uint32_t)((1u << g.b2) - 1), (uint32_t)g.b2};
+    return g;
+}
 
+int ensure_radix_buffers(const RadixGeom &g, bool bypass, Workspace &w) {
     cudaError_t e;
 #define ENSURE(buf, bytes)                                        \
     do {                                                          \
         e = (buf).ensure(bytes);                                  \
         if (e != cudaSuccess) return cuda_error(e, "cudaMalloc"); \
     } while (0)
+    const uint64_t nR = g.n[0], nS = g.n[1];
     ENSURE(w.ctrl, sizeof(Ctrl));
-    ENSURE(w.histR, (uint64_t)GR * P * 4);
-    ENSURE(w.histS, (uint64_t)GS * P * 4);
-    ENSURE(w.totR, P * 4);
-    ENSURE(w.totS, P * 4);
-    ENSURE(w.baseR, (P + 1) * 8);
-    ENSURE(w.baseS, (P + 1) * 8);
-    ENSURE(w.off1R, (uint64_t)GR * F1 * 4);
-    ENSURE(w.off1S, (uint64_t)GS * F1 * 4);
-    ENSURE(w.cnt1R, (uint64_t)GR * F1 * 4);
-    ENSURE(w.cnt1S, (uint64_t)GS * F1 * 4);
+    ENSURE(w.histR, (uint64_t)g.G[0] * g.P * 4);
+    ENSURE(w.histS, (uint64_t)g.G[1] * g.P * 4);
+    ENSURE(w.totR, g.P * 4);
+    ENSURE(w.totS, g.P * 4);
+    ENSURE(w.baseR, (g.P + 1) * 8);
+    ENSURE(w.baseS, (g.P + 1) * 8);
+    ENSURE(w.off1R, (uint64_t)g.G[0] * g.F1 * 4);
+    ENSURE(w.off1S, (uint64_t)g.G[1] * g.F1 * 4);
+    ENSURE(w.cnt1R, (uint64_t)g.G[0] * g.F1 * 4);
+    ENSURE(w.cnt1S, (uint64_t)g.G[1] * g.F1 * 4);
     ENSURE(w.partR, std::max<uint64_t>(nR, 1) * 8);
     ENSURE(w.partS, std::max<uint64_t>(nS, 1) * 8);
-    if (passes == 2) {
+    if (g.passes == 2) {
         ENSURE(w.tmpR, std::max<uint64_t>(nR, 1) * 8);
         ENSURE(w.tmpS, std::max<uint64_t>(nS, 1) * 8);
     }
-    ENSURE(w.items, item_cap * sizeof(Item));
+    ENSURE(w.items, g.item_cap * sizeof(Item));
+    if (bypass) {
+        ENSURE(w.sc, std::max<uint64_t>(nS, 1) * 8);
+        ENSURE(w.kept, (uint64_t)g.G[1] * 4);
+    }
 #undef ENSURE
+    return TBG_OK;
+}
 
+// Histogram of one relation (with the heavy bypass for S when given), column
+// prefix and partition bases.
+int part_histogram(int rel, const RadixGeom &g, const Row *d, const tbg_config &cfg, Workspace &w, cudaStream_t st,
+                   const SBypass *bypass) {
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
-    mark(w, timing, 0, st);
-    if ((e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st)) != cudaSuccess) return cuda_error(e, "memset");
+    DevBuf &hist = rel ? w.histS : w.histR;
+    DevBuf &tot = rel ? w.totS : w.totR;
+    DevBuf &base = rel ? w.baseS : w.baseR;
+    cudaError_t e;
+    if (!bypass) {
+        e = launch_hist_chunks(d, g.n[rel], g.ch[rel], g.G[rel], hist.as<uint32_t>(), g.B, g.rf, st);
+    } else {
+        BypassArgs ba;
+        ba.in = d;
+        ba.n = g.n[rel];
+        ba.chunk = g.ch[rel];
+        ba.G = g.G[rel];
+        ba.nbins = (int)g.P;
+        ba.rf = g.rf;
+        ba.out = w.sc.as<Row>();
+        ba.hist = hist.as<uint32_t>();
+        ba.kept = w.kept.as<uint32_t>();
+        ba.filter = bypass->filter;
+        ba.hkeys = bypass->keys;
+        ba.hcnt = bypass->cnt;
+        ba.hstart = bypass->start;
+        ba.rpay = bypass->rpay;
+        ba.matches = &ctrl->matches;
+        ba.heavy_rows = &ctrl->heavy_rows_S;
+        ba.rows_ctr = &ctrl->rows;
+        ba.rows = bypass->rows;
+        ba.cap = bypass->rows ? bypass->cap : 0;
+        e = launch_hist_bypass(ba, cfg.materialize != 0, st);
+    }
+    if (e != cudaSuccess) return cuda_error(e, "histogram");
+    if ((e = launch_colscan(hist.as<uint32_t>(), g.G[rel], (int)g.P, tot.as<uint32_t>(), st)) != cudaSuccess)
+        return cuda_error(e, "colscan");
+    if ((e = launch_plan_bases(tot.as<uint32_t>(), base.as<uint64_t>(), g.B,
+                               rel ? &ctrl->max_part_S : &ctrl->max_part_R, st)) != cudaSuccess)
+        return cuda_error(e, "bases");
+    return TBG_OK;
+}
 
-    const RadixF rf = passes == 1 ? RadixF{(uint32_t)(P - 1), 0, 0, 0}
-                                  : RadixF{(uint32_t)(F1 - 1), (uint32_t)b1,
-                                           (uint32_t)((1u << b2) - 1), (uint32_t)b2};
-    if ((e = launch_hist_chunks(dR, nR, chR, GR, w.histR.as<uint32_t>(), B, rf, st)) != cudaSuccess)
-        return cuda_error(e, "hist R");
-    if ((e = launch_hist_chunks(dS, nS, chS, GS, w.histS.as<uint32_t>(), B, rf, st)) != cudaSuccess)
-        return cuda_error(e, "hist S");
-    if ((e = launch_colscan(w.histR.as<uint32_t>(), GR, (int)P, w.totR.as<uint32_t>(), st)) != cudaSuccess)
-        return cuda_error(e, "colscan R");
-    if ((e = launch_colscan(w.histS.as<uint32_t>(), GS, (int)P, w.totS.as<uint32_t>(), st)) != cudaSuccess)
-        return cuda_error(e, "colscan S");
+// Pass `which` (1 or 2) of one relation.  Pass 1 reads the relation (or, with
+// the bypass, the compacted S); the last pass writes partR / partS.
+int part_pass(int rel, int which, const RadixGeom &g, const Row *d, Workspace &w, cudaStream_t st, bool bypass) {
+    Ctrl *ctrl = w.ctrl.as<Ctrl>();
+    const uint64_t n = g.n[rel];
+    PartArgs a;
+    a.n = n;
+    a.chunk = g.ch[rel];
+    a.chunk_len = nullptr;
+    a.G = g.G[rel];
+    const uint64_t per_unit = std::max<uint64_t>(n / ((uint64_t)a.G * g.F1), 1);
+    a.group = (int)std::min<uint64_t>((uint64_t)a.G, std::max<uint64_t>(1, 65536 / per_unit));
+    a.b1 = g.b1;
+    a.b2 = g.b2;
+    a.rf = g.rf;
+    a.pre = (rel ? w.histS : w.histR).as<uint32_t>();
+    a.totals = (rel ? w.totS : w.totR).as<uint32_t>();
+    a.base = (rel ? w.baseS : w.baseR).as<uint64_t>();
+    a.off1 = g.passes == 2 ? (rel ? w.off1S : w.off1R).as<uint32_t>() : nullptr;
+    a.cnt1 = g.passes == 2 ? (rel ? w.cnt1S : w.cnt1R).as<uint32_t>() : nullptr;
+    a.err = &ctrl->error;
+    Row *part = (rel ? w.partS : w.partR).as<Row>();
+    Row *tmp = g.passes == 2 ? (rel ? w.tmpS : w.tmpR).as<Row>() : part;
+    cudaError_t e;
+    if (which == 1) {
+        a.in = bypass ? w.sc.as<Row>() : d;
+        if (bypass) a.chunk_len = w.kept.as<uint32_t>();
+        a.out = tmp;
+        e = launch_part_pass1(a, st);
+    } else {
+        if (g.passes != 2) return TBG_OK;
+        a.in = tmp;
+        a.out = part;
+        e = launch_part_pass2(a, st);
+    }
+    return e == cudaSuccess ? TBG_OK : cuda_error(e, "partition pass");
+}
 
+int plan_items(const RadixGeom &g, Workspace &w, cudaStream_t st) {
     PlanArgs pa;
     pa.r = RelPlan{w.totR.as<uint32_t>(), w.baseR.as<uint64_t>()};
     pa.s = RelPlan{w.totS.as<uint32_t>(), w.baseS.as<uint64_t>()};
-    pa.nR = nR;
-    pa.nS = nS;
-    pa.P_log2 = B;
-    pa.b1 = b1;
-    pa.b2 = b2;
-    pa.passes = passes;
-    pa.capR = capR;
-    pa.capS = capS;
+    pa.nR = g.n[0];
+    pa.nS = g.n[1];
+    pa.P_log2 = g.B;
+    pa.b1 = g.b1;
+    pa.b2 = g.b2;
+    pa.passes = g.passes;
+    pa.capR = g.capR;
+    pa.capS = g.capS;
     pa.items = w.items.as<Item>();
-    pa.item_cap = item_cap;
-    pa.ctrl = ctrl;
-    if ((e = launch_plan(pa, st)) != cudaSuccess) return cuda_error(e, "plan");
-    mark(w, timing, 1, st);
+    pa.item_cap = g.item_cap;
+    pa.ctrl = w.ctrl.as<Ctrl>();
+    cudaError_t e = launch_plan(pa, st);
+    return e == cudaSuccess ? TBG_OK : cuda_error(e, "plan");
+}
 
-    auto args = [&](const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, DevBuf &hist,
-                    DevBuf &tot, DevBuf &base, DevBuf &off1, DevBuf &cnt1) {
-        PartArgs a;
-        a.in = in;
-        a.out = out;
-        a.n = n;
-        a.chunk = chunk;
-        a.G = G;
-        // pass-2 units of about 64K rows: group consecutive chunks of a segment
-        const uint64_t per_unit = std::max<uint64_t>(n / ((uint64_t)G * F1), 1);
-        a.group = (int)std::min<uint64_t>((uint64_t)G, std::max<uint64_t>(1, 65536 / per_unit));
-        a.b1 = b1;
-        a.b2 = b2;
-        a.rf = rf;
-        a.pre = hist.as<uint32_t>();
-        a.totals = tot.as<uint32_t>();
-        a.base = base.as<uint64_t>();
-        a.off1 = passes == 2 ? off1.as<uint32_t>() : nullptr;
-        a.cnt1 = passes == 2 ? cnt1.as<uint32_t>() : nullptr;
-        a.err = &ctrl->error;
-        return a;
-    };
-    Row *outR = w.partR.as<Row>(), *outS = w.partS.as<Row>();
-    Row *p1R = passes == 2 ? w.tmpR.as<Row>() : outR, *p1S = passes == 2 ? w.tmpS.as<Row>() : outS;
-    PartArgs aR = args(dR, p1R, nR, chR, GR, w.histR, w.totR, w.baseR, w.off1R, w.cnt1R);
-    PartArgs aS = args(dS, p1S, nS, chS, GS, w.histS, w.totS, w.baseS, w.off1S, w.cnt1S);
-    if ((e = launch_part_pass1(aR, st)) != cudaSuccess) return cuda_error(e, "pass 1 R");
-    if ((e = launch_part_pass1(aS, st)) != cudaSuccess) return cuda_error(e, "pass 1 S");
+// Single-stream radix partitioning of R and S (RHO, RHT, RSM).
+int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
+                    int capR, Workspace &w, cudaStream_t st, JoinRun *run, int *join_grid_out) {
+    const bool timing = cfg.timing != 0;
+    const RadixGeom g = radix_geometry(cfg, nR, nS, capR, w);
+    run->B = g.B;
+    run->passes = g.passes;
+    run->P = g.P;
+    *join_grid_out = g.join_grid;
+    int rc = ensure_radix_buffers(g, false, w);
+    if (rc) return rc;
+    mark(w, timing, 0, st);
+    cudaError_t e = cudaMemsetAsync(w.ctrl.p, 0, sizeof(Ctrl), st);
+    if (e != cudaSuccess) return cuda_error(e, "memset");
+    if ((rc = part_histogram(0, g, dR, cfg, w, st, nullptr))) return rc;
+    if ((rc = part_histogram(1, g, dS, cfg, w, st, nullptr))) return rc;
+    if ((rc = plan_items(g, w, st))) return rc;
+    mark(w, timing, 1, st);
+    if ((rc = part_pass(0, 1, g, dR, w, st, false))) return rc;
+    if ((rc = part_pass(1, 1, g, dS, w, st, false))) return rc;
     mark(w, timing, 2, st);
-    if (passes == 2) {
-        aR.in = p1R;
-        aR.out = outR;
-        aS.in = p1S;
-        aS.out = outS;
-        if ((e = launch_part_pass2(aR, st)) != cudaSuccess) return cuda_error(e, "pass 2 R");
-        if ((e = launch_part_pass2(aS, st)) != cudaSuccess) return cuda_error(e, "pass 2 S");
-    }
+    if ((rc = part_pass(0, 2, g, dR, w, st, false))) return rc;
+    if ((rc = part_pass(1, 2, g, dS, w, st, false))) return rc;
     mark(w, timing, 3, st);
     return TBG_OK;
 }
@@ -280,6 +343,12 @@ int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row 
     int join_grid = 0;
     int rc = radix_partition(cfg, dR, nR, dS, nS, capR, w, st, run, &join_grid);
     if (rc) return rc;
+    return radix_join_phase(cfg, d_rows, cap, w, st, run, capR, join_grid);
+}
+
+// Build/probe over the partitions radix_partition left in partR / partS.
+int radix_join_phase(const tbg_config &cfg, tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
+                     JoinRun *run, int capR, int join_grid) {
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
     JoinArgs ja;
     ja.R = w.partR.as<Row>();
@@ -406,7 +475,7 @@ void tbg_config_init(tbg_config *cfg) {
     cfg->algo = TBG_RHO;
     cfg->skew_split = 1;
     cfg->model = TBG_MODEL_MLP;
-    cfg->train_steps = 300;
+    cfg->train_steps = 30;
     cfg->heavy_bypass = 1;
     cfg->sample_rate = 0.01;
     cfg->imbalance_limit = 4.0;

@@ -123,29 +123,40 @@ __global__ void __launch_bounds__(HIST_THREADS) k_hist_chunks(const Row *__restr
 }
 
 // ---------------------------------------------------------------------------
-// K2 column prefix over chunks (in place) and per-partition totals
+// K2 column prefix over chunks (in place) and per-partition totals.  A CTA
+// owns 32 consecutive partitions (threadIdx.x, coalesced) and splits the
+// chunks into 32 segments (threadIdx.y): segment sums, a prefix over the
+// segments, then each segment rewritten with running prefixes.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_colscan(uint32_t *__restrict__ hist, int G, int P,
-                                                 uint32_t *__restrict__ totals) {
-    const int f = blockIdx.x * 256 + threadIdx.x;
-    if (f >= P) return;
-    uint32_t run = 0;
-    int c = 0;
-    for (; c + 4 <= G; c += 4) {
-        uint32_t a = hist[(uint64_t)c * P + f], b = hist[(uint64_t)(c + 1) * P + f];
-        uint32_t d = hist[(uint64_t)(c + 2) * P + f], e = hist[(uint64_t)(c + 3) * P + f];
-        hist[(uint64_t)c * P + f] = run;
-        hist[(uint64_t)(c + 1) * P + f] = run + a;
-        hist[(uint64_t)(c + 2) * P + f] = run + a + b;
-        hist[(uint64_t)(c + 3) * P + f] = run + a + b + d;
-        run += a + b + d + e;
+__global__ void __launch_bounds__(1024) k_colscan(uint32_t *__restrict__ hist, int G, int P,
+                                                  uint32_t *__restrict__ totals) {
+    __shared__ uint32_t seg[32][33];
+    const int f = blockIdx.x * 32 + threadIdx.x;
+    const int per = (G + 31) / 32;
+    const int c0 = min(G, (int)threadIdx.y * per), c1 = min(G, c0 + per);
+    uint32_t sum = 0;
+    if (f < P)
+        for (int c = c0; c < c1; c++) sum += hist[(uint64_t)c * P + f];
+    seg[threadIdx.y][threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        uint32_t run = 0;
+        for (int y = 0; y < 32; y++) {
+            const uint32_t v = seg[y][threadIdx.x];
+            seg[y][threadIdx.x] = run;
+            run += v;
+        }
+        if (f < P) totals[f] = run;
     }
-    for (; c < G; c++) {
-        uint32_t a = hist[(uint64_t)c * P + f];
-        hist[(uint64_t)c * P + f] = run;
-        run += a;
+    __syncthreads();
+    if (f < P) {
+        uint32_t run = seg[threadIdx.y][threadIdx.x];
+        for (int c = c0; c < c1; c++) {
+            const uint32_t v = hist[(uint64_t)c * P + f];
+            hist[(uint64_t)c * P + f] = run;
+            run += v;
+        }
     }
-    totals[f] = run;
 }
 
 // ---------------------------------------------------------------------------
@@ -171,17 +182,23 @@ __device__ void plan_bases(const uint32_t *hist, uint64_t *base, uint64_t n, int
         base[f] = run;
         run += hist[f];
     }
-    if (threadIdx.x == 0) base[P] = n;
+    if (threadIdx.x == 0) base[P] = total;  // rows counted (n unless rows were bypassed)
+    (void)n;
     unsigned wmax = warp_max_u32(mx);
     if ((threadIdx.x & 31) == 0 && wmax) atomicMax(maxp, (unsigned long long)wmax);
 }
 
+__global__ void __launch_bounds__(PLAN_THREADS) k_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2,
+                                                            unsigned long long *maxp) {
+    __shared__ uint64_t scratch[PLAN_THREADS / 32 + 1];
+    plan_bases(totals, base, 0, 1 << P_log2, maxp, scratch);
+}
+
+// Join work items from both relations' totals and bases (written by
+// k_plan_bases).
 __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
     __shared__ uint64_t scratch[PLAN_THREADS / 32 + 1];
     const int P = 1 << a.P_log2;
-    plan_bases(a.r.hist, a.r.base, a.nR, P, &a.ctrl->max_part_R, scratch);
-    plan_bases(a.s.hist, a.s.base, a.nS, P, &a.ctrl->max_part_S, scratch);
-    __syncthreads();
 
     const int C = (P + PLAN_THREADS - 1) / PLAN_THREADS;
     const int lo = min(P, (int)threadIdx.x * C), hi = min(P, lo + C);
@@ -436,7 +453,8 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
         }
     }
     __syncthreads();
-    const uint64_t lo = (uint64_t)c * a.chunk, hi = umin64(a.n, lo + a.chunk);
+    const uint64_t lo = (uint64_t)c * a.chunk;
+    const uint64_t hi = a.chunk_len ? lo + a.chunk_len[c] : umin64(a.n, lo + a.chunk);
     DigitOp dop{0u, (uint32_t)F - 1};
     part_range<PART_THREADS>(a.in, lo, hi, a.out, (uint32_t)a.n, dop, F, sm, a.err);
 }
@@ -490,7 +508,14 @@ cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G,
 }
 
 cudaError_t launch_colscan(uint32_t *hist, int G, int P, uint32_t *totals, cudaStream_t st) {
-    k_colscan<<<(P + 255) / 256, 256, 0, st>>>(hist, G, P, totals);
+    k_colscan<<<(P + 31) / 32, dim3(32, 32), 0, st>>>(hist, G, P, totals);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2, unsigned long long *maxp,
+                              cudaStream_t st) {
+    k_plan_bases<<<1, PLAN_THREADS, 0, st>>>(totals, base, P_log2, maxp);
     count_launch();
     return cudaGetLastError();
 }

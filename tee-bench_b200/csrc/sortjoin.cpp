@@ -15,8 +15,6 @@ namespace tbg {
 
 cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaStream_t st);
 int rsm_ctas_per_sm(int capR);
-cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_t *bases, int nsm,
-                              cudaStream_t st);
 cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t ns, uint64_t *splits,
                               unsigned long long *matches, unsigned long long *rows_ctr, tbg_row_out *out,
                               uint64_t cap, bool mat, cudaStream_t st);
@@ -55,7 +53,7 @@ int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const 
 }
 
 // LSD sort of n rows by key; returns the buffer holding the sorted rows.
-static int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist,
+int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist,
                     const uint64_t *dbases, int slot0, Workspace &w, cudaStream_t st, const Row **out,
                     int *passes) {
     const Row *src = in;

@@ -77,6 +77,7 @@ struct PartArgs {
     Row *out;
     uint64_t n;               // rows (< 2^32)
     uint64_t chunk;           // rows per pass-1 chunk
+    const uint32_t *chunk_len;  // rows of chunk c (null: full chunks of `chunk` rows)
     int G;                    // chunks
     int group;                // pass 2: consecutive chunks per unit
     int b1, b2;               // digit bits of pass 1 and pass 2 (b2 = 0: one pass)
@@ -138,6 +139,8 @@ cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G,
                                int P_log2, RadixF rf, cudaStream_t st);
 cudaError_t launch_colscan(uint32_t *hist, int G, int P, uint32_t *totals, cudaStream_t st);
 cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st);
+cudaError_t launch_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2, unsigned long long *maxp,
+                              cudaStream_t st);
 cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st);
 cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st);
 cudaError_t launch_scatter(const ScatterArgs &a, uint64_t max_tiles, cudaStream_t st);

@@ -27,10 +27,13 @@ struct Workspace {
     DevBuf ctrl, histR, histS, totR, totS, baseR, baseS, off1R, off1S, cnt1R, cnt1S;
     DevBuf status, tmpR, tmpS, partR, partS, items, misc;
     DevBuf inR, inS, rows;      // drop-in layer: device copies of host inputs and output rows
+    DevBuf sc, kept;            // learned path: compacted S and kept rows per chunk
     DevBuf aux[8];              // algorithm-specific scratch (sort, learned model)
     uint32_t epoch = 0;         // last look-back epoch used on `status`
     Ctrl *host_ctrl = nullptr;  // pinned mirror of the control block
     cudaEvent_t ev[8];
+    cudaStream_t side = nullptr;       // second stream (learned path), created on first use
+    cudaEvent_t fork = nullptr, joined = nullptr;
     uint32_t next_epoch(cudaStream_t st);
 };
 
@@ -58,8 +61,41 @@ int join_device_impl(const tbg_config *cfg, const Row *dR, uint64_t nR, const Ro
 int finish_join(const tbg_config &cfg, Workspace &w, cudaStream_t st, const JoinRun &run,
                 uint64_t nR, uint64_t nS, uint64_t cap, uint64_t *matches, tbg_stats *stats);
 
+// Heavy-key table used by the S histogram of the learned path (device pointers).
+struct SBypass {
+    const uint32_t *filter;
+    const uint32_t *keys;
+    const unsigned *cnt;
+    const unsigned *start;
+    const uint32_t *rpay;
+    tbg_row_out *rows;
+    uint64_t cap;
+};
+struct RadixGeom {
+    int B, passes, b1, b2;
+    uint64_t P, F1;
+    int capR, join_grid;
+    uint64_t capS, item_cap;
+    int G[2];          // chunks of R, S
+    uint64_t ch[2];    // rows per chunk
+    uint64_t n[2];     // rows of R, S
+    RadixF rf;
+};
+RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int capR, Workspace &w);
+int ensure_radix_buffers(const RadixGeom &g, bool bypass, Workspace &w);
+int part_histogram(int rel, const RadixGeom &g, const Row *d, const tbg_config &cfg, Workspace &w, cudaStream_t st,
+                   const SBypass *bypass);
+int part_pass(int rel, int which, const RadixGeom &g, const Row *d, Workspace &w, cudaStream_t st, bool bypass);
+int plan_items(const RadixGeom &g, Workspace &w, cudaStream_t st);
+void mark(Workspace &w, bool timing, int i, cudaStream_t st);
 int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                     int capR, Workspace &w, cudaStream_t st, JoinRun *run, int *join_grid_out);
+int radix_join_phase(const tbg_config &cfg, tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
+                     JoinRun *run, int capR, int join_grid);
+int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, const uint64_t *dbases,
+             int slot0, Workspace &w, cudaStream_t st, const Row **out, int *passes);
+cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_t *bases, int nsm,
+                              cudaStream_t st);
 int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                    tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
 int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,

@@ -1,0 +1,157 @@
+"""LRN, the learned skew-aware join: the GPU model kernels against the float64
+oracle, exactness against the reference's RHO result, the fallback, and what
+the trained network gains over the same method without it."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import gen_relation
+from gpu_util import dev_relation, run_join
+
+pytestmark = pytest.mark.gpu
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def zipf_cdf_points(n=4096, N=1 << 20, z=1.0, seed=0):
+    """Training points shaped like LRN's: log-key feature -> empirical CDF."""
+    rng = np.random.default_rng(seed)
+    w = 1.0 / np.arange(1, N + 1) ** z
+    cdf = np.cumsum(w) / w.sum()
+    keys = np.sort(np.searchsorted(cdf, rng.random(n)) + 1)
+    x = (np.log2(keys + 1.0) / 16.0 - 1.0).astype(np.float32)
+    y = ((np.arange(n) + 0.5) / n).astype(np.float32)
+    return x, y
+
+
+def test_gpu_gradient_matches_oracle(tbg, oracle, cuda):
+    H = 32
+    x, y = zipf_cdf_points(1000, seed=1)
+    for seed in (1, 2, 3):
+        p = tbg.mlp_init(seed)
+        loss, g = tbg.mlp_grad(p, x, y)
+        loss_ref, g_ref = oracle.mlp_loss_grad(H, p, x, y)
+        assert abs(loss - loss_ref) <= 1e-4 * max(1.0, abs(loss_ref))
+        # float32 forward/backward and float32 accumulation against float64
+        err = np.abs(g.astype(np.float64) - g_ref)
+        assert np.all(err <= 2e-3 * np.abs(g_ref) + 2e-5), (err.max(), np.abs(g_ref).max())
+
+
+def test_gpu_forward_matches_oracle(tbg, oracle, cuda):
+    # the gradient kernel's loss with y = 0 is the mean squared output
+    x = np.linspace(-1, 1, 257).astype(np.float32)
+    p = tbg.mlp_init(9)
+    out = oracle.mlp_forward(32, p, x)
+    loss, _ = tbg.mlp_grad(p, x, np.zeros_like(x))
+    assert abs(loss - float(np.mean(out ** 2))) <= 1e-4 * max(1.0, float(np.mean(out ** 2)))
+
+
+def test_training_reduces_loss(tbg, oracle, cuda):
+    x, y = zipf_cdf_points(8192, seed=2)
+    p0 = tbg.mlp_init(5)
+    l0, _ = tbg.mlp_grad(p0, x, y)
+    p1 = tbg.mlp_train(p0, x, y, steps=300, lr=0.01, seed=7)
+    l1, _ = tbg.mlp_grad(p1, x, y)
+    l1_ref, _ = oracle.mlp_loss_grad(32, p1, x, y)
+    assert abs(l1 - l1_ref) <= 1e-4 * max(1.0, l1_ref)
+    assert l1 < l0 / 20 and l1 < 2e-3, (l0, l1)
+
+
+@pytest.mark.parametrize("idx", range(8))
+def test_lrn_matches_reference_golden(tbg, oracle, golden, cuda, idx):
+    j = golden["joins"][idx]
+    R = gen_relation(oracle, j["R"], j["seedR"], 0)
+    S = gen_relation(oracle, j["S"], j["seedS"], 1)
+    m, _, st = run_join(tbg, cuda, "LRN", R, S)
+    assert m == j["RHO_n1"]
+    m2, rows, st2 = run_join(tbg, cuda, "LRN", R, S, materialize=True)
+    assert m2 == j["RHO_mat_count"] == len(rows)
+    assert sha(oracle.sort_rows(rows)) == j["RHO_mat_sorted_sha256"]
+    if j["name"] == "zipf15":  # most of S sits on a few keys: the heavy path runs
+        assert st.used_fallback == 0 and st.heavy_keys > 0 and st.heavy_rows_S > len(S) // 2
+
+
+def test_lrn_falls_back_on_uniform_data(tbg, oracle, cuda):
+    R = gen_relation(oracle, ("pk", 1 << 16, 0, 0.0), 3, 0)
+    S = gen_relation(oracle, ("fk", 1 << 19, 1 << 16, 0.0), 4, 1)
+    m, _, st = run_join(tbg, cuda, "LRN", R, S)
+    assert m == 1 << 19 and st.used_fallback == 1 and st.heavy_rows_S == 0
+
+
+def test_lrn_duplicate_R_keys_on_heavy_path(tbg, oracle, cuda):
+    """Heavy keys with several R rows: every (R, S) pair is produced."""
+    rng = np.random.default_rng(23)
+    R = np.zeros(50000, dtype=oracle.ROW)
+    R["key"] = rng.integers(1, 20000, len(R))
+    R["key"][:30] = 1
+    R["key"][30:40] = 2
+    S = gen_relation(oracle, ("zipf", 1 << 19, 20000, 1.5), 8, 1)
+    oracle.fill_payloads(R, 0)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    m, rows, st = run_join(tbg, cuda, "LRN", R, S, materialize=True, cap=ref)
+    assert st.used_fallback == 0 and st.heavy_rows_S > 0
+    assert m == ref and np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+
+
+def test_lrn_dropin(tbg, oracle, cuda):
+    R = gen_relation(oracle, ("pk", 1 << 16, 0, 0.0), 11111, 0)
+    S = gen_relation(oracle, ("zipf", 1 << 19, 1 << 16, 1.0), 22222, 1)
+    ref = oracle.rho(R, S)
+    assert tbg.find("LRN").join(R, S, 4) == ref
+    c, rows = tbg.find("LRN").join(R, S, 2, materialize=True)
+    assert c == ref and len(rows) == ref
+
+
+def _ablation(tbg, cuda, nR, nS, z):
+    tR, pR = dev_relation(cuda, nR)
+    tS, pS = dev_relation(cuda, nS)
+    tbg.gen_pk(pR, nR, 1)
+    tbg.gen_zipf(pS, nS, nR, z, 0, 2)
+    cuda.cuda.synchronize()
+    out = {}
+    for name, algo, model in [("radix", "RHO", 0), ("trained", "LRN", tbg.MODEL_MLP),
+                              ("untrained", "LRN", tbg.MODEL_UNTRAINED), ("sample", "LRN", tbg.MODEL_QUANTILE)]:
+        cfg = tbg.config(algo, model=model)
+        _, m, st = tbg.join_device(cfg, pR, nR, pS, nS)
+        out[name] = (m, st.heavy_rows_S / nS, st.used_fallback, st.train_loss)
+    return out
+
+
+def test_trained_network_gain_over_method_without_it(tbg, cuda):
+    """Same pipeline, same data (Zipf over R's keys, hot keys at small ranks as
+    the reference generator makes them).  At z = 1.0 the trained frequency
+    model routes the heaviest keys (a large share of S) around partitioning,
+    the untrained network picks candidates at random and routes far less.  At
+    z = 0.5 no key is heavy: the trained model predicts that and falls back to
+    radix, the untrained one commits to a bypass that cannot pay.  Results are
+    identical in every case."""
+    nR, nS = 1 << 22, 1 << 25
+    o = _ablation(tbg, cuda, nR, nS, 1.0)
+    counts = {k: v[0] for k, v in o.items()}
+    assert len(set(counts.values())) == 1 and counts["radix"] == nS
+    assert o["trained"][2] == 0 and o["trained"][1] > 0.30, o
+    assert o["untrained"][1] < o["trained"][1] - 0.10, o
+    assert o["trained"][1] > 0.8 * o["sample"][1], o
+    o = _ablation(tbg, cuda, nR, nS, 0.5)
+    assert len({v[0] for v in o.values()}) == 1
+    assert o["trained"][2] == 1, o          # predicted no heavy mass: radix
+    assert o["sample"][2] == 1, o
+
+
+def test_full_size_skewed_config(tbg, cuda):
+    """|R| = 2^26, |S| = 2^29 Zipf z = 1.0: LRN and RHO agree with |S|."""
+    nR, nS = 1 << 26, 1 << 29
+    tR, pR = dev_relation(cuda, nR)
+    tS, pS = dev_relation(cuda, nS)
+    tbg.gen_pk(pR, nR, 11111)
+    tbg.gen_zipf(pS, nS, nR, 1.0, 0, 22222)
+    cuda.cuda.synchronize()
+    _, m1, st1 = tbg.join_device(tbg.config("LRN"), pR, nR, pS, nS)
+    _, m0, st0 = tbg.join_device(tbg.config("RHO"), pR, nR, pS, nS)
+    assert m0 == m1 == nS
+    assert st1.used_fallback == 0 and st1.heavy_rows_S > nS // 3
