@@ -53,6 +53,46 @@ WORKLOADS = {
 }
 
 
+# Batched workload (4096 joins): |R_i| = round(2^U), U ~ Uniform[lo, hi];
+# |S_i| = k |R_i|, k ~ UniformInt[1, 16]; R_i a seeded permutation of
+# 1..|R_i|; S_i uniform foreign keys, or Zipf z = 1.0 over R_i's keys for a
+# seeded 20% of the joins.
+BATCH_WORKLOADS = {
+    # name: (joins, log2 |R| low, log2 |R| high, Zipf fraction)
+    "batch_c4": (4096, 10, 20, 0.2),
+}
+
+
+def batch_sizes(njoins, lo, hi, zipf_frac, seed=4):
+    rs = np.random.RandomState(seed)
+    nR = np.round(2.0 ** rs.uniform(lo, hi, njoins)).astype(np.int64)
+    k = rs.randint(1, 17, njoins)
+    zipf = rs.random_sample(njoins) < zipf_frac
+    return nR, nR * k, zipf
+
+
+def make_batch_device(torch, tbg, njoins, lo, hi, zipf_frac, seed=4, stream=0):
+    """Generates the batched workload on the device (the library's seeded
+    generators) in one buffer.  Returns (buffer, [(dR, nR, dS, nS)], zipf)."""
+    nR, nS, zipf = batch_sizes(njoins, lo, hi, zipf_frac, seed)
+    total = int(nR.sum() + nS.sum())
+    buf = torch.empty(max(total, 1), dtype=torch.int64, device="cuda")
+    base = buf.data_ptr()
+    joins, off = [], 0
+    for i in range(njoins):
+        pR = base + 8 * off
+        off += int(nR[i])
+        pS = base + 8 * off
+        off += int(nS[i])
+        tbg.gen_pk(pR, int(nR[i]), 1000 + 2 * i + seed * 100003, stream)
+        if zipf[i]:
+            tbg.gen_zipf(pS, int(nS[i]), int(nR[i]), 1.0, 0, 1001 + 2 * i + seed * 100003, stream)
+        else:
+            tbg.gen_fk(pS, int(nS[i]), int(nR[i]), 1001 + 2 * i + seed * 100003, stream)
+        joins.append((pR, int(nR[i]), pS, int(nS[i])))
+    return buf, joins, zipf
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 

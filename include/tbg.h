@@ -233,6 +233,41 @@ TBG_API int tbg_mlp_grad(const float *params, const float *x, const float *y, ui
 TBG_API int tbg_mlp_train(float *params, const float *x, const float *y, uint64_t n, int steps,
                           float lr, uint64_t seed);
 
+/* ---- batched joins (many independent joins, one persistent launch) -------- *
+ * No counterpart in the reference, whose driver runs one join per call
+ * (App/main.cpp:157-196); each join's count equals RHO's on that join.     */
+typedef struct tbg_batch_join {
+    const struct row_t *dR; /* device memory, 8-byte aligned                   */
+    uint64_t nR;            /* < 2^32                                          */
+    const struct row_t *dS;
+    uint64_t nS;
+} tbg_batch_join;
+
+typedef struct tbg_batch tbg_batch; /* opaque plan: tuned, graph-captured */
+
+/* Plans njoins joins.  cfg (NULL = defaults): algo TBG_RHO or TBG_RHT (RHT
+ * fixes the histogram table layout), count only; radix_bits 0 autotunes the
+ * partitioning (direct or 1..8 radix bits), table layout, S rows per work
+ * item and chunk size per size class by timing the batch's own joins;
+ * radix_bits > 0 partitions every join with that many bits (one pass, <= 8);
+ * radix_bits < 0 uses the built-in heuristic without timing.  The whole
+ * batch is captured as one CUDA graph.  Waits for `stream` (the inputs may be
+ * written there), then works on a private stream; the relations must stay
+ * allocated, at the same addresses, until tbg_batch_destroy (their contents
+ * may change between runs).                                                */
+TBG_API int tbg_batch_create(const tbg_batch_join *joins, int njoins, const tbg_config *cfg,
+                             void *stream, tbg_batch **out);
+/* Replays the graph on `stream` (asynchronous); d_counts[i] (device, may be
+ * NULL) receives join i's match count. */
+TBG_API int tbg_batch_run(tbg_batch *b, uint64_t *d_counts, void *stream);
+/* Waits for the last run; returns its device status (TBG_ERR_TIMEOUT if a
+ * bounded wait inside the kernel gave up). */
+TBG_API int tbg_batch_sync(tbg_batch *b);
+/* JSON summary of the plan (grid, tickets, per-size-class choices and tuned
+ * times) into buf[cap]; returns the full length. */
+TBG_API int tbg_batch_describe(const tbg_batch *b, char *buf, size_t cap);
+TBG_API void tbg_batch_destroy(tbg_batch *b);
+
 /* ---- on-GPU seeded generators (App/Lib/generator.cpp semantics) ----------- */
 /* pk: keys a seeded permutation of 1..n, payload = row index.               */
 TBG_API int tbg_gen_pk(struct row_t *d, uint64_t n, uint64_t seed, void *stream);

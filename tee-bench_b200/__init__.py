@@ -149,12 +149,15 @@ def lib():
         f.restype = I
     L.tbg_rows_checksum.argtypes = [P, U64, C.POINTER(U64), P]
     L.tbg_rows_checksum.restype = I
-    if hasattr(L, "tbg_batch_create"):
-        L.tbg_batch_create.argtypes = [C.POINTER(BatchJoin), I, C.POINTER(Config), P, C.POINTER(P)]
-        L.tbg_batch_create.restype = I
-        L.tbg_batch_run.argtypes = [P, P, P]
-        L.tbg_batch_run.restype = I
-        L.tbg_batch_destroy.argtypes = [P]
+    L.tbg_batch_create.argtypes = [C.POINTER(BatchJoin), I, C.POINTER(Config), P, C.POINTER(P)]
+    L.tbg_batch_create.restype = I
+    L.tbg_batch_run.argtypes = [P, P, P]
+    L.tbg_batch_run.restype = I
+    L.tbg_batch_sync.argtypes = [P]
+    L.tbg_batch_sync.restype = I
+    L.tbg_batch_describe.argtypes = [P, C.c_char_p, C.c_size_t]
+    L.tbg_batch_describe.restype = I
+    L.tbg_batch_destroy.argtypes = [P]
     L.tbg_last_transfer_bytes.argtypes = [C.POINTER(U64), C.POINTER(U64)]
     L.tbg_mlp_param_count.restype = I
     L.tbg_mlp_feature.argtypes = [C.c_uint32]
@@ -326,6 +329,48 @@ def mlp_train(params, x, y, steps, lr=0.01, seed=1):
 def mlp_feature(keys) -> np.ndarray:
     """Model input of keys: log2(key + 1) / 16 - 1 (what LRN feeds the MLP)."""
     return (np.log2(np.asarray(keys, dtype=np.float64) + 1.0) / 16.0 - 1.0).astype(np.float32)
+
+
+# ------------------------------------------------------------------ batches
+class Batch:
+    """Many independent joins planned once (autotuned, one CUDA graph) and
+    replayed with run(); joins = [(dR, nR, dS, nS), ...] device pointers."""
+
+    def __init__(self, joins, cfg: Config = None, stream: int = 0):
+        L = lib()
+        self.n = len(joins)
+        arr = (BatchJoin * max(1, self.n))()
+        for i, (dR, nR, dS, nS) in enumerate(joins):
+            arr[i] = BatchJoin(dR or None, nR, dS or None, nS)
+        h = C.c_void_p()
+        _check(L.tbg_batch_create(arr, self.n, C.byref(cfg) if cfg is not None else None, stream or None,
+                                  C.byref(h)))
+        self._h = h
+
+    def run(self, d_counts: int = 0, stream: int = 0):
+        _check(lib().tbg_batch_run(self._h, d_counts or None, stream or None))
+
+    def sync(self):
+        _check(lib().tbg_batch_sync(self._h))
+
+    def describe(self) -> dict:
+        import json
+        L = lib()
+        n = L.tbg_batch_describe(self._h, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        L.tbg_batch_describe(self._h, buf, n + 1)
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if self._h:
+            lib().tbg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def kernel_launches() -> int:

@@ -1,0 +1,141 @@
+// Device building blocks of the build/probe join (shared-memory bucket-chain
+// or histogram table, count probe), shared by the single-join kernel
+// (join.cu) and the batched join (batch.cu).
+#pragma once
+
+#include "tbg_device.cuh"
+
+namespace tbg {
+
+struct Table {
+    uint32_t *key;    // [capR]
+    uint32_t *pay;    // [capR]
+    uint32_t *heads;  // layout 0: [N] 1-based chain heads; layout 1: [Nb+1] starts, then cursors
+    uint16_t *next;   // layout 0: [capR] 1-based next links
+    uint32_t mask;    // bucket mask
+    int hs;           // hash shift (radix bits already consumed)
+    int layout;
+
+    __device__ __forceinline__ uint32_t bucket(uint32_t k) const { return (k >> hs) & mask; }
+
+    template <class Fn>
+    __device__ __forceinline__ void for_each(uint32_t k, Fn fn) const {
+        const uint32_t b = bucket(k);
+        if (layout == 0) {
+            for (uint32_t h = heads[b]; h; h = next[h - 1])
+                if (key[h - 1] == k) fn(pay[h - 1]);
+        } else {
+            for (uint32_t j = heads[b], e = heads[b + 1]; j < e; j++)
+                if (key[j] == k) fn(pay[j]);
+        }
+    }
+    __device__ __forceinline__ uint32_t count(uint32_t k) const {
+        uint32_t c = 0;
+        const uint32_t b = bucket(k);
+        if (layout == 0) {
+            for (uint32_t h = heads[b]; h; h = next[h - 1]) c += (key[h - 1] == k);
+        } else {
+            for (uint32_t j = heads[b], e = heads[b + 1]; j < e; j++) c += (key[j] == k);
+        }
+        return c;
+    }
+};
+
+
+// R rows are read with plain loads, or with L2-only loads (CG) when they were
+// written earlier in the same kernel launch by other CTAs.
+template <bool CG>
+__device__ __forceinline__ uint2 ld_row(const Row *R, uint64_t i) {
+    const uint2 *p = reinterpret_cast<const uint2 *>(R) + i;
+    if (CG) return __ldcg(p);
+    return *p;
+}
+template <bool CG>
+__device__ __forceinline__ uint4 ld_pair(const uint4 *p) {
+    if (CG) return __ldcg(p);
+    return ldg_stream(p);
+}
+
+template <int THREADS, bool CG = false>
+__device__ void build_table(Table &t, const Row *__restrict__ R, uint64_t r_off, uint32_t r_len,
+                            uint64_t *scan_scratch) {
+    const int tid = threadIdx.x;
+    if (t.layout == 0) {
+        const uint32_t N = next_pow2(r_len);
+        t.mask = N - 1;
+        for (uint32_t i = tid; i < r_len; i += THREADS) {
+            uint2 x = ld_row<CG>(R, r_off + i);
+            t.key[i] = x.x;
+            t.pay[i] = x.y;
+        }
+        for (uint32_t i = tid; i < N; i += THREADS) t.heads[i] = 0;
+        __syncthreads();
+        for (uint32_t i = tid; i < r_len; i += THREADS) {
+            uint32_t b = t.bucket(t.key[i]);
+            t.next[i] = (uint16_t)atomicExch(&t.heads[b], i + 1);
+        }
+        __syncthreads();
+    } else {
+        uint32_t Nb = next_pow2(r_len) >> 2;
+        if (Nb < 4) Nb = 4;
+        t.mask = Nb - 1;
+        uint32_t *cnt = t.heads;            // [Nb + 1]
+        uint32_t *cur = t.heads + Nb + 1;   // cursors, Nb entries (fits: capR + 2 >= 2 Nb + 1)
+        for (uint32_t i = tid; i <= Nb; i += THREADS) cnt[i] = 0;
+        __syncthreads();
+        for (uint32_t i = tid; i < r_len; i += THREADS)
+            atomicAdd(&cnt[t.bucket(ld_row<CG>(R, r_off + i).x)], 1u);
+        __syncthreads();
+        // exclusive scan of cnt[0..Nb) in place, cnt[Nb] = r_len
+        const uint32_t per = (Nb + THREADS - 1) / THREADS;
+        const uint32_t lo = min(Nb, tid * per), hi = min(Nb, lo + per);
+        uint64_t s = 0;
+        for (uint32_t i = lo; i < hi; i++) s += cnt[i];
+        uint64_t tot;
+        uint64_t run = block_excl_scan<THREADS>(s, &tot, scan_scratch);
+        for (uint32_t i = lo; i < hi; i++) {
+            uint32_t c = cnt[i];
+            cnt[i] = (uint32_t)run;
+            cur[i] = (uint32_t)run;
+            run += c;
+        }
+        if (tid == 0) cnt[Nb] = r_len;
+        __syncthreads();
+        for (uint32_t i = tid; i < r_len; i += THREADS) {
+            uint2 x = ld_row<CG>(R, r_off + i);
+            uint32_t pos = atomicAdd(&cur[t.bucket(x.x)], 1u);
+            t.key[pos] = x.x;
+            t.pay[pos] = x.y;
+        }
+        __syncthreads();
+    }
+}
+
+// Matches of S rows [0, len) (row pointer s, any 8-byte alignment) against
+// the table, this thread's share: 16-byte loads, four in flight.
+template <int THREADS, bool CG = false>
+__device__ __forceinline__ unsigned long long probe_count(const Table &t, const Row *s, uint64_t len) {
+    unsigned long long local = 0;
+    const uint64_t head = ((reinterpret_cast<uintptr_t>(s) & 15) && len) ? 1 : 0;
+    const uint64_t body = len - head;
+    const uint64_t nv = body / 2;
+    const bool tail = body & 1;
+    const uint4 *v = reinterpret_cast<const uint4 *>(s + head);
+    const int tid = threadIdx.x;
+    if (head && tid == 0) local += t.count(ld_row<CG>(s, 0).x);
+    if (tail && tid == THREADS - 1) local += t.count(ld_row<CG>(s, len - 1).x);
+    uint64_t i = tid;
+    for (; i + 3 * THREADS < nv; i += 4 * THREADS) {
+        uint4 x0 = ld_pair<CG>(v + i), x1 = ld_pair<CG>(v + i + THREADS);
+        uint4 x2 = ld_pair<CG>(v + i + 2 * THREADS), x3 = ld_pair<CG>(v + i + 3 * THREADS);
+        local += t.count(x0.x) + t.count(x0.z) + t.count(x1.x) + t.count(x1.z);
+        local += t.count(x2.x) + t.count(x2.z) + t.count(x3.x) + t.count(x3.z);
+    }
+    for (; i < nv; i += THREADS) {
+        uint4 x0 = ld_pair<CG>(v + i);
+        local += t.count(x0.x) + t.count(x0.z);
+    }
+    return local;
+}
+
+}  // namespace tbg

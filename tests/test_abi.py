@@ -35,6 +35,7 @@ int main(void) {
   O(struct table_t, num_tuples); O(struct table_t, sorted); O(struct output_list_t, next);
   O(struct threadresult_t, threadid); O(struct result_t, nthreads); O(algorithm_t, join);
   O(tbg_config, seed); O(tbg_config, timing); O(tbg_stats, ms_total); O(tbg_stats, kernel_launches);
+  P(tbg_batch_join); O(tbg_batch_join, nS);
   return 0;
 }
 """
@@ -66,6 +67,8 @@ def test_struct_layouts(tbg):
     assert tbg.Config.seed.offset == out["tbg_config.seed"]
     assert C.sizeof(tbg.Stats) == out["tbg_stats"]
     assert tbg.Stats.ms_total.offset == out["tbg_stats.ms_total"]
+    assert C.sizeof(tbg.BatchJoin) == out["tbg_batch_join"] == 32
+    assert tbg.BatchJoin.nS.offset == out["tbg_batch_join.nS"]
 
 
 def test_registry(tbg):
