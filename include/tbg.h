@@ -268,6 +268,25 @@ TBG_API int tbg_batch_sync(tbg_batch *b);
 TBG_API int tbg_batch_describe(const tbg_batch *b, char *buf, size_t cap);
 TBG_API void tbg_batch_destroy(tbg_batch *b);
 
+/* ---- join count without device allocation ---------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * or cudaFree: engines whose device memory is owned and budgeted by their own
+ * pool allocator, and latency-bound pipelines that cannot take the
+ * device-wide synchronisation of cudaFree or an out-of-memory failure in the
+ * middle of a query.  Count-only RHO of device relations with
+ * |R| + |S| <= TBG_STATIC_MAX_ROWS (larger inputs: TBG_ERR_ARG, nothing
+ * launched).  Its scratch is one static device array of about 32.3 MiB
+ * compiled into the library, which every GPU that loads the library holds
+ * until the process exits.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and sizes the grid: make that first call before any
+ * stream capture.  Asynchronous on `stream`: *d_count (device) receives the
+ * count and, if d_status is not NULL, *d_status (device) the kernel's status
+ * (0, or TBG_ERR_TIMEOUT).  Every call reuses the same array, clearing what
+ * must start at zero; calls that overlap on the GPU race, so serialise them. */
+#define TBG_STATIC_MAX_ROWS (1ull << 22)
+TBG_API int tbg_join_count_static(const struct row_t *dR, uint64_t nR, const struct row_t *dS,
+                                  uint64_t nS, uint64_t *d_count, uint32_t *d_status, void *stream);
+
 /* ---- on-GPU seeded generators (App/Lib/generator.cpp semantics) ----------- */
 /* pk: keys a seeded permutation of 1..n, payload = row index.               */
 TBG_API int tbg_gen_pk(struct row_t *d, uint64_t n, uint64_t seed, void *stream);
