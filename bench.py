@@ -218,16 +218,27 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rho_c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="rho_c2", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-log2", type=int, default=27)
+    ap.add_argument("--cpu-sample-log2", type=int, default=29)
+    # smaller cases of the same workload (profiling captures); never the reported configuration
+    ap.add_argument("--log2-r", type=int, default=None)
+    ap.add_argument("--log2-s", type=int, default=None)
+    ap.add_argument("--joins", type=int, default=None)
+    ap.add_argument("--log2-lo", type=int, default=None)
+    ap.add_argument("--log2-hi", type=int, default=None)
+    ap.add_argument("--no-autotune", action="store_true", help="batch: built-in heuristic plan")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload in BATCH_WORKLOADS:
+        return batch_main(args, rank, world, local)
     algo, lr, ls, kind, param = WORKLOADS[args.workload]
+    lr = args.log2_r if args.log2_r is not None else lr
+    ls = args.log2_s if args.log2_s is not None else ls
     nR, nS = 1 << lr, 1 << ls
     workload_name = f"{algo} |R|=2^{lr} |S|=2^{ls} " + (
         f"uniform FK {param}% selectivity" if kind == "fk" else f"Zipf z={param}") + ", count only"
@@ -350,8 +361,8 @@ def main():
                "count": int(cnt)}
 
     peak, peak_kind = read_peaks()
-    # algorithmic bytes: histogram reads 8 B/row; each scatter pass reads and
-    # writes 8 B/row; build/probe reads 8 B/row
+    # algorithmic bytes: histogram reads 8 B/row; each partitioning pass
+    # reads and writes 8 B/row; build/probe reads 8 B/row
     rows = nR + nS
     K = args.steps
     passes = st.passes or 2
@@ -363,8 +374,8 @@ def main():
     if os.path.exists(tp):
         with open(tp) as f:
             tt = json.load(f)
-        k = tt.get("k_scatter")
-        if k:
+        k = tt.get("k_part_pass")
+        if k:  # DRAM bytes per row moved, from one ncu capture; per launch like `achieved`
             traffic = k["dram_bytes_per_row"] * rows * passes
     total_bytes = (8 + 16 * passes + 8) * rows
     pipe_ms = ms / K
@@ -375,15 +386,20 @@ def main():
         "config": {"workload": workload_name, "global_batch": world * rows, "nR": nR, "nS": nS,
                    "radix_bits": st.radix_bits, "passes": st.passes,
                    "parallelism": f"{world} independent joins (R replicated, S per rank)",
-                   "l2": "inputs 9.7 GB per step > 126 MB L2; no flush needed",
-                   "generator": "on-GPU pk / fk permutations (generator.cpp semantics)"},
+                   "l2": f"inputs {rows * 8 / 1e9:.1f} GB per step > 126 MB L2; no flush needed",
+                   "generator": "on-GPU pk / fk / zipf (generator.cpp semantics)"},
         "gpu_launches": int(launches),
         "e2e": e2e,
-        "roofline": {"bound": "hbm", "kernel": "k_scatter (partitioning pass, R and S)",
+        "roofline": {"bound": "hbm",
+                     "kernel": f"k_part_pass1 + k_part_pass2 ({passes} partitioning passes over R and S, "
+                               f"{2 * passes} launches per join)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": traffic,
-                     "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch_row": 16,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "algorithmic_bytes_per_row_per_pass": 16,
+                     "timing": "library CUDA events on the join stream around each pass, summed over "
+                               "the timed steps",
                      "pipeline": {"bytes_per_row": 8 + 16 * passes + 8,
                                   "achieved_gbs": total_bytes / (pipe_ms / 1e3) / 1e9,
                                   "frac": total_bytes / (pipe_ms / 1e3) / 1e9 / peak}},
@@ -399,6 +415,215 @@ def main():
                                     "kind": "reference",
                                     "sample": f"reference {res['algo']} (oracle/_ref) on |R|={res['nR']}, "
                                               f"|S|={res['nS']} rows of the workload, its own timer"}
+        else:
+            line["cpu_baseline"] = {"value": None, "unavailable": why}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------------------------------ batch
+def batch_algorithmic_bytes(dj, desc):
+    """Bytes each join must move under the plan's choices: partitioned joins
+    8 (histogram) + 16 (scatter) + 8 (build/probe) per row; direct joins read
+    S once and R once per S slice."""
+    choice = {c["log2_R"]: c for c in desc["classes"]}
+    total = 0
+    for (_, nR, _, nS) in dj:
+        if not nR or not nS:
+            continue
+        c = choice[int(nR).bit_length() - 1]
+        if c["bits"] > 0:
+            total += 32 * (nR + nS)
+        else:
+            total += 8 * nS + 8 * nR * (-(-nS // c["capS"]))
+    return total
+
+
+def batch_reference_run(njoins, lo, hi, zf, max_rows, threads):
+    """The reference's RHO (oracle/_ref) looped over the first joins of the
+    seeded batch until max_rows input rows, as its driver runs one join per
+    call.  Returns (Mtuples/s, seconds, joins, rows) or (None, why)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if O.ref() is None:
+        return None, "oracle/_ref/libtbref.so not built"
+    nR, nS, zipf = batch_sizes(njoins, lo, hi, zf)
+    rng = np.random.default_rng(4)
+    t = 0.0
+    rows = 0
+    n = 0
+    for i in range(njoins):
+        if rows and rows + nR[i] + nS[i] > max_rows:
+            break
+        R = np.zeros(nR[i], dtype=[("key", "<u4"), ("payload", "<u4")])
+        R["key"] = rng.permutation(nR[i]).astype(np.uint32) + 1
+        S = np.zeros(nS[i], dtype=R.dtype)
+        if zipf[i]:
+            w = 1.0 / np.arange(1, nR[i] + 1)
+            cdf = np.cumsum(w)
+            cdf /= cdf[-1]
+            S["key"] = (np.searchsorted(cdf, rng.random(nS[i])) + 1).astype(np.uint32)
+        else:
+            S["key"] = rng.integers(1, nR[i] + 1, nS[i]).astype(np.uint32)
+        c, _, rt_us = O.ref_join("RHO", R, S, nthreads=threads)
+        if c != nS[i]:
+            return None, f"reference RHO count {c} != {nS[i]} on join {i}"
+        t += rt_us * 1e-6
+        rows += int(nR[i] + nS[i])
+        n += 1
+    return (rows / t / 1e6, t, n, rows), None
+
+
+def batch_main(args, rank, world, local):
+    nj, lo, hi, zf = BATCH_WORKLOADS[args.workload]
+    nj = args.joins or nj
+    lo = args.log2_lo if args.log2_lo is not None else lo
+    hi = args.log2_hi if args.log2_hi is not None else hi
+    workload_name = (f"{nj} batched RHO joins, |R_i| log-uniform 2^{lo}..2^{hi}, |S_i| = k|R_i| k in 1..16, "
+                     f"{int(zf * 100)}% Zipf z=1.0 else uniform FK, count only, one persistent launch (CUDA graph)")
+    metric = "input Mtuples/s sum(|R_i|+|S_i|)/t over the batch, per-join bit-exact counts"
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = host_threads()
+        steps = max(1, args.steps)
+        res, why = None, None
+        vals = []
+        for _ in range(steps):
+            res, why = batch_reference_run(nj, lo, hi, zf, 1 << 27, threads)
+            if res is None:
+                print(json.dumps({"impl": "reference", "unavailable": why}))
+                return 0
+            vals.append(res)
+        v = statistics.median(r[0] for r in vals)
+        _, t, n, rows = vals[-1]
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": v, "unit": "Mtuples/s", "n_gpus": world,
+            "steps": steps, "warmup": 0, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": workload_name, "global_batch": rows},
+            "cpu_baseline": {"value": v, "unit": "Mtuples/s", "cores": threads, "kind": "reference",
+                             "sample": f"reference RHO (oracle/_ref) looped over the first {n} joins of the "
+                                       f"batch ({rows} rows), {threads} threads, its own Total Runtime"},
+            "e2e": {"value": v, "unit": "Mtuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    tbg = importlib.import_module("tee-bench_b200")
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        buf, dj, zipf = make_batch_device(torch, tbg, nj, lo, hi, zf, seed=4 + rank, stream=sh)
+    stream.synchronize()
+    rows = sum(j[1] + j[3] for j in dj)
+    want = [j[3] for j in dj]
+    b = tbg.Batch(dj, tbg.config("RHO", radix_bits=-1 if args.no_autotune else 0), sh)
+    desc = b.describe()
+    counts = torch.empty(nj, dtype=torch.int64, device=dev)
+    for _ in range(args.warmup):
+        b.run(counts.data_ptr(), sh)
+        b.sync()
+    if counts.cpu().tolist() != want:
+        raise SystemExit("wrong per-join counts")
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = tbg.kernel_launches()
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            b.run(counts.data_ptr(), sh)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    b.sync()
+    launches = tbg.kernel_launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    K = args.steps
+    value = world * rows * K / (ms / 1e3) / 1e6
+    peak, peak_kind = read_peaks()
+    alg = batch_algorithmic_bytes(dj, desc)
+    achieved = alg / (ms / K / 1e3) / 1e9
+
+    # e2e through the public batch API: each step copies every join's inputs
+    # from pinned host memory, replays the graph and reads the counts back
+    e2e = None
+    host = None
+    if args.e2e_steps > 0:
+        try:
+            host = torch.empty(buf.numel(), dtype=torch.int64, pin_memory=True)
+        except RuntimeError as ex:
+            e2e = {"value": None, "unavailable": f"pinned host buffer of {buf.numel() * 8} bytes: {ex}"[:200]}
+    if host is not None:
+        host.copy_(buf)
+        hcounts = torch.empty(nj, dtype=torch.int64, pin_memory=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            with torch.cuda.stream(stream):
+                buf.copy_(host, non_blocking=True)
+            b.run(counts.data_ptr(), sh)
+            with torch.cuda.stream(stream):
+                hcounts.copy_(counts, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        el = e0.elapsed_time(e1) / 1e3
+        if world > 1:
+            t = torch.tensor([el], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        if hcounts.tolist() != want:
+            raise SystemExit("wrong per-join counts (e2e)")
+        e2e = {"value": world * rows * args.e2e_steps / el / 1e6, "unit": "Mtuples/s",
+               "h2d_bytes_per_step": int(buf.numel() * 8), "d2h_bytes_per_step": int(nj * 8),
+               "api": "tbg_batch_run with every join's R_i, S_i copied from pinned host memory each step"}
+        del host
+    b.close()
+    line = {
+        "metric": metric, "value": value, "unit": "Mtuples/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": workload_name, "global_batch": world * rows, "joins": nj,
+                   "zipf_joins": int(zipf.sum()), "grid": desc["grid"], "tickets": desc["tickets"],
+                   "autotune_ms": desc["tune_ms"],
+                   "classes": [{k: c[k] for k in ("log2_R", "joins", "bits", "layout", "capS", "chunk")}
+                               for c in desc["classes"]],
+                   "l2": f"inputs {rows * 8 / 1e9:.1f} GB per step > 126 MB L2; no flush needed",
+                   "generator": "on-GPU pk / fk / zipf per join (generator.cpp semantics)"},
+        "gpu_launches": int(launches),
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "kernel": "k_batch (the batch's only kernel; one launch per step)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": alg,
+                     "timing": "CUDA events around each graph replay on its stream"},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        res, why = batch_reference_run(nj, lo, hi, zf, 1 << 27, threads)
+        if res:
+            line["cpu_baseline"] = {"value": res[0], "unit": "Mtuples/s", "cores": threads, "kind": "reference",
+                                    "sample": f"reference RHO (oracle/_ref) looped over the first {res[2]} joins "
+                                              f"({res[3]} rows), its own timer"}
         else:
             line["cpu_baseline"] = {"value": None, "unavailable": why}
     if rank == 0:
