@@ -146,12 +146,14 @@ TBG_API const char *tbg_last_error_string(void);
 /* ---- device-resident API (layer 2) ---------------------------------------- */
 enum { TBG_RHO = 0, TBG_RHT = 1, TBG_RSM = 2, TBG_PSM = 3, TBG_LRN = 4 };
 
-/* learned-partitioner model choices */
+/* LRN model choices: how the heavy (frequent) S keys that bypass
+ * partitioning are picked from the 1% sample's candidate keys */
 enum {
-    TBG_MODEL_MLP = 0,        /* FP32 MLP 1->32->32->1 trained on the GPU     */
-    TBG_MODEL_QUANTILE = 1,   /* ablation: boundaries from sample quantiles    */
+    TBG_MODEL_MLP = 0,        /* FP32 MLP 1->32->32->1, trained on the GPU,
+                                 predicts each candidate's S rows            */
+    TBG_MODEL_SAMPLE = 1,     /* ablation: rank by raw sample counts, no model */
     TBG_MODEL_UNTRAINED = 2,  /* ablation: the MLP at its initialisation       */
-    TBG_MODEL_UNIFORM = 3     /* ablation: equal-width key ranges              */
+    TBG_MODEL_UNIFORM = 3     /* ablation: no heavy keys (plain radix, RHO)    */
 };
 
 typedef struct tbg_config {
@@ -235,7 +237,7 @@ TBG_API int tbg_mlp_train(float *params, const float *x, const float *y, uint64_
 
 /* ---- batched joins (many independent joins, one persistent launch) -------- *
  * No counterpart in the reference, whose driver runs one join per call
- * (App/main.cpp:157-196); each join's count equals RHO's on that join.     */
+ * (native.cpp:125); each join's count equals RHO's on that join.     */
 typedef struct tbg_batch_join {
     const struct row_t *dR; /* device memory, 8-byte aligned                   */
     uint64_t nR;            /* < 2^32                                          */

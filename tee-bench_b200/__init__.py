@@ -29,7 +29,7 @@ OUT_ROW = np.dtype([("key", "<u4"), ("Rpayload", "<u4"), ("Spayload", "<u4")])
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_CAPACITY, ERR_UNKNOWN_ALGO, ERR_NO_DEVICE = range(8)
 RHO_ID, RHT_ID, RSM_ID, PSM_ID, LRN_ID = range(5)
 ALGO_IDS = {"RHO": RHO_ID, "RHT": RHT_ID, "RSM": RSM_ID, "PSM": PSM_ID, "LRN": LRN_ID}
-MODEL_MLP, MODEL_QUANTILE, MODEL_UNTRAINED, MODEL_UNIFORM = range(4)
+MODEL_MLP, MODEL_SAMPLE, MODEL_UNTRAINED, MODEL_UNIFORM = range(4)
 ERRMODE_EXIT, ERRMODE_RETURN = 0, 1
 
 

@@ -12,7 +12,7 @@
 // the device error word to pinned host memory.
 //
 // The reference has no batched mode: its driver runs one join per call
-// (App/main.cpp:157-196), so each join's count here is checked against the
+// (native.cpp:125), so each join's count here is checked against the
 // reference's RHO count of that join.
 #include <algorithm>
 #include <cmath>

@@ -16,8 +16,8 @@
 // items, partitioned rows) is read with L2-only loads.
 //
 // Each join's count equals the reference's RHO count on that join
-// (Joins/radix_join.c:1392-1438; bucket chaining :187-244, histogram join
-// :374-440).
+// (Joins/radix_join.c:1558-1561, join_init_run :1237-1396; bucket
+// chaining :187-244, histogram join :374-440).
 #include "batch.h"
 #include "join_dev.cuh"
 #include "part_dev.cuh"

@@ -2,10 +2,10 @@
 // persistent kernel launch.  Device-side plan structures shared by batch.cu
 // (kernel) and batch.cpp (planner, autotuner, CUDA graph).
 //
-// The reference runs one join per process call (App/main.cpp:157-196 picks
-// the algorithm by name and calls it once; a harness loops RHO over the
-// joins), so there is no counterpart to this layout in the reference; each
-// join's result equals RHO's count (Joins/radix_join.c:1392-1438) on that
+// The reference runs one join per process (native.cpp:125 calls the
+// algorithm picked by name once; a harness loops RHO over the joins), so
+// there is no counterpart to this layout in the reference; each
+// join's result equals RHO's count (Joins/radix_join.c:1558-1561) on that
 // join's two relations.
 #pragma once
 

@@ -138,7 +138,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     // 3. score: the model (or, for the ablation, the sample) proposes; keys the
     // sample saw once are not scored (they cannot reach the threshold)
     const double tau_min = std::max(64.0, (double)nS / (double)(1 << 20));
-    const int use_model = cfg.model == TBG_MODEL_QUANTILE ? 0 : 1;
+    const int use_model = cfg.model == TBG_MODEL_SAMPLE ? 0 : 1;
     const double single = (double)nS / (double)m;
     if ((e = launch_heavy_score(cand, ncand, params, use_model, tau_min, 1.5 * single, lc->bins, lc->mass, s2)) !=
         cudaSuccess)

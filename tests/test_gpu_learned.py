@@ -115,7 +115,7 @@ def _ablation(tbg, cuda, nR, nS, z):
     cuda.cuda.synchronize()
     out = {}
     for name, algo, model in [("radix", "RHO", 0), ("trained", "LRN", tbg.MODEL_MLP),
-                              ("untrained", "LRN", tbg.MODEL_UNTRAINED), ("sample", "LRN", tbg.MODEL_QUANTILE)]:
+                              ("untrained", "LRN", tbg.MODEL_UNTRAINED), ("sample", "LRN", tbg.MODEL_SAMPLE)]:
         cfg = tbg.config(algo, model=model)
         _, m, st = tbg.join_device(cfg, pR, nR, pS, nS)
         out[name] = (m, st.heavy_rows_S / nS, st.used_fallback, st.train_loss)
