@@ -261,6 +261,7 @@ __device__ void join_ticket(const BatchArgs &a, uint32_t q, unsigned char *smem,
     t.next = reinterpret_cast<uint16_t *>(t.heads + capR + 2);
     t.hs = (int)J.B;
     t.layout = (int)J.layout;
+    t.hcap = floor_pow2(capR + 2);
     unsigned long long local = 0;
     if (J.B == 0) {
         const uint64_t lo = (uint64_t)jt.y * J.capS;

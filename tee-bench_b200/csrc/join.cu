@@ -28,6 +28,7 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     t.next = reinterpret_cast<uint16_t *>(t.heads + a.capR + 2);
     t.hs = a.hash_shift;
     t.layout = a.layout;
+    t.hcap = floor_pow2((uint32_t)a.capR + 2);
     const int tid = threadIdx.x;
     const unsigned nitems = *a.nitems;
     unsigned long long local = 0;

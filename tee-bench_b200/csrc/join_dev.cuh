@@ -7,12 +7,20 @@
 
 namespace tbg {
 
+// Largest power of two <= x (x >= 1).
+__host__ __device__ __forceinline__ uint32_t floor_pow2(uint32_t x) {
+    uint32_t p = 1;
+    while (p <= x / 2) p <<= 1;
+    return p;
+}
+
 struct Table {
     uint32_t *key;    // [capR]
     uint32_t *pay;    // [capR]
     uint32_t *heads;  // layout 0: [N] 1-based chain heads; layout 1: [Nb+1] starts, then cursors
     uint16_t *next;   // layout 0: [capR] 1-based next links
     uint32_t mask;    // bucket mask
+    uint32_t hcap;    // head slots available (a power of two <= capR + 2)
     int hs;           // hash shift (radix bits already consumed)
     int layout;
 
@@ -61,7 +69,9 @@ __device__ void build_table(Table &t, const Row *__restrict__ R, uint64_t r_off,
                             uint64_t *scan_scratch) {
     const int tid = threadIdx.x;
     if (t.layout == 0) {
-        const uint32_t N = next_pow2(r_len);
+        // next_pow2(|R_p|) buckets as in the reference, at most hcap (a
+        // longer average chain when capR is not a power of two)
+        const uint32_t N = min(next_pow2(r_len), t.hcap);
         t.mask = N - 1;
         for (uint32_t i = tid; i < r_len; i += THREADS) {
             uint2 x = ld_row<CG>(R, r_off + i);

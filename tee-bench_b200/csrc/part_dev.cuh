@@ -33,7 +33,7 @@ __device__ __forceinline__ void hist_add_warp(uint32_t *h, uint32_t f, bool vali
     }
 }
 
-// Rank of a row within its warp's digit counter (returns the old count).
+// Rank of a row on a shared digit counter (returns the old count).
 // Correct either way; `dup` only picks the faster path.
 __device__ __forceinline__ uint32_t rank_warp(uint32_t *cnt, uint32_t d, bool valid, bool dup) {
     const int lane = threadIdx.x & 31;
@@ -59,9 +59,8 @@ template <int THREADS>
 struct PartSmem {
     static constexpr int NW = THREADS / 32;
     static constexpr int T = THREADS * PART_ITEMS;
-    static constexpr int CW = NW + 1;           // padded (digit, warp) row: spreads banks
     Row buf[2][T + 2];                          // input tile (bulk copy), then the same tile digit-sorted
-    uint32_t cnt[2][SCATTER_FMAX * CW];         // per (digit, warp) counts, double-buffered
+    uint32_t cnt[2][SCATTER_FMAX];              // per-digit counts of the tile, double-buffered
     uint32_t cursor[SCATTER_FMAX];              // next output row of each digit
     uint32_t delta[SCATTER_FMAX];               // cursor - tile offset of the digit
     uint64_t scan[NW + 1];
@@ -103,11 +102,11 @@ __device__ __forceinline__ void issue_tile(const Row *in, const TileGeo &g, Row 
     if (bytes) bulk_g2s(buf + g.a_lo + g.off, in + g.t + g.a_lo, bytes, bar);
 }
 
-// One tile: rows are read from the landed buffer, ranked inside their warp,
-// the (digit, warp) counts are prefixed (column scan per digit + one block
-// scan over digits), then the tile is staged digit-sorted into the same
-// buffer with each row's output position and written out in slot order,
-// so consecutive threads store consecutive rows of each digit's run.
+// One tile: rows are read from the landed buffer and ranked on one shared
+// counter per digit (order inside a digit is free: partitions are
+// multisets), one warp prefixes the counts over digits, then the
+// tile is staged digit-sorted into the same buffer and written out in slot
+// order, so consecutive threads store consecutive rows of each digit's run.
 //
 // kseq counts the tiles this CTA has processed on the barrier pair `mbar`
 // (buffer kseq & 1, phase parity (kseq >> 1) & 1), so a persistent CTA can
@@ -117,7 +116,8 @@ __device__ __forceinline__ void part_tile(const Row *__restrict__ in, const Tile
                                           bool has_next, const TileGeo &gnext, uint2 *__restrict__ out,
                                           uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm,
                                           uint64_t *mbar, unsigned *err) {
-    constexpr int NW = THREADS / 32, CW = NW + 1;
+    constexpr int NW = THREADS / 32;
+    (void)NW;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int b = kseq & 1;
     const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
@@ -137,41 +137,52 @@ __device__ __forceinline__ void part_tile(const Row *__restrict__ in, const Tile
             }
         }
     }
-    for (int i = tid; i < F * CW; i += THREADS) sm.cnt[b ^ 1][i] = 0;
+    for (int i = tid; i < F; i += THREADS) sm.cnt[b ^ 1][i] = 0;
     uint32_t rank[PART_ITEMS];
     const bool dup = warp_has_dups(dop(v[0].x), FULL || wbase + lane < cnt);
 #pragma unroll
     for (int i = 0; i < PART_ITEMS; i++) {
         const bool valid = FULL || wbase + i * 32 + lane < cnt;
-        rank[i] = rank_warp(c + w, valid ? dop(v[i].x) * CW : 0, valid, dup);
+        rank[i] = rank_warp(c, valid ? dop(v[i].x) : 0, valid, dup);
     }
     __syncthreads();
     // the other buffer is free (its tile was written out before this barrier)
     if (tid == 0 && has_next) issue_tile(in, gnext, sm.buf[b ^ 1], &mbar[b ^ 1]);
-    uint32_t tot = 0;
-    if (tid < F) {
+    if (w == 0) {
+        // one warp prefixes the digit counts; lane l owns digits l, l + 32, ...
+        // and the tile lays digits out in that (lane, i) order: any order
+        // works as long as each digit's rows stay contiguous
+        constexpr int PER = SCATTER_FMAX / 32;
+        uint32_t sum = 0;
 #pragma unroll
-        for (int ww = 0; ww < NW; ww++) tot += c[tid * CW + ww];
-    }
-    uint64_t dummy;
-    const uint32_t toff = (uint32_t)block_excl_scan<THREADS, false>(tid < F ? tot : 0, &dummy, sm.scan);
-    if (tid < F) {
-        uint32_t run = toff;
-#pragma unroll
-        for (int ww = 0; ww < NW; ww++) {
-            const uint32_t x = c[tid * CW + ww];
-            c[tid * CW + ww] = run;
-            run += x;
+        for (int i = 0; i < PER; i++) {
+            const int d = lane + 32 * i;
+            sum += d < F ? c[d] : 0;
         }
-        sm.delta[tid] = sm.cursor[tid] - toff;
-        sm.cursor[tid] += tot;
+        uint32_t inc = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        uint32_t run = inc - sum;
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            const int d = lane + 32 * i;
+            if (d < F) {
+                const uint32_t x = c[d];
+                c[d] = run;
+                sm.delta[d] = sm.cursor[d] - run;
+                sm.cursor[d] += x;
+                run += x;
+            }
+        }
     }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < PART_ITEMS; i++) {
         if (FULL || wbase + i * 32 + lane < cnt) {
-            const uint32_t d = dop(v[i].x);
-            const uint32_t j = c[d * CW + w] + rank[i];
+            const uint32_t j = c[dop(v[i].x)] + rank[i];
             sm.buf[b][j] = Row{v[i].x, v[i].y};
         }
     }
@@ -197,10 +208,10 @@ template <int THREADS>
 __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
                            uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm, uint64_t *mbar,
                            uint32_t &kseq, unsigned *err) {
-    constexpr int T = THREADS * PART_ITEMS, CW = THREADS / 32 + 1;
+    constexpr int T = THREADS * PART_ITEMS;
     uint2 *o = reinterpret_cast<uint2 *>(out);
     const int ntiles = (int)((hi - lo + T - 1) / T);
-    for (int i = threadIdx.x; i < F * CW; i += THREADS) sm.cnt[kseq & 1][i] = 0;
+    for (int i = threadIdx.x; i < F; i += THREADS) sm.cnt[kseq & 1][i] = 0;
     __syncthreads();
     if (ntiles == 0) return;
     TileGeo g = tile_geo(in, lo, (uint32_t)umin64(T, hi - lo));

@@ -89,9 +89,19 @@ __global__ void __launch_bounds__(1024) k_colscan(uint32_t *__restrict__ hist, i
     const int f = blockIdx.x * 32 + threadIdx.x;
     const int per = (G + 31) / 32;
     const int c0 = min(G, (int)threadIdx.y * per), c1 = min(G, c0 + per);
+    uint32_t *col = hist + f;
     uint32_t sum = 0;
-    if (f < P)
-        for (int c = c0; c < c1; c++) sum += hist[(uint64_t)c * P + f];
+    if (f < P) {
+        int c = c0;
+        for (; c + 8 <= c1; c += 8) {  // eight independent loads in flight
+            uint32_t x[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) x[u] = col[(uint64_t)(c + u) * P];
+#pragma unroll
+            for (int u = 0; u < 8; u++) sum += x[u];
+        }
+        for (; c < c1; c++) sum += col[(uint64_t)c * P];
+    }
     seg[threadIdx.y][threadIdx.x] = sum;
     __syncthreads();
     if (threadIdx.y == 0) {
@@ -106,9 +116,20 @@ __global__ void __launch_bounds__(1024) k_colscan(uint32_t *__restrict__ hist, i
     __syncthreads();
     if (f < P) {
         uint32_t run = seg[threadIdx.y][threadIdx.x];
-        for (int c = c0; c < c1; c++) {
-            const uint32_t v = hist[(uint64_t)c * P + f];
-            hist[(uint64_t)c * P + f] = run;
+        int c = c0;
+        for (; c + 8 <= c1; c += 8) {
+            uint32_t x[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) x[u] = col[(uint64_t)(c + u) * P];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                col[(uint64_t)(c + u) * P] = run;
+                run += x[u];
+            }
+        }
+        for (; c < c1; c++) {
+            const uint32_t v = col[(uint64_t)c * P];
+            col[(uint64_t)c * P] = run;
             run += v;
         }
     }
@@ -121,48 +142,61 @@ __global__ void __launch_bounds__(1024) k_colscan(uint32_t *__restrict__ hist, i
 // ---------------------------------------------------------------------------
 constexpr int PLAN_THREADS = 1024;
 
-__device__ void plan_bases(const uint32_t *hist, uint64_t *base, uint64_t n, int P,
-                           unsigned long long *maxp, uint64_t *scratch) {
+// Shared-memory index of entry i when every thread scans 32 consecutive
+// entries: one word of padding per 32 keeps those reads conflict-free.
+__device__ __forceinline__ uint32_t skew32(uint32_t i) { return i + (i >> 5); }
+
+// Exclusive scan of hist[0..P) into base[0..P], base[P] = total, and the
+// largest entry into *maxp.  The counts are staged through shared memory
+// (`sh`, P + P / 32 words) so global reads and writes are coalesced.
+__device__ void plan_bases(const uint32_t *hist, uint64_t *base, int P, unsigned long long *maxp, uint64_t *scratch,
+                           uint32_t *sh) {
+    const int tid = threadIdx.x;
+    for (int i = tid; i < P; i += PLAN_THREADS) sh[skew32(i)] = hist[i];
+    __syncthreads();
     const int C = (P + PLAN_THREADS - 1) / PLAN_THREADS;
-    const int lo = min(P, (int)threadIdx.x * C), hi = min(P, lo + C);
+    const int lo = min(P, tid * C), hi = min(P, lo + C);
     uint64_t sum = 0;
     uint32_t mx = 0;
     for (int f = lo; f < hi; f++) {
-        sum += hist[f];
-        mx = max(mx, hist[f]);
+        const uint32_t x = sh[skew32(f)];
+        sum += x;
+        mx = max(mx, x);
     }
     uint64_t total;
     uint64_t run = block_excl_scan<PLAN_THREADS>(sum, &total, scratch);
-    for (int f = lo; f < hi; f++) {
-        base[f] = run;
-        run += hist[f];
+    for (int f = lo; f < hi; f++) {  // prefixes fit 32 bits: a relation holds < 2^32 rows
+        const uint32_t x = sh[skew32(f)];
+        sh[skew32(f)] = (uint32_t)run;
+        run += x;
     }
-    if (threadIdx.x == 0) base[P] = total;  // rows counted (n unless rows were bypassed)
-    (void)n;
+    __syncthreads();
+    for (int i = tid; i < P; i += PLAN_THREADS) base[i] = sh[skew32(i)];
+    if (tid == 0) base[P] = total;  // rows counted (n unless rows were bypassed)
     unsigned wmax = warp_max_u32(mx);
-    if ((threadIdx.x & 31) == 0 && wmax) atomicMax(maxp, (unsigned long long)wmax);
+    if ((tid & 31) == 0 && wmax) atomicMax(maxp, (unsigned long long)wmax);
 }
 
 __global__ void __launch_bounds__(PLAN_THREADS) k_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2,
                                                             unsigned long long *maxp) {
+    extern __shared__ uint32_t sh[];
     __shared__ uint64_t scratch[PLAN_THREADS / 32 + 1];
-    plan_bases(totals, base, 0, 1 << P_log2, maxp, scratch);
+    plan_bases(totals, base, 1 << P_log2, maxp, scratch, sh);
 }
 
 // Join work items from both relations' totals and bases (written by
-// k_plan_bases).
+// k_plan_bases).  Thread t plans partitions t, t + 1024, ... (coalesced
+// reads); its items are written contiguously at its block-scan offset, so
+// the item list is grouped by thread, not sorted by partition.
 __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
     __shared__ uint64_t scratch[PLAN_THREADS / 32 + 1];
     const int P = 1 << a.P_log2;
-
-    const int C = (P + PLAN_THREADS - 1) / PLAN_THREADS;
-    const int lo = min(P, (int)threadIdx.x * C), hi = min(P, lo + C);
     uint64_t cnt = 0, nonempty = 0;
-    for (int f = lo; f < hi; f++) {
-        uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
+    for (int f = threadIdx.x; f < P; f += PLAN_THREADS) {
+        const uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
         if (hr == 0 || hs == 0) continue;
-        uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
-        uint64_t nsc = (nrc == 1 && a.capS) ? (hs + a.capS - 1) / a.capS : 1;
+        const uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
+        const uint64_t nsc = (nrc == 1 && a.capS) ? (hs + a.capS - 1) / a.capS : 1;
         cnt += nrc * nsc;
         nonempty++;
     }
@@ -175,19 +209,20 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
         }
         return;
     }
-    for (int f = lo; f < hi; f++) {
-        uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
+    for (int f = threadIdx.x; f < P; f += PLAN_THREADS) {
+        const uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
         if (hr == 0 || hs == 0) continue;
-        uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
-        uint64_t nsc = (nrc == 1 && a.capS) ? (hs + a.capS - 1) / a.capS : 1;
-        uint64_t sstep = (hs + nsc - 1) / nsc;
+        const uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
+        const uint64_t nsc = (nrc == 1 && a.capS) ? (hs + a.capS - 1) / a.capS : 1;
+        const uint64_t sstep = (hs + nsc - 1) / nsc;
+        const uint64_t rb = a.r.base[f], sb = a.s.base[f];
         for (uint64_t rc = 0; rc < nrc; rc++) {
             for (uint64_t sc = 0; sc < nsc; sc++) {
                 Item it;
                 it.part = (uint32_t)f;
-                it.r_off = a.r.base[f] + rc * (uint64_t)a.capR;
+                it.r_off = rb + rc * (uint64_t)a.capR;
                 it.r_len = (uint32_t)umin64((uint64_t)a.capR, hr - rc * (uint64_t)a.capR);
-                it.s_off = a.s.base[f] + sc * sstep;
+                it.s_off = sb + sc * sstep;
                 it.s_len = umin64(sstep, hs - sc * sstep);
                 a.items[off++] = it;
             }
@@ -311,7 +346,11 @@ cudaError_t launch_colscan(uint32_t *hist, int G, int P, uint32_t *totals, cudaS
 
 cudaError_t launch_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2, unsigned long long *maxp,
                               cudaStream_t st) {
-    k_plan_bases<<<1, PLAN_THREADS, 0, st>>>(totals, base, P_log2, maxp);
+    const int P = 1 << P_log2;
+    const size_t smem = (size_t)(P + P / 32 + 1) * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(k_plan_bases, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_plan_bases<<<1, PLAN_THREADS, smem, st>>>(totals, base, P_log2, maxp);
     count_launch();
     return cudaGetLastError();
 }

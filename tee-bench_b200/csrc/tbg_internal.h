@@ -54,7 +54,7 @@ constexpr int PART_ITEMS = 8;
 
 // Shared-memory table capacity of the build/probe kernels (rows of R_p).
 constexpr int JOIN_THREADS = 512;
-constexpr int JOIN_CAPR_DEFAULT = 8192;
+constexpr int JOIN_CAPR_DEFAULT = 5120;
 
 // Bounded device waits: iterations before a wait gives up with TBG_ERR_TIMEOUT.
 constexpr unsigned int SPIN_LIMIT = 1u << 21;
