@@ -297,13 +297,12 @@ static_assert(sizeof(Item) == 32, "join_ticket reads an item as two 16-byte word
 
 __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch(BatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t mbar[2];
+    __shared__ uint64_t mbar[PART_NBUF];
     __shared__ uint64_t scratch[BATCH_THREADS / 32 + 1];
     __shared__ uint32_t s_ticket, s_item;
     const int tid = threadIdx.x;
     if (tid == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
+        for (int i = 0; i < PART_NBUF; i++) mbar_init(&mbar[i], 1);
         fence_mbar_init();
     }
     uint32_t kseq = 0;

@@ -55,16 +55,20 @@ __device__ __forceinline__ uint32_t rank_warp(uint32_t *cnt, uint32_t d, bool va
 // ---------------------------------------------------------------------------
 // tile scatter shared by both passes
 // ---------------------------------------------------------------------------
+// Tiles in flight per CTA: tile q is loaded and ranked while tile q - 1 is
+// written out and tile q + 1 is being copied in.
+constexpr int PART_NBUF = 3;
+
 template <int THREADS>
 struct PartSmem {
     static constexpr int NW = THREADS / 32;
     static constexpr int T = THREADS * PART_ITEMS;
-    Row buf[2][T + 2];                          // input tile (bulk copy), then the same tile digit-sorted
-    uint32_t cnt[2][SCATTER_FMAX];              // per-digit counts of the tile, double-buffered
+    Row buf[PART_NBUF][T + 2];                  // input tiles (bulk copies), each then staged digit-sorted in place
+    uint32_t cnt[2][SCATTER_FMAX];              // per-digit counts, then tile offsets, of the two newest tiles
+    uint32_t delta[2][SCATTER_FMAX];            // output row - tile slot per digit, of the two newest tiles
     uint32_t cursor[SCATTER_FMAX];              // next output row of each digit
-    uint32_t delta[SCATTER_FMAX];               // cursor - tile offset of the digit
     uint64_t scan[NW + 1];
-    uint64_t mbar[2];
+    uint64_t mbar[PART_NBUF];
 };
 
 // Digit of a pass: a bit field of the key (pass 1: bits [0, b1); pass 2:
@@ -102,29 +106,28 @@ __device__ __forceinline__ void issue_tile(const Row *in, const TileGeo &g, Row 
     if (bytes) bulk_g2s(buf + g.a_lo + g.off, in + g.t + g.a_lo, bytes, bar);
 }
 
-// One tile: rows are read from the landed buffer and ranked on one shared
+// A tile's rows are read from its landed buffer and ranked on one shared
 // counter per digit (order inside a digit is free: partitions are
-// multisets), one warp prefixes the counts over digits, then the
-// tile is staged digit-sorted into the same buffer and written out in slot
-// order, so consecutive threads store consecutive rows of each digit's run.
+// multisets); one warp prefixes the counts over digits while the other warps
+// write out the previous tile; then the tile is staged digit-sorted into its
+// own buffer, to be written out in slot order (consecutive threads store
+// consecutive rows of each digit's run) during the next tile's prefix.
 //
-// kseq counts the tiles this CTA has processed on the barrier pair `mbar`
-// (buffer kseq & 1, phase parity (kseq >> 1) & 1), so a persistent CTA can
-// run many ranges without re-initialising the barriers.
+// Tile q (the CTA's running tile count, continued across ranges so a
+// persistent CTA never re-initialises its barriers) uses buffer q % 3 with
+// barrier mbar[q % 3] at phase parity (q / 3) & 1, and counters and deltas
+// q & 1.
+
+// Waits for tile q and ranks its rows on cnt[q & 1].
 template <int THREADS, bool FULL>
-__device__ __forceinline__ void part_tile(const Row *__restrict__ in, const TileGeo &g, uint32_t kseq,
-                                          bool has_next, const TileGeo &gnext, uint2 *__restrict__ out,
-                                          uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm,
-                                          uint64_t *mbar, unsigned *err) {
-    constexpr int NW = THREADS / 32;
-    (void)NW;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int b = kseq & 1;
+__device__ __forceinline__ void tile_load_rank(const Row *__restrict__ in, const TileGeo &g, uint32_t q, DigitOp dop,
+                                               PartSmem<THREADS> &sm, uint64_t *mbar, uint2 (&v)[PART_ITEMS],
+                                               uint32_t (&rank)[PART_ITEMS], unsigned *err) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
     const uint32_t cnt = g.cnt;
-    uint32_t *c = sm.cnt[b];
-    if (!mbar_wait(&mbar[b], (kseq >> 1) & 1, SPIN_LIMIT * 16)) atomicCAS(err, 0u, (unsigned)TBG_ERR_TIMEOUT);
-    uint2 v[PART_ITEMS];
+    const int b = q % PART_NBUF;
+    if (!mbar_wait(&mbar[b], (q / PART_NBUF) & 1, SPIN_LIMIT * 16)) atomicCAS(err, 0u, (unsigned)TBG_ERR_TIMEOUT);
 #pragma unroll
     for (int i = 0; i < PART_ITEMS; i++) {
         const uint32_t r = wbase + i * 32 + lane;
@@ -137,103 +140,141 @@ __device__ __forceinline__ void part_tile(const Row *__restrict__ in, const Tile
             }
         }
     }
-    for (int i = tid; i < F; i += THREADS) sm.cnt[b ^ 1][i] = 0;
-    uint32_t rank[PART_ITEMS];
+    uint32_t *c = sm.cnt[q & 1];
     const bool dup = warp_has_dups(dop(v[0].x), FULL || wbase + lane < cnt);
 #pragma unroll
     for (int i = 0; i < PART_ITEMS; i++) {
         const bool valid = FULL || wbase + i * 32 + lane < cnt;
         rank[i] = rank_warp(c, valid ? dop(v[i].x) : 0, valid, dup);
     }
-    __syncthreads();
-    // the other buffer is free (its tile was written out before this barrier)
-    if (tid == 0 && has_next) issue_tile(in, gnext, sm.buf[b ^ 1], &mbar[b ^ 1]);
-    if (w == 0) {
-        // one warp prefixes the digit counts; lane l owns digits l, l + 32, ...
-        // and the tile lays digits out in that (lane, i) order: any order
-        // works as long as each digit's rows stay contiguous
-        constexpr int PER = SCATTER_FMAX / 32;
-        uint32_t sum = 0;
+}
+
+// Warp 0: digit counts of tile q -> tile offsets (in place), deltas and
+// cursors; clears the counters of tile q + 1.  Lane l owns digits l, l + 32,
+// ... and the tile lays digits out in that (lane, i) order: any order works
+// as long as each digit's rows stay contiguous.
+template <int THREADS>
+__device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS> &sm) {
+    const int lane = threadIdx.x & 31;
+    constexpr int PER = SCATTER_FMAX / 32;
+    uint32_t *c = sm.cnt[q & 1];
+    uint32_t *dl = sm.delta[q & 1];
+    uint32_t *cn = sm.cnt[(q + 1) & 1];
+    uint32_t sum = 0;
 #pragma unroll
-        for (int i = 0; i < PER; i++) {
-            const int d = lane + 32 * i;
-            sum += d < F ? c[d] : 0;
-        }
-        uint32_t inc = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        uint32_t run = inc - sum;
-#pragma unroll
-        for (int i = 0; i < PER; i++) {
-            const int d = lane + 32 * i;
-            if (d < F) {
-                const uint32_t x = c[d];
-                c[d] = run;
-                sm.delta[d] = sm.cursor[d] - run;
-                sm.cursor[d] += x;
-                run += x;
-            }
-        }
+    for (int i = 0; i < PER; i++) {
+        const int d = lane + 32 * i;
+        sum += d < F ? c[d] : 0;
     }
-    __syncthreads();
+    uint32_t inc = sum;
 #pragma unroll
-    for (int i = 0; i < PART_ITEMS; i++) {
-        if (FULL || wbase + i * 32 + lane < cnt) {
-            const uint32_t j = c[dop(v[i].x)] + rank[i];
-            sm.buf[b][j] = Row{v[i].x, v[i].y};
-        }
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
     }
-    __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < PART_ITEMS; kk++) {
-        const uint32_t j = kk * THREADS + tid;
-        if (FULL || j < cnt) {
-            const Row x = sm.buf[b][j];
-            const uint32_t pos = sm.delta[dop(x.key)] + j;
-            if (pos < out_n) out[pos] = make_uint2(x.key, x.payload);
-            else atomicCAS(err, 0u, (unsigned)TBG_ERR_ARG);
+    uint32_t run = inc - sum;
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int d = lane + 32 * i;
+        if (d < F) {
+            const uint32_t x = c[d];
+            c[d] = run;
+            dl[d] = sm.cursor[d] - run;
+            sm.cursor[d] += x;
+            cn[d] = 0;
+            run += x;
         }
     }
 }
 
+// Stages tile q's rows digit-sorted into its own buffer.
+template <int THREADS, bool FULL>
+__device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, DigitOp dop, PartSmem<THREADS> &sm,
+                                           const uint2 (&v)[PART_ITEMS], const uint32_t (&rank)[PART_ITEMS]) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
+    const uint32_t *c = sm.cnt[q & 1];
+    Row *buf = sm.buf[q % PART_NBUF];
+#pragma unroll
+    for (int i = 0; i < PART_ITEMS; i++) {
+        if (FULL || wbase + i * 32 + lane < g.cnt) {
+            const uint32_t j = c[dop(v[i].x)] + rank[i];
+            buf[j] = Row{v[i].x, v[i].y};
+        }
+    }
+}
+
+// Writes staged tile q (cnt rows) to out, by threads [t0, THREADS).
+template <int THREADS>
+__device__ __forceinline__ void tile_write(uint32_t q, uint32_t cnt, uint2 *__restrict__ out, uint32_t out_n,
+                                           DigitOp dop, PartSmem<THREADS> &sm, int t0, unsigned *err) {
+    if ((int)threadIdx.x < t0) return;
+    const Row *buf = sm.buf[q % PART_NBUF];
+    const uint32_t *dl = sm.delta[q & 1];
+#pragma unroll 4
+    for (uint32_t j = threadIdx.x - t0; j < cnt; j += THREADS - t0) {
+        const Row x = buf[j];
+        const uint32_t pos = dl[dop(x.key)] + j;
+        if (pos < out_n) out[pos] = make_uint2(x.key, x.payload);
+        else atomicCAS(err, 0u, (unsigned)TBG_ERR_ARG);
+    }
+}
+
+__device__ __forceinline__ TileGeo range_tile(const Row *in, uint64_t lo, uint64_t hi, int k, uint32_t T) {
+    const uint64_t t = lo + (uint64_t)k * T;
+    return tile_geo(in, t, (uint32_t)umin64(T, hi - t));
+}
+
 // Scatters rows [lo, hi) of `in`, digit by digit, to out[sm.cursor[d]...];
-// the caller initialises sm.cursor[0..F) and synchronises.  Tile k + 1 is
-// bulk-copied into the second buffer while tile k is processed.  `kseq` is
-// the CTA's running tile count on the barrier pair (see part_tile); the
-// barriers are initialised once by the caller.
+// the caller initialises sm.cursor[0..F) and synchronises.  Three barriers
+// per tile; `kseq` is the CTA's running tile count (see above), and the
+// barriers mbar[0..PART_NBUF) are initialised once by the caller.
 template <int THREADS>
 __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
                            uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm, uint64_t *mbar,
                            uint32_t &kseq, unsigned *err) {
-    constexpr int T = THREADS * PART_ITEMS;
+    constexpr uint32_t T = THREADS * PART_ITEMS;
     uint2 *o = reinterpret_cast<uint2 *>(out);
     const int ntiles = (int)((hi - lo + T - 1) / T);
     for (int i = threadIdx.x; i < F; i += THREADS) sm.cnt[kseq & 1][i] = 0;
     __syncthreads();
     if (ntiles == 0) return;
-    TileGeo g = tile_geo(in, lo, (uint32_t)umin64(T, hi - lo));
-    if (threadIdx.x == 0) issue_tile(in, g, sm.buf[kseq & 1], &mbar[kseq & 1]);
-    for (int k = 0; k < ntiles; k++, kseq++) {
-        const uint64_t t1 = g.t + T;
-        const bool more = k + 1 < ntiles;
-        const TileGeo gn = more ? tile_geo(in, t1, (uint32_t)umin64(T, hi - t1)) : g;
-        if (g.cnt == T) part_tile<THREADS, true>(in, g, kseq, more, gn, o, out_n, dop, F, sm, mbar, err);
-        else part_tile<THREADS, false>(in, g, kseq, more, gn, o, out_n, dop, F, sm, mbar, err);
-        g = gn;
+    if (threadIdx.x == 0) {
+        issue_tile(in, range_tile(in, lo, hi, 0, T), sm.buf[kseq % PART_NBUF], &mbar[kseq % PART_NBUF]);
+        if (ntiles > 1)
+            issue_tile(in, range_tile(in, lo, hi, 1, T), sm.buf[(kseq + 1) % PART_NBUF], &mbar[(kseq + 1) % PART_NBUF]);
     }
-    __syncthreads();  // the last tile's staging buffer is free again
+    uint32_t prev_cnt = 0;
+    for (int k = 0; k < ntiles; k++) {
+        const uint32_t q = kseq + k;
+        const TileGeo g = range_tile(in, lo, hi, k, T);
+        uint2 v[PART_ITEMS];
+        uint32_t rank[PART_ITEMS];
+        if (g.cnt == T) tile_load_rank<THREADS, true>(in, g, q, dop, sm, mbar, v, rank, err);
+        else tile_load_rank<THREADS, false>(in, g, q, dop, sm, mbar, v, rank, err);
+        __syncthreads();
+        if (threadIdx.x < 32) tile_scan<THREADS>(q, F, sm);
+        else if (k > 0) tile_write<THREADS>(q - 1, prev_cnt, o, out_n, dop, sm, 32, err);
+        __syncthreads();
+        // tile q - 1's buffer is free: copy tile k + 2 into it
+        if (threadIdx.x == 0 && k + 2 < ntiles)
+            issue_tile(in, range_tile(in, lo, hi, k + 2, T), sm.buf[(q + 2) % PART_NBUF], &mbar[(q + 2) % PART_NBUF]);
+        if (g.cnt == T) tile_stage<THREADS, true>(g, q, dop, sm, v, rank);
+        else tile_stage<THREADS, false>(g, q, dop, sm, v, rank);
+        __syncthreads();
+        prev_cnt = g.cnt;
+    }
+    tile_write<THREADS>(kseq + ntiles - 1, prev_cnt, o, out_n, dop, sm, 0, err);
+    __syncthreads();  // every buffer is free again
+    kseq += ntiles;
 }
 
-// One range per CTA: initialises the barrier pair held in `sm`.
+// One range per CTA: initialises the barriers held in `sm`.
 template <int THREADS>
 __device__ void part_range(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
                            uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm, unsigned *err) {
     if (threadIdx.x == 0) {
-        mbar_init(&sm.mbar[0], 1);
-        mbar_init(&sm.mbar[1], 1);
+        for (int i = 0; i < PART_NBUF; i++) mbar_init(&sm.mbar[i], 1);
         fence_mbar_init();
     }
     uint32_t kseq = 0;

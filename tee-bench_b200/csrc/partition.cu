@@ -245,9 +245,11 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
     const uint32_t *pre = a.pre + (uint64_t)c * P;
     const uint32_t *nxt = c + 1 < a.G ? a.pre + (uint64_t)(c + 1) * P : a.totals;
     // cursors: sum the chunk's prefix over each pass-1 digit's final partitions
+    // (delta[0] holds the chunk's row count per pass-1 digit until the scatter)
+    uint32_t *rows1 = sm.delta[0];
     for (int i = tid; i < F; i += PART_THREADS) {
         sm.cursor[i] = 0;
-        sm.delta[i] = 0;
+        rows1[i] = 0;
     }
     __syncthreads();
     {
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
             if (s != cur_s) {
                 if (cur_s >= 0) {
                     atomicAdd(&sm.cursor[cur_s], acc_c);
-                    atomicAdd(&sm.delta[cur_s], acc_t);
+                    atomicAdd(&rows1[cur_s], acc_t);
                 }
                 cur_s = s;
                 acc_c = acc_t = 0;
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
         }
         if (cur_s >= 0) {
             atomicAdd(&sm.cursor[cur_s], acc_c);
-            atomicAdd(&sm.delta[cur_s], acc_t);
+            atomicAdd(&rows1[cur_s], acc_t);
         }
     }
     __syncthreads();
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
         sm.cursor[s] = cur;
         if (a.off1) {
             a.off1[(uint64_t)c * F + s] = cur;
-            a.cnt1[(uint64_t)c * F + s] = sm.delta[s];
+            a.cnt1[(uint64_t)c * F + s] = rows1[s];
         }
     }
     __syncthreads();
