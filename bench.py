@@ -48,9 +48,21 @@ WORKLOADS = {
     "rsm_c2": ("RSM", 27, 30, "fk", 100),
     "psm_c2": ("PSM", 27, 30, "fk", 100),
     "radix_c3_z1": ("RHO", 26, 29, "zipf", 1.0),
+    "plain_c3_z1": ("RHO", 26, 29, "zipf", 1.0, {"skew_split": 0}),
     "lrn_c3_z1": ("LRN", 26, 29, "zipf", 1.0),
+    "plain_c3_z15": ("RHO", 26, 29, "zipf", 1.5, {"skew_split": 0}),
+    "lrn_c3_z15": ("LRN", 26, 29, "zipf", 1.5),
     "rho_c1": ("RHO", 21, 21, "fk", 100),
+    # 2^28 / 2^31 Zipf z = 1.0, materialised (2^31 output rows, 25.8 GB)
+    "lrn_c5_mat": ("LRN", 28, 31, "zipf", 1.0, {"materialize": 1}),
+    "radix_c5_mat": ("RHO", 28, 31, "zipf", 1.0, {"materialize": 1}),
 }
+
+
+def wl_spec(wl):
+    """(algo, log2 |R|, log2 |S|, S kind, selectivity or z, config overrides)."""
+    w = WORKLOADS[wl]
+    return tuple(w[:5]) + (dict(w[5]) if len(w) > 5 else {},)
 
 
 # Batched workload (4096 joins): |R_i| = round(2^U), U ~ Uniform[lo, hi];
@@ -91,6 +103,23 @@ def make_batch_device(torch, tbg, njoins, lo, hi, zipf_frac, seed=4, stream=0):
             tbg.gen_fk(pS, int(nS[i]), int(nR[i]), 1001 + 2 * i + seed * 100003, stream)
         joins.append((pR, int(nR[i]), pS, int(nS[i])))
     return buf, joins, zipf
+
+
+def max_over_ranks(x, dist, device):
+    """The job's time: the largest of the ranks' device times (every rank
+    calls it with its own x; with one process it returns x)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mtuples(world, rows_per_rank, steps, seconds):
+    """Whole-job throughput under weak scaling: every rank joins its own
+    rows_per_rank input rows per step."""
+    return world * rows_per_rank * steps / seconds / 1e6
 
 
 def log(*a):
@@ -156,7 +185,7 @@ class ClockSampler:
 def host_workload(wl, nS_sample, seed=1):
     """Host copy of the workload for the CPU reference: R a permutation of
     1..|R|, S a bounded sample drawn like the GPU generator's S."""
-    algo, lr, ls, kind, param = WORKLOADS[wl]
+    algo, lr, ls, kind, param, _ = wl_spec(wl)
     nR = 1 << lr
     rng = np.random.default_rng(seed)
     R = np.zeros(nR, dtype=[("key", "<u4"), ("payload", "<u4")])
@@ -187,21 +216,24 @@ def cpu_reference_run(wl, nS_sample, steps, warmup, threads):
     import oracle as O
     if O.ref() is None:
         return None, "oracle/_ref/libtbref.so not built"
+    algo, _, _, _, _, over = wl_spec(wl)
+    mat = bool(over.get("materialize"))
+    if mat:  # the reference materialises one malloc'd node per row: keep the sample modest
+        nS_sample = min(nS_sample, 1 << 26)
     R, S = host_workload(wl, nS_sample)
-    algo = WORKLOADS[wl][0]
     ref_algo = algo if algo in ("RHO", "RHT", "RSM", "PSM") else "RHO"
     times = []
     counts = []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
-        c, _, rt_us = O.ref_join(ref_algo, R, S, nthreads=threads)
+        c, _, rt_us = O.ref_join(ref_algo, R, S, nthreads=threads, materialize=mat)
         wall = time.perf_counter() - t0
         if i >= warmup:
             times.append(rt_us * 1e-6 if rt_us and rt_us > 0 else wall)
             counts.append(c)
     t = statistics.median(times)
     return {"value": (len(R) + len(S)) / t / 1e6, "seconds_per_step": t, "count": counts[-1],
-            "nR": len(R), "nS": len(S), "algo": ref_algo}, None
+            "nR": len(R), "nS": len(S), "algo": ref_algo + ("_mat" if mat else "")}, None
 
 
 def host_threads():
@@ -236,13 +268,17 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload in BATCH_WORKLOADS:
         return batch_main(args, rank, world, local)
-    algo, lr, ls, kind, param = WORKLOADS[args.workload]
+    algo, lr, ls, kind, param, over = wl_spec(args.workload)
     lr = args.log2_r if args.log2_r is not None else lr
     ls = args.log2_s if args.log2_s is not None else ls
     nR, nS = 1 << lr, 1 << ls
+    mat = bool(over.get("materialize"))
     workload_name = f"{algo} |R|=2^{lr} |S|=2^{ls} " + (
-        f"uniform FK {param}% selectivity" if kind == "fk" else f"Zipf z={param}") + ", count only"
-    metric = "input Mtuples/s (|R|+|S|)/t, count-only equi-join, bit-exact"
+        f"uniform FK {param}% selectivity" if kind == "fk" else f"Zipf z={param}") + (
+        ", materialised (key, R payload, S payload) rows" if mat else ", count only") + (
+        "".join(f", {k}={v}" for k, v in over.items() if k != "materialize"))
+    metric = ("input Mtuples/s (|R|+|S|)/t, " + ("materialising" if mat else "count-only") +
+              " equi-join, bit-exact")
 
     if args.impl == "reference":
         if rank != 0:
@@ -291,14 +327,19 @@ def main():
             tbg.gen_zipf(pS, nS, nR, float(param), 0, 22222 + rank, sh)
     stream.synchronize()
 
-    cfg = tbg.config(algo)
+    cfg = tbg.config(algo, **over)
     cfg.timing = 1
     expect = None
     if kind == "fk" or kind == "zipf":
         expect = nS * nR // (nR * 100 // int(param)) if kind == "fk" else nS
+    pO, cap = 0, 0
+    if mat:  # every S key is one of R's unique keys: exactly |S| output rows
+        cap = nS
+        tO = torch.empty(3 * cap, dtype=torch.int32, device=dev)
+        pO = tO.data_ptr()
     # warm-up
     for _ in range(args.warmup):
-        _, m, st = tbg.join_device(cfg, pR, nR, pS, nS, stream=sh)
+        _, m, st = tbg.join_device(cfg, pR, nR, pS, nS, pO, cap, stream=sh)
     if expect is not None and m != expect:
         raise SystemExit(f"wrong match count {m} != {expect}")
 
@@ -313,23 +354,52 @@ def main():
     with ClockSampler(local) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
-            _, m, st = tbg.join_device(cfg, pR, nR, pS, nS, stream=sh)
+            _, m, st = tbg.join_device(cfg, pR, nR, pS, nS, pO, cap, stream=sh)
             for k in phase:
                 phase[k] += getattr(st, k)
         ev1.record(stream)
         torch.cuda.synchronize()
     launches = tbg.kernel_launches() - l0
     ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, dist, dev)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * (nR + nS) * args.steps / (ms / 1e3) / 1e6
+    value = job_mtuples(world, nR + nS, args.steps, ms / 1e3)
 
     # e2e through the drop-in entry point with pinned host buffers
     e2e = None
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and mat:
+        # the drop-in would build 2^31 list nodes on the host; the device API
+        # with every step's inputs copied in and its rows copied out stands in
+        hR = torch.empty(nR, dtype=torch.int64, pin_memory=True)
+        hS = torch.empty(nS, dtype=torch.int64, pin_memory=True)
+        hO = torch.empty(3 * cap, dtype=torch.int32, pin_memory=True)
+        hR.copy_(tR)
+        hS.copy_(tS)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            with torch.cuda.stream(stream):
+                tR.copy_(hR, non_blocking=True)
+                tS.copy_(hS, non_blocking=True)
+            _, cnt, _ = tbg.join_device(cfg, pR, nR, pS, nS, pO, cap, stream=sh)
+            with torch.cuda.stream(stream):
+                hO[: 3 * cnt].copy_(tO[: 3 * cnt], non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        el = e0.elapsed_time(e1) / 1e3
+        el = max_over_ranks(el, dist, dev)
+        e2e = {"value": job_mtuples(world, nR + nS, args.e2e_steps, el), "unit": "Mtuples/s",
+               "h2d_bytes_per_step": (nR + nS) * 8, "d2h_bytes_per_step": int(cnt) * 12,
+               "api": "tbg_join_device(materialize) with R, S copied from and the rows copied to pinned host "
+                      "memory each step",
+               "count": int(cnt)}
+        del hR, hS, hO
+    elif args.e2e_steps > 0:
         hR = torch.empty(nR, dtype=torch.int64, pin_memory=True)
         hS = torch.empty(nS, dtype=torch.int64, pin_memory=True)
         hR.copy_(tR)
@@ -349,13 +419,9 @@ def main():
             res = fn(C.byref(tabR), C.byref(tabS), 1)
             cnt = res.contents.totalresults
             tbg.lib().tbg_result_free(res)
-        el = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([el], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(time.perf_counter() - t0, dist, dev)
         h2d, d2h = tbg.last_transfer_bytes()
-        e2e = {"value": world * (nR + nS) * args.e2e_steps / el / 1e6, "unit": "Mtuples/s",
+        e2e = {"value": job_mtuples(world, nR + nS, args.e2e_steps, el), "unit": "Mtuples/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "api": f"{algo}(table_t*, table_t*, int) drop-in, pinned host buffers",
                "count": int(cnt)}
@@ -366,19 +432,55 @@ def main():
     rows = nR + nS
     K = args.steps
     passes = st.passes or 2
-    scat_ms = (phase["ms_pass1"] + phase["ms_pass2"]) / K
-    scat_bytes = 16 * rows * passes
-    achieved = scat_bytes / (scat_ms / 1e3) / 1e9 if scat_ms > 0 else None
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            tt = json.load(f)
-        k = tt.get("k_part_pass")
-        if k:  # DRAM bytes per row moved, from one ncu capture; per launch like `achieved`
-            traffic = k["dram_bytes_per_row"] * rows * passes
-    total_bytes = (8 + 16 * passes + 8) * rows
     pipe_ms = ms / K
+    peak_source = (f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                   else "fallback 6650 GB/s")
+    if algo in ("RHO", "RHT") and not mat:
+        scat_ms = (phase["ms_pass1"] + phase["ms_pass2"]) / K
+        scat_bytes = 16 * rows * passes
+        achieved = scat_bytes / (scat_ms / 1e3) / 1e9 if scat_ms > 0 else None
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as f:
+                tt = json.load(f)
+            k = tt.get("k_part_pass")
+            if k:  # DRAM bytes per row moved, from one ncu capture; per launch like `achieved`
+                traffic = k["dram_bytes_per_row"] * rows * passes
+        total_bytes = (8 + 16 * passes + 8) * rows
+        roofline = {"bound": "hbm",
+                    "kernel": f"k_part_pass1 + k_part_pass2 ({passes} partitioning passes over R and S, "
+                              f"{2 * passes} launches per join)",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak if achieved else None, "traffic": traffic,
+                    "peak_source": peak_source,
+                    "algorithmic_bytes_per_row_per_pass": 16,
+                    "timing": "library CUDA events on the join stream around each pass, summed over "
+                              "the timed steps",
+                    "pipeline": {"bytes_per_row": 8 + 16 * passes + 8,
+                                 "achieved_gbs": total_bytes / (pipe_ms / 1e3) / 1e9,
+                                 "frac": total_bytes / (pipe_ms / 1e3) / 1e9 / peak}}
+    else:
+        # whole join: LRN's learning and bypass run on two streams and PSM's
+        # sort passes are not radix passes, so the pipeline is the unit
+        if algo == "PSM":
+            alg = 8 * rows + 16 * 4 * rows + 8 * rows  # digit histogram, 4 LSD passes, merge
+            model = "PSM: digit histogram 8 + 4 LSD passes x 16 + merge read 8 B/row"
+        else:
+            heavy = int(st.heavy_rows_S) if algo == "LRN" else 0
+            part_rows = rows - heavy
+            alg = 8 * rows + (16 * passes + 8) * part_rows
+            model = (f"histogram read 8 B/row of R and S; {passes} passes x 16 + build/probe 8 B/row of the "
+                     f"rows that are partitioned ({part_rows}" + (f", {heavy} heavy S rows joined in the "
+                                                                   f"histogram read" if heavy else "") + ")")
+        if mat:
+            alg += 12 * int(m)
+            model += "; 12 B per output row"
+        achieved = alg / (pipe_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": f"all kernels of one {algo} join (pipeline)",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "peak_source": peak_source, "algorithmic_bytes_per_join": alg,
+                    "bytes_model": model, "timing": "CUDA events around the timed joins on their stream"}
     line = {
         "metric": metric, "value": value, "unit": "Mtuples/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": pipe_ms, "higher_is_better": True,
@@ -390,19 +492,10 @@ def main():
                    "generator": "on-GPU pk / fk / zipf (generator.cpp semantics)"},
         "gpu_launches": int(launches),
         "e2e": e2e,
-        "roofline": {"bound": "hbm",
-                     "kernel": f"k_part_pass1 + k_part_pass2 ({passes} partitioning passes over R and S, "
-                               f"{2 * passes} launches per join)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None, "traffic": traffic,
-                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                     else "fallback 6650 GB/s",
-                     "algorithmic_bytes_per_row_per_pass": 16,
-                     "timing": "library CUDA events on the join stream around each pass, summed over "
-                               "the timed steps",
-                     "pipeline": {"bytes_per_row": 8 + 16 * passes + 8,
-                                  "achieved_gbs": total_bytes / (pipe_ms / 1e3) / 1e9,
-                                  "frac": total_bytes / (pipe_ms / 1e3) / 1e9 / peak}},
+        "roofline": roofline,
+        "stats": {"used_fallback": st.used_fallback, "heavy_keys": st.heavy_keys,
+                  "heavy_rows_S": st.heavy_rows_S, "imbalance": st.imbalance,
+                  "max_part_S": st.max_part_S},
         "phases_ms": {k: v / K for k, v in phase.items()},
         "clocks": clocks.summary(),
         "matches": int(m),
@@ -549,12 +642,9 @@ def batch_main(args, rank, world, local):
     b.sync()
     launches = tbg.kernel_launches() - l0
     ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     K = args.steps
-    value = world * rows * K / (ms / 1e3) / 1e6
+    value = job_mtuples(world, rows, K, ms / 1e3)
     peak, peak_kind = read_peaks()
     alg = batch_algorithmic_bytes(dj, desc)
     achieved = alg / (ms / K / 1e3) / 1e9
@@ -586,13 +676,10 @@ def batch_main(args, rank, world, local):
         e1.record(stream)
         torch.cuda.synchronize()
         el = e0.elapsed_time(e1) / 1e3
-        if world > 1:
-            t = torch.tensor([el], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(el, dist, dev)
         if hcounts.tolist() != want:
             raise SystemExit("wrong per-join counts (e2e)")
-        e2e = {"value": world * rows * args.e2e_steps / el / 1e6, "unit": "Mtuples/s",
+        e2e = {"value": job_mtuples(world, rows, args.e2e_steps, el), "unit": "Mtuples/s",
                "h2d_bytes_per_step": int(buf.numel() * 8), "d2h_bytes_per_step": int(nj * 8),
                "api": "tbg_batch_run with every join's R_i, S_i copied from pinned host memory each step"}
         del host

@@ -143,6 +143,18 @@ void mark(Workspace &w, bool timing, int i, cudaStream_t st) {
 
 // Geometry of the chunked radix partitioning of R and S into 2^B final
 // partitions (shared by RHO, RHT, RSM and LRN).
+// R rows per shared-memory join table: JOIN_CAPR_DEFAULT (three CTAs per SM)
+// while R's partitions at the largest radix (15 bits) fit it, else the next
+// power of two, up to 16384 (one CTA per SM), so a partition of R is built
+// once and S is not probed twice.
+int join_capacity(uint64_t nR) {
+    const uint64_t per = (nR + (1u << 15) - 1) >> 15;
+    if (per <= (uint64_t)JOIN_CAPR_DEFAULT) return JOIN_CAPR_DEFAULT;
+    uint64_t c = 8192;
+    while (c < per && c < 16384) c <<= 1;
+    return (int)c;
+}
+
 RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int capR, Workspace &w) {
     RadixGeom g;
     choose_radix(cfg, nR, capR, &g.B, &g.passes);
@@ -157,7 +169,9 @@ RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int ca
         g.capS = nS / ((uint64_t)g.join_grid * 4);
         if (g.capS < 65536) g.capS = 65536;
     }
-    g.item_cap = nR / capR + (g.capS ? nS / g.capS : 0) + 2 * g.P + 16;
+    // room for every R chunk of a partition to split its S side (k_plan
+    // keeps oversized S sides whole if a skewed input still overflows this)
+    g.item_cap = 2 * (nR / capR + (g.capS ? nS / g.capS : 0) + 2 * g.P) + 16;
     // four chunks per SM (two resident partitioning CTAs each), >= 32K rows each
     auto chunks = [&](uint64_t n) {
         uint64_t c = std::min<uint64_t>((uint64_t)w.nsm * 4, (n + 32767) / 32768);
@@ -339,7 +353,7 @@ int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row
 int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                    tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
                    JoinRun *run) {
-    const int capR = JOIN_CAPR_DEFAULT;
+    const int capR = join_capacity(nR);
     int join_grid = 0;
     int rc = radix_partition(cfg, dR, nR, dS, nS, capR, w, st, run, &join_grid);
     if (rc) return rc;

@@ -59,7 +59,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     m = std::max<uint64_t>(m, 65536);
     m = std::min<uint64_t>(m, nS);
     const uint64_t tiles = (m + SCATTER_TILE - 1) / SCATTER_TILE + 1;
-    const int capR = JOIN_CAPR_DEFAULT;
+    const int capR = join_capacity(nR);
     const RadixGeom g = radix_geometry(cfg, nR, nS, capR, w);
     run->B = g.B;
     run->passes = g.passes;

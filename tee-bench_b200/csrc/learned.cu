@@ -485,7 +485,6 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     uint32_t *filt = hist + a.nbins;              // 2^FILTER_LOG2 bits
     uint32_t *hkeys = filt + (1 << FILTER_LOG2) / 32;
     unsigned *hcnt = hkeys + HEAVY_CAP;
-    unsigned *hstart = hcnt + HEAVY_CAP;  // MAT only
     __shared__ unsigned s_keep;
     __shared__ unsigned long long s_base;
     __shared__ uint64_t scan_scratch[1024 / 32 + 1];
@@ -495,7 +494,6 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     for (int i = tid; i < HEAVY_CAP; i += 1024) {
         hkeys[i] = a.hkeys[i];
         hcnt[i] = a.hcnt[i];
-        if (MAT) hstart[i] = a.hstart[i];
     }
     if (tid == 0) s_keep = 0;
     __syncthreads();
@@ -567,7 +565,8 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 if (slot[j] >= 0) {
-                    const unsigned st0 = hstart[slot[j]], c = hcnt[slot[j]];
+                    // R-row starts stay in global memory: only heavy rows read them
+                    const unsigned st0 = a.hstart[slot[j]], c = hcnt[slot[j]];
                     for (unsigned q = 0; q < c; q++, op++)
                         if (op < a.cap) a.rows[op] = tbg_row_out{k[j], a.rpay[st0 + q], v[j]};
                 }
@@ -586,7 +585,8 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
 }
 
 size_t bypass_smem(int nbins, bool mat) {
-    return (size_t)nbins * 4 + (1 << FILTER_LOG2) / 8 + (size_t)HEAVY_CAP * 4 * (mat ? 3 : 2);
+    (void)mat;  // 2^15 bins + filter + keys + counts: 204,800 B at most
+    return (size_t)nbins * 4 + (1 << FILTER_LOG2) / 8 + (size_t)HEAVY_CAP * 4 * 2;
 }
 
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st) {

@@ -190,18 +190,30 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan_bases(const uint32_t *tot
 // the item list is grouped by thread, not sorted by partition.
 __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
     __shared__ uint64_t scratch[PLAN_THREADS / 32 + 1];
+    __shared__ int s_split;
     const int P = 1 << a.P_log2;
-    uint64_t cnt = 0, nonempty = 0;
+    // S sides larger than capS are split (skew) for every R chunk of the
+    // partition; if that would overflow the item buffer, partitions whose R
+    // side needs several chunks keep S whole
+    auto s_chunks = [&](uint32_t hs, uint64_t nrc, bool split_all) -> uint64_t {
+        if (!a.capS || (nrc > 1 && !split_all)) return 1;
+        return (hs + a.capS - 1) / a.capS;
+    };
+    uint64_t cnt_all = 0, cnt_one = 0, nonempty = 0;
     for (int f = threadIdx.x; f < P; f += PLAN_THREADS) {
         const uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
         if (hr == 0 || hs == 0) continue;
         const uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
-        const uint64_t nsc = (nrc == 1 && a.capS) ? (hs + a.capS - 1) / a.capS : 1;
-        cnt += nrc * nsc;
+        cnt_all += nrc * s_chunks(hs, nrc, true);
+        cnt_one += nrc * s_chunks(hs, nrc, false);
         nonempty++;
     }
-    uint64_t total;
-    uint64_t off = block_excl_scan<PLAN_THREADS>(cnt, &total, scratch);
+    uint64_t total_all, total;
+    block_excl_scan<PLAN_THREADS>(cnt_all, &total_all, scratch);
+    if (threadIdx.x == 0) s_split = total_all <= a.item_cap;
+    __syncthreads();
+    const bool split_all = s_split != 0;
+    uint64_t off = block_excl_scan<PLAN_THREADS>(split_all ? cnt_all : cnt_one, &total, scratch);
     if (total > a.item_cap) {  // cannot happen with the host's bound; guard anyway
         if (threadIdx.x == 0) {
             atomicCAS(&a.ctrl->error, 0u, (unsigned)TBG_ERR_CAPACITY);
@@ -213,7 +225,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
         const uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
         if (hr == 0 || hs == 0) continue;
         const uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
-        const uint64_t nsc = (nrc == 1 && a.capS) ? (hs + a.capS - 1) / a.capS : 1;
+        const uint64_t nsc = s_chunks(hs, nrc, split_all);
         const uint64_t sstep = (hs + nsc - 1) / nsc;
         const uint64_t rb = a.r.base[f], sb = a.s.base[f];
         for (uint64_t rc = 0; rc < nrc; rc++) {

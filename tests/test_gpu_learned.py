@@ -98,6 +98,32 @@ def test_lrn_duplicate_R_keys_on_heavy_path(tbg, oracle, cuda):
     assert m == ref and np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
 
 
+def test_lrn_materialise_at_fifteen_bits(tbg, oracle, cuda):
+    """15 radix bits with materialisation: the bypass histogram's shared
+    memory (2^15 bins, filter, heavy keys and counts) must fit one block."""
+    R = gen_relation(oracle, ("pk", 1 << 20, 0, 0.0), 31, 0)
+    S = gen_relation(oracle, ("zipf", 1 << 22, 1 << 20, 1.0), 32, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    m, rows, st = run_join(tbg, cuda, "LRN", R, S, materialize=True, cap=ref, radix_bits=15, passes=2)
+    assert st.radix_bits == 15 and st.used_fallback == 0 and st.heavy_rows_S > 0
+    assert m == ref and np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+
+
+def test_skew_split_with_several_R_chunks(tbg, oracle, cuda):
+    """R partitions larger than one shared-memory table (duplicate R keys,
+    few radix bits) with a hot S side: every R chunk probes every S slice."""
+    rng = np.random.default_rng(41)
+    R = np.zeros(60000, dtype=oracle.ROW)
+    R["key"] = rng.integers(1, 4000, len(R))
+    oracle.fill_payloads(R, 0)
+    S = gen_relation(oracle, ("zipf", 1 << 20, 4000, 1.2), 42, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    for algo in ("RHO", "RHT"):
+        m, rows, st = run_join(tbg, cuda, algo, R, S, materialize=True, cap=ref, radix_bits=2, passes=1)
+        assert st.max_part_R > 8192 and st.work_items > 4
+        assert m == ref and np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows)), algo
+
+
 def test_lrn_dropin(tbg, oracle, cuda):
     R = gen_relation(oracle, ("pk", 1 << 16, 0, 0.0), 11111, 0)
     S = gen_relation(oracle, ("zipf", 1 << 19, 1 << 16, 1.0), 22222, 1)
