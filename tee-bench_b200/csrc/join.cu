@@ -8,9 +8,10 @@
 //             over max(next_pow2(|R_p|)/4, 4) slots, prefix sum, R_p reordered
 //             by bucket, probe scans the bucket's range.
 // Counting uses per-thread counters folded once per CTA; materialisation
-// reserves output rows once per CTA round with a block scan, so one global
-// atomic covers up to JOIN_THREADS * 8 probe rows (the reference's
-// insert_output, Include/util.c:20-29, mallocs one node per row).
+// reserves output rows once per CTA round (one global atomic for up to
+// JOIN_THREADS * 8 probe rows) and places them in (row slot, lane) order, so
+// consecutive lanes store consecutive rows (the reference's insert_output,
+// Include/util.c:20-29, mallocs one node per row).
 #include "join_dev.cuh"
 
 namespace tbg {
@@ -19,7 +20,6 @@ template <bool MAT>
 __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t s_item;
-    __shared__ unsigned long long s_base;
     __shared__ uint64_t scan_scratch[JOIN_THREADS / 32 + 1];
     Table t;
     t.key = reinterpret_cast<uint32_t *>(smem);
@@ -74,31 +74,32 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
                         }
                     }
                 }
-                uint32_t c = 0;
-#pragma unroll
-                for (int j = 0; j < 8; j++)
-                    if (valid >> j & 1) c += t.count(k[j]);
-                uint64_t tot;
-                uint64_t off = block_excl_scan<JOIN_THREADS>(c, &tot, scan_scratch);
-                if (tid == 0) s_base = tot ? atomicAdd(a.rows_ctr, (unsigned long long)tot) : 0;
-                __syncthreads();
-                uint64_t pos = s_base + off;
+                uint32_t c[8];
+                uint32_t csum = 0;
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
-                    if (valid >> j & 1) {
+                    c[j] = (valid >> j & 1) ? t.count(k[j]) : 0;
+                    csum += c[j];
+                }
+                uint64_t pos[8];
+                block_emit_positions<JOIN_THREADS, 8>(c, pos, a.rows_ctr, scan_scratch);
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    if (c[j]) {
                         const uint32_t kk = k[j], pp = p[j];
+                        uint64_t q = pos[j];
                         t.for_each(kk, [&](uint32_t rp) {
-                            if (pos < a.cap) {
+                            if (q < a.cap) {
                                 tbg_row_out o;
                                 o.key = kk; o.Rpayload = rp; o.Spayload = pp;
-                                a.out[pos] = o;
+                                a.out[q] = o;
                             }
-                            pos++;
+                            q++;
                         });
                     }
                 }
-                local += c;
-                __syncthreads();
+                const uint32_t c_total = csum;
+                local += c_total;
             }
         }
         __syncthreads();  // table reused by the next item

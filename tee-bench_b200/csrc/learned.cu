@@ -486,7 +486,6 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     uint32_t *hkeys = filt + (1 << FILTER_LOG2) / 32;
     unsigned *hcnt = hkeys + HEAVY_CAP;
     __shared__ unsigned s_keep;
-    __shared__ unsigned long long s_base;
     __shared__ uint64_t scan_scratch[1024 / 32 + 1];
     const int tid = threadIdx.x, lane = tid & 31;
     for (int i = tid; i < a.nbins; i += 1024) hist[i] = 0;
@@ -557,17 +556,19 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
             wb += __popc(m[j]);
         }
         if (MAT) {
-            uint64_t tot;
-            const uint64_t off = block_excl_scan<1024>(emit, &tot, scan_scratch);
-            if (tid == 0) s_base = tot ? atomicAdd(a.rows_ctr, (unsigned long long)tot) : 0;
-            __syncthreads();
-            uint64_t op = s_base + off;
+            // heavy rows' output in (row slot, lane) order: coalesced stores
+            uint32_t c[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) c[j] = slot[j] >= 0 ? hcnt[slot[j]] : 0;
+            uint64_t pos[8];
+            block_emit_positions<1024, 8>(c, pos, a.rows_ctr, scan_scratch);
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                if (slot[j] >= 0) {
+                if (c[j]) {
                     // R-row starts stay in global memory: only heavy rows read them
-                    const unsigned st0 = a.hstart[slot[j]], c = hcnt[slot[j]];
-                    for (unsigned q = 0; q < c; q++, op++)
+                    const unsigned st0 = a.hstart[slot[j]];
+                    uint64_t op = pos[j];
+                    for (unsigned q = 0; q < c[j]; q++, op++)
                         if (op < a.cap) a.rows[op] = tbg_row_out{k[j], a.rpay[st0 + q], v[j]};
                 }
             }

@@ -38,6 +38,53 @@ __device__ __forceinline__ unsigned warp_max_u32(unsigned v) {
     for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
+// Output rows of one block round, NJ row slots per thread: thread t emits
+// c[j] rows for slot j.  Positions follow (slot j, warp, lane) order within
+// a warp's share, so when each row has at most one match consecutive lanes
+// write consecutive rows (coalesced stores).  One atomicAdd on *rows_ctr
+// reserves the whole block's rows.  `scratch` holds THREADS / 32 + 1 words;
+// every thread of the block must call it; it ends with a barrier.
+template <int THREADS, int NJ>
+__device__ __forceinline__ void block_emit_positions(const uint32_t (&c)[NJ], uint64_t (&pos)[NJ],
+                                                     unsigned long long *rows_ctr, uint64_t *scratch) {
+    constexpr int NW = THREADS / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t wpre[NJ];
+    uint32_t wtot = 0;
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+        uint32_t inc = c[j];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        wpre[j] = wtot + inc - c[j];
+        wtot += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0) scratch[w] = wtot;
+    __syncthreads();
+    if (w == 0) {
+        const uint64_t mine = lane < NW ? scratch[lane] : 0;
+        uint64_t inc = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const uint64_t total = __shfl_sync(0xffffffffu, inc, 31);
+        uint64_t base = 0;
+        if (lane == 0 && total) base = atomicAdd(rows_ctr, (unsigned long long)total);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (lane < NW) scratch[lane] = base + inc - mine;
+    }
+    __syncthreads();
+    const uint64_t wbase = scratch[w];
+#pragma unroll
+    for (int j = 0; j < NJ; j++) pos[j] = wbase + wpre[j];
+    __syncthreads();  // scratch is reused by the next round
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
