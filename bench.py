@@ -141,32 +141,39 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, interval_ms=50):
         self.idx = gpu_index
+        self.interval_ms = interval_ms
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._th = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            line = line.strip()
+            if line:
+                self.samples.append([x.strip() for x in line.split(",")])
 
     def __enter__(self):
-        self._th = threading.Thread(target=self._run, daemon=True)
-        self._th.start()
+        # one nvidia-smi child streaming a line every interval_ms
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", str(self.interval_ms)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._th = threading.Thread(target=self._read, daemon=True)
+            self._th.start()
+        except OSError:
+            self._proc = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._th.join(timeout=10)
+        if self._proc is not None:
+            self._proc.terminate()  # our own child, by its handle
+            try:
+                self._proc.wait(timeout=10)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+            self._th.join(timeout=10)
 
     def summary(self):
         if not self.samples:
@@ -247,7 +254,7 @@ def host_threads():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rho_c2", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))

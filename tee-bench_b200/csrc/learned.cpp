@@ -176,21 +176,14 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         if ((e = launch_heavy_build(cand, ncand, tau, hkeys, hfilter, &lc->inserted, s2)) != cudaSuccess)
             return cuda_error(e, "heavy build");
         uint32_t *rpay = nullptr;
-        if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, false, w.nsm, s2)) !=
+        if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, s2)) !=
             cudaSuccess)
             return cuda_error(e, "heavy R");
-        if (mat) {  // heavy R payload lists, sized exactly
-            std::vector<unsigned> cnts(HEAVY_CAP);
-            if ((e = cudaMemcpyAsync(cnts.data(), hcnt, HEAVY_CAP * 4, cudaMemcpyDeviceToHost, s2)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(s2)) != cudaSuccess)
-                return cuda_error(e, "heavy R");
-            uint64_t total = 0;
-            for (unsigned c : cnts) total += c;
-            if ((e = w.misc.ensure(std::max<uint64_t>(total, 1) * 4 + 64)) != cudaSuccess)
+        if (mat) {  // heavy R payload lists: at most |R| entries, so no count read-back
+            if ((e = w.misc.ensure(std::max<uint64_t>(nR, 1) * 4 + 64)) != cudaSuccess)
                 return cuda_error(e, "cudaMalloc");
             rpay = w.misc.as<uint32_t>();
-            if ((e = cudaMemsetAsync(hcnt, 0, HEAVY_CAP * 4, s2)) != cudaSuccess) return cuda_error(e, "memset");
-            if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, hstart, hcur, rpay, true, w.nsm, s2)) != cudaSuccess)
+            if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, hstart, hcur, rpay, 1, w.nsm, s2)) != cudaSuccess)
                 return cuda_error(e, "heavy R");
         }
         if ((e = cudaMemcpyAsync(&ctrl->heavy_keys, &lc->inserted, 4, cudaMemcpyDeviceToDevice, s2)) != cudaSuccess)

@@ -422,14 +422,28 @@ __global__ void __launch_bounds__(512) k_heavy_r(const Row *__restrict__ R, uint
     }
     for (int i = threadIdx.x; i < (1 << FILTER_LOG2) / 32; i += 512) filt[i] = gfilter[i];
     __syncthreads();
-    for (uint64_t i = (uint64_t)blockIdx.x * 512 + threadIdx.x; i < n; i += (uint64_t)gridDim.x * 512) {
-        const Row x = R[i];
-        const uint32_t fb = filter_bit(x.key);
-        if (!(filt[fb >> 5] >> (fb & 31) & 1)) continue;
-        const int s = heavy_find(keys, x.key);
-        if (s < 0) continue;
-        if (PASS == 0) atomicAdd(&cnt[s], 1u);
-        else rpay[start[s] + atomicAdd(&cur[s], 1u)] = x.payload;
+    // four rows in flight per thread
+    const uint64_t stride = (uint64_t)gridDim.x * 512;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * 512 + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        Row x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint64_t i = i0 + u * stride;
+            if (i < n) {
+                const uint2 v = ldg_stream(reinterpret_cast<const uint2 *>(R) + i);
+                x[u] = Row{v.x, v.y};
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (i0 + u * stride >= n) continue;
+            const uint32_t fb = filter_bit(x[u].key);
+            if (!(filt[fb >> 5] >> (fb & 31) & 1)) continue;
+            const int s = heavy_find(keys, x[u].key);
+            if (s < 0) continue;
+            if (PASS == 0) atomicAdd(&cnt[s], 1u);
+            else rpay[start[s] + atomicAdd(&cur[s], 1u)] = x[u].payload;
+        }
     }
     if (PASS == 0) {
         __syncthreads();
@@ -454,17 +468,20 @@ __global__ void k_heavy_prefix(const unsigned *cnt, unsigned *start, unsigned *c
     }
 }
 
+// stage 0: per-slot counts of R's heavy rows; stage 1 (materialisation):
+// prefix of the counts, then every heavy row's payload into rpay.
 cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const uint32_t *filter, unsigned *cnt,
-                           unsigned *start, unsigned *cur, uint32_t *rpay, bool materialize, int nsm, cudaStream_t st) {
+                           unsigned *start, unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st) {
     if (!n) return cudaSuccess;
     const unsigned g = (unsigned)umin64((n + 511) / 512, (uint64_t)nsm * 4);
     const size_t smem = (size_t)HEAVY_CAP * 8 + (1 << FILTER_LOG2) / 8;
     cudaError_t e = cudaFuncSetAttribute(k_heavy_r<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_heavy_r<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_heavy_r<0><<<g, 512, smem, st>>>(R, n, keys, filter, cnt, nullptr, nullptr, nullptr);
-    count_launch();
-    if (materialize) {
+    if (stage == 0) {
+        k_heavy_r<0><<<g, 512, smem, st>>>(R, n, keys, filter, cnt, nullptr, nullptr, nullptr);
+        count_launch();
+    } else {
         k_heavy_prefix<<<1, 1024, 0, st>>>(cnt, start, cur);
         k_heavy_r<1><<<g, 512, smem, st>>>(R, n, keys, filter, cnt, start, cur, rpay);
         count_launch(2);

@@ -77,7 +77,7 @@ cudaError_t launch_heavy_score(HeavyCand *cand, unsigned ncand, const float *par
 cudaError_t launch_heavy_build(const HeavyCand *cand, unsigned ncand, float tau, uint32_t *keys, uint32_t *filter,
                                unsigned *inserted, cudaStream_t st);
 cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const uint32_t *filter, unsigned *cnt,
-                           unsigned *start, unsigned *cur, uint32_t *rpay, bool materialize, int nsm, cudaStream_t st);
+                           unsigned *start, unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st);
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st);
 size_t bypass_smem(int nbins, bool mat);
 
