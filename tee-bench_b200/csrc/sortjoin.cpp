@@ -21,7 +21,6 @@ cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t 
 uint64_t merge_ctas(uint64_t nr, uint64_t ns);
 
 constexpr int RSM_CAPR = 4096;
-static_assert((RSM_CAPR & (RSM_CAPR - 1)) == 0, "RSM_CAPR must be a power of two");
 
 static void mark_ev(Workspace &w, bool timing, int i, cudaStream_t st) {
     if (timing) cudaEventRecord(w.ev[i], st);
@@ -29,7 +28,7 @@ static void mark_ev(Workspace &w, bool timing, int i, cudaStream_t st) {
 
 int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                        tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run) {
-    // a power of two: the shared-memory sort pads R_p to next_pow2(|R_p|) <= capR
+    // one shared-memory radix-sorted tile (512 threads x 8 rows) of R per item
     const int capR = RSM_CAPR;
     int join_grid = 0;
     int rc = radix_partition(cfg, dR, nR, dS, nS, capR, w, st, run, &join_grid);

@@ -1,8 +1,9 @@
 // Sort-merge joins for sm_100a.
 //
 // RSM (Joins/radix_sortmerge_join.c:74-100): the radix partitions of RHO,
-// then per partition pair both sides are sorted in shared memory (bitonic
-// network on packed (key, payload) words) and merged.  PSM
+// then per partition pair both sides are sorted in shared memory (a stable
+// LSD radix sort of packed (key, payload) words over the key bits that vary
+// inside the tile) and merged.  PSM
 // (Joins/psm/parallel_sortmerge_join.h:61-111): R and S are sorted globally
 // (LSD radix sort with the one-sweep scatter of sweep.cu) and merged.
 //
@@ -14,6 +15,8 @@
 // (Joins/radix_sortmerge_join.c:40-71, parallel_sortmerge_join.h:18-51) has
 // unbounded inner loops and a stale S cursor that miscount duplicates and
 // misses; this merge counts exactly the equi-join.
+#include <algorithm>
+
 #include "tbg_device.cuh"
 
 namespace tbg {
@@ -22,42 +25,104 @@ __device__ __forceinline__ uint64_t pack_row(uint32_t k, uint32_t p) { return ((
 __device__ __forceinline__ uint32_t row_key(uint64_t x) { return (uint32_t)(x >> 32); }
 __device__ __forceinline__ uint32_t row_pay(uint64_t x) { return (uint32_t)x; }
 
-// Bitonic sort of s[0..N) (N a power of two) by the packed value.
+// Block-wide stable LSD radix sort of n <= THREADS * 8 packed rows by key
+// (their high 32 bits) in shared memory.  Only the key bits that differ
+// inside the tile are sorted, 8 per pass.  In a pass, thread (w, lane) holds
+// rows e = w * 256 + i * 32 + lane (i < 8); a row's rank counts the rows of
+// the same digit before it in that order (per-warp counters advanced slot by
+// slot, __match_any_sync inside a slot), so every pass is stable.  `a` holds
+// the rows, `b` is scratch for n rows, `cnt` 256 * THREADS / 32 counters,
+// `scratch` THREADS / 32 + 1 words, `red` 2 words.  Returns the buffer that
+// holds the sorted rows (a or b).
 template <int THREADS>
-__device__ void bitonic_sort(uint64_t *s, uint32_t N) {
-    for (uint32_t k = 2; k <= N; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < N / 2; i += THREADS) {
-                const uint32_t lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
-                const uint32_t hi = lo | j;
-                const bool asc = (lo & k) == 0;
-                const uint64_t a = s[lo], b = s[hi];
-                if ((a > b) == asc) {
-                    s[lo] = b;
-                    s[hi] = a;
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-// Loads rows [off, off + n) into s[0..N) packed, pads with the maximum
-// value, and sorts.  N = next power of two >= n.
-template <int THREADS>
-__device__ uint32_t load_sorted(const Row *__restrict__ src, uint64_t off, uint32_t n, uint64_t *s) {
-    const uint32_t N = next_pow2(n < 2 ? 2 : n);
-    for (uint32_t i = threadIdx.x; i < N; i += THREADS) {
-        uint64_t v = ~0ull;
-        if (i < n) {
-            const uint2 x = reinterpret_cast<const uint2 *>(src)[off + i];
-            v = pack_row(x.x, x.y);
-        }
-        s[i] = v;
+__device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint16_t *cnt, uint64_t *scratch,
+                                      uint32_t *red) {
+    constexpr int NW = THREADS / 32, ITEMS = 8, C = 256 * NW / THREADS;
+    static_assert(THREADS * ITEMS <= 65535 && 256 * NW % THREADS == 0, "16-bit counters, even split");
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid == 0) {
+        red[0] = 0;
+        red[1] = ~0u;
     }
     __syncthreads();
-    bitonic_sort<THREADS>(s, N);
-    return N;
+    uint32_t vor = 0, vand = ~0u;
+    for (uint32_t e = tid; e < n; e += THREADS) {
+        const uint32_t k = row_key(a[e]);
+        vor |= k;
+        vand &= k;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        vor |= __shfl_xor_sync(0xffffffffu, vor, o);
+        vand &= __shfl_xor_sync(0xffffffffu, vand, o);
+    }
+    if (lane == 0) {
+        atomicOr(&red[0], vor);
+        atomicAnd(&red[1], vand);
+    }
+    __syncthreads();
+    const uint32_t varying = red[0] & ~red[1];
+    __syncthreads();  // red is reused by the next call
+    uint64_t *src = a, *dst = b;
+    if (!varying) return src;  // every key equal: already sorted
+    const int lo = __ffs(varying) - 1, hi = 31 - __clz(varying);
+    for (int shift = lo; shift <= hi; shift += 8) {
+        for (int i = tid; i < 256 * NW; i += THREADS) cnt[i] = 0;
+        __syncthreads();
+        uint64_t x[ITEMS];
+        uint32_t r[ITEMS], dg[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t e = (uint32_t)w * 32 * ITEMS + i * 32 + lane;
+            const bool valid = e < n;
+            x[i] = valid ? src[e] : 0;
+            const uint32_t d = valid ? (row_key(x[i]) >> shift) & 255 : 256;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            uint32_t base = 0;
+            if (valid) base = cnt[d * NW + w];
+            __syncwarp();
+            if (valid && (peers & lanemask_lt()) == 0) cnt[d * NW + w] = (uint16_t)(base + __popc(peers));
+            __syncwarp();
+            r[i] = base + __popc(peers & lanemask_lt());
+            dg[i] = d;
+        }
+        __syncthreads();
+        // exclusive scan over (digit, warp), digit-major: thread t owns C counters
+        uint32_t loc[C], sum = 0;
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            loc[c] = cnt[tid * C + c];
+            sum += loc[c];
+        }
+        uint64_t tot;
+        uint32_t run = (uint32_t)block_excl_scan<THREADS>(sum, &tot, scratch);
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            cnt[tid * C + c] = (uint16_t)run;
+            run += loc[c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++)
+            if (dg[i] < 256) dst[cnt[dg[i] * NW + w] + r[i]] = x[i];
+        __syncthreads();
+        uint64_t *t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+// Loads rows [off, off + n) (n <= THREADS * 8) into s packed and sorts them
+// by key with `tmp` as scratch; returns the buffer holding the sorted rows.
+template <int THREADS>
+__device__ uint64_t *load_sorted(const Row *__restrict__ src, uint64_t off, uint32_t n, uint64_t *s, uint64_t *tmp,
+                                 uint16_t *cnt, uint64_t *scratch, uint32_t *red) {
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+        const uint2 x = reinterpret_cast<const uint2 *>(src)[off + i];
+        s[i] = pack_row(x.x, x.y);
+    }
+    __syncthreads();
+    return block_radix_sort<THREADS>(s, tmp, n, cnt, scratch, red);
 }
 
 // Merge-path split of diagonal d over sorted arrays A (na) and B (nb):
@@ -78,18 +143,24 @@ __device__ __forceinline__ uint64_t merge_split(uint64_t d, uint64_t na, uint64_
 // RSM: per work item, sorted R chunk in shared memory against sorted S tiles.
 // ---------------------------------------------------------------------------
 constexpr int RSM_THREADS = 512;
-constexpr int RSM_STILE = 4096;
+constexpr int RSM_STILE = RSM_THREADS * 8;  // one radix-sorted S tile
 
-size_t rsm_smem_bytes(int capR) { return ((size_t)capR + RSM_STILE) * 8; }
+// R rows, an S tile, sort scratch, 16-bit sort counters
+size_t rsm_smem_bytes(int capR) {
+    return ((size_t)capR + RSM_STILE + std::max(capR, RSM_STILE)) * 8 + 256 * (RSM_THREADS / 32) * 2;
+}
 
 template <bool MAT>
-__global__ void __launch_bounds__(RSM_THREADS) k_join_rsm(JoinArgs a) {
+__global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t *Rs = reinterpret_cast<uint64_t *>(smem);
-    uint64_t *Ss = Rs + a.capR;
+    uint64_t *Sbuf = Rs + a.capR;
+    uint64_t *tmp = Sbuf + RSM_STILE;
+    uint16_t *cnt = reinterpret_cast<uint16_t *>(tmp + max(a.capR, RSM_STILE));
     __shared__ uint32_t s_item;
     __shared__ unsigned long long s_base;
     __shared__ uint64_t scan_scratch[RSM_THREADS / 32 + 1];
+    __shared__ uint32_t red[2];
     const int tid = threadIdx.x;
     const unsigned nitems = *a.nitems;
     unsigned long long local = 0;
@@ -100,10 +171,13 @@ __global__ void __launch_bounds__(RSM_THREADS) k_join_rsm(JoinArgs a) {
         if (it >= nitems) break;
         const Item m = a.items[it];
         const uint32_t nr = m.r_len;
-        load_sorted<RSM_THREADS>(a.R, m.r_off, nr, Rs);
+        if (load_sorted<RSM_THREADS>(a.R, m.r_off, nr, Rs, tmp, cnt, scan_scratch, red) != Rs) {
+            for (uint32_t q = tid; q < nr; q += RSM_THREADS) Rs[q] = tmp[q];  // sorted R stays in Rs
+            __syncthreads();
+        }
         for (uint64_t s0 = 0; s0 < m.s_len; s0 += RSM_STILE) {
             const uint32_t ns = (uint32_t)umin64(RSM_STILE, m.s_len - s0);
-            load_sorted<RSM_THREADS>(a.S, m.s_off + s0, ns, Ss);
+            const uint64_t *Ss = load_sorted<RSM_THREADS>(a.S, m.s_off + s0, ns, Sbuf, tmp, cnt, scan_scratch, red);
             // each thread walks an equal share of the merge path of R[0..nr) and S[0..ns)
             const uint32_t L = nr + ns;
             const uint32_t per = (L + RSM_THREADS - 1) / RSM_THREADS;
