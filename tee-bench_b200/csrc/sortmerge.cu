@@ -25,6 +25,11 @@ __device__ __forceinline__ uint64_t pack_row(uint32_t k, uint32_t p) { return ((
 __device__ __forceinline__ uint32_t row_key(uint64_t x) { return (uint32_t)(x >> 32); }
 __device__ __forceinline__ uint32_t row_pay(uint64_t x) { return (uint32_t)x; }
 
+// Skewed layout of a sorted tile: row i at i + i / 16, so threads that walk
+// merge-path segments about 8 rows apart hit different banks.
+__device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
+__host__ __device__ constexpr uint32_t padded_rows(uint32_t n) { return n + n / 16 + 1; }
+
 // Block-wide stable LSD radix sort of n <= THREADS * 8 packed rows by key
 // (their high 32 bits) in shared memory.  Only the key bits that differ
 // inside the tile are sorted, 8 per pass.  In a pass, thread (w, lane) holds
@@ -32,8 +37,9 @@ __device__ __forceinline__ uint32_t row_pay(uint64_t x) { return (uint32_t)x; }
 // the same digit before it in that order (per-warp counters advanced slot by
 // slot, __match_any_sync inside a slot), so every pass is stable.  `a` holds
 // the rows, `b` is scratch for n rows, `cnt` 256 * THREADS / 32 counters,
-// `scratch` THREADS / 32 + 1 words, `red` 2 words.  Returns the buffer that
-// holds the sorted rows (a or b).
+// `scratch` THREADS / 32 + 1 words, `red` 2 words.  `a` is read in plain
+// layout; the sorted rows are left in the skewed layout (pad16) in the
+// returned buffer, a or b, each sized padded_rows(n).
 template <int THREADS>
 __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint16_t *cnt, uint64_t *scratch,
                                       uint32_t *red) {
@@ -63,9 +69,14 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
     const uint32_t varying = red[0] & ~red[1];
     __syncthreads();  // red is reused by the next call
     uint64_t *src = a, *dst = b;
-    if (!varying) return src;  // every key equal: already sorted
+    if (!varying) {  // every key equal: already sorted, only the layout changes
+        for (uint32_t e = tid; e < n; e += THREADS) b[pad16(e)] = a[e];
+        __syncthreads();
+        return b;
+    }
     const int lo = __ffs(varying) - 1, hi = 31 - __clz(varying);
     for (int shift = lo; shift <= hi; shift += 8) {
+        const bool last = shift + 8 > hi;
         for (int i = tid; i < 256 * NW; i += THREADS) cnt[i] = 0;
         __syncthreads();
         uint64_t x[ITEMS];
@@ -102,8 +113,12 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
         }
         __syncthreads();
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++)
-            if (dg[i] < 256) dst[cnt[dg[i] * NW + w] + r[i]] = x[i];
+        for (int i = 0; i < ITEMS; i++) {
+            if (dg[i] < 256) {
+                const uint32_t p = cnt[dg[i] * NW + w] + r[i];
+                dst[last ? pad16(p) : p] = x[i];
+            }
+        }
         __syncthreads();
         uint64_t *t = src;
         src = dst;
@@ -113,7 +128,8 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
 }
 
 // Loads rows [off, off + n) (n <= THREADS * 8) into s packed and sorts them
-// by key with `tmp` as scratch; returns the buffer holding the sorted rows.
+// by key with `tmp` as scratch; returns the buffer holding the sorted rows
+// (skewed layout).
 template <int THREADS>
 __device__ uint64_t *load_sorted(const Row *__restrict__ src, uint64_t off, uint32_t n, uint64_t *s, uint64_t *tmp,
                                  uint16_t *cnt, uint64_t *scratch, uint32_t *red) {
@@ -145,18 +161,20 @@ __device__ __forceinline__ uint64_t merge_split(uint64_t d, uint64_t na, uint64_
 constexpr int RSM_THREADS = 512;
 constexpr int RSM_STILE = RSM_THREADS * 8;  // one radix-sorted S tile
 
-// R rows, an S tile, sort scratch, 16-bit sort counters
+// R rows, an S tile, sort scratch (each in the skewed layout), 16-bit sort
+// counters
 size_t rsm_smem_bytes(int capR) {
-    return ((size_t)capR + RSM_STILE + std::max(capR, RSM_STILE)) * 8 + 256 * (RSM_THREADS / 32) * 2;
+    return ((size_t)padded_rows(capR) + padded_rows(RSM_STILE) + padded_rows(std::max(capR, RSM_STILE))) * 8 +
+           256 * (RSM_THREADS / 32) * 2;
 }
 
 template <bool MAT>
 __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t *Rs = reinterpret_cast<uint64_t *>(smem);
-    uint64_t *Sbuf = Rs + a.capR;
-    uint64_t *tmp = Sbuf + RSM_STILE;
-    uint16_t *cnt = reinterpret_cast<uint16_t *>(tmp + max(a.capR, RSM_STILE));
+    uint64_t *Sbuf = Rs + padded_rows(a.capR);
+    uint64_t *tmp = Sbuf + padded_rows(RSM_STILE);
+    uint16_t *cnt = reinterpret_cast<uint16_t *>(tmp + padded_rows(max(a.capR, RSM_STILE)));
     __shared__ uint32_t s_item;
     __shared__ unsigned long long s_base;
     __shared__ uint64_t scan_scratch[RSM_THREADS / 32 + 1];
@@ -172,7 +190,7 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
         const Item m = a.items[it];
         const uint32_t nr = m.r_len;
         if (load_sorted<RSM_THREADS>(a.R, m.r_off, nr, Rs, tmp, cnt, scan_scratch, red) != Rs) {
-            for (uint32_t q = tid; q < nr; q += RSM_THREADS) Rs[q] = tmp[q];  // sorted R stays in Rs
+            for (uint32_t q = tid; q < padded_rows(nr); q += RSM_THREADS) Rs[q] = tmp[q];  // sorted R stays in Rs
             __syncthreads();
         }
         for (uint64_t s0 = 0; s0 < m.s_len; s0 += RSM_STILE) {
@@ -182,8 +200,8 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
             const uint32_t L = nr + ns;
             const uint32_t per = (L + RSM_THREADS - 1) / RSM_THREADS;
             const uint32_t d0 = min(L, tid * per), d1 = min(L, d0 + per);
-            auto kr = [&](uint64_t i) { return row_key(Rs[i]); };
-            auto ks = [&](uint64_t j) { return row_key(Ss[j]); };
+            auto kr = [&](uint64_t i) { return row_key(Rs[pad16((uint32_t)i)]); };
+            auto ks = [&](uint64_t j) { return row_key(Ss[pad16((uint32_t)j)]); };
             uint32_t i = (uint32_t)merge_split(d0, nr, ns, kr, ks);
             uint32_t j = d0 - i;
             // pass 1: count this thread's matches
@@ -193,13 +211,13 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
                 uint32_t last_key = 0, last_cnt = 0;
                 bool have = false;
                 for (uint32_t d = d0; d < d1; d++) {
-                    if (ii < nr && (jj >= ns || row_key(Rs[ii]) < row_key(Ss[jj]))) {
+                    if (ii < nr && (jj >= ns || kr(ii) < ks(jj))) {
                         ii++;
                     } else {
-                        const uint32_t k = row_key(Ss[jj]);
+                        const uint32_t k = ks(jj);
                         if (!have || k != last_key) {
                             last_cnt = 0;
-                            for (uint32_t q = ii; q < nr && row_key(Rs[q]) == k; q++) last_cnt++;
+                            for (uint32_t q = ii; q < nr && kr(q) == k; q++) last_cnt++;
                             last_key = k;
                             have = true;
                         }
@@ -216,16 +234,16 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
                 __syncthreads();
                 uint64_t pos = s_base + off;
                 for (uint32_t d = d0; d < d1; d++) {
-                    if (i < nr && (j >= ns || row_key(Rs[i]) < row_key(Ss[j]))) {
+                    if (i < nr && (j >= ns || kr(i) < ks(j))) {
                         i++;
                     } else {
-                        const uint32_t k = row_key(Ss[j]);
-                        for (uint32_t q = i; q < nr && row_key(Rs[q]) == k; q++) {
+                        const uint32_t k = ks(j);
+                        for (uint32_t q = i; q < nr && kr(q) == k; q++) {
                             if (pos < a.cap) {
                                 tbg_row_out o;
                                 o.key = k;
-                                o.Rpayload = row_pay(Rs[q]);
-                                o.Spayload = row_pay(Ss[j]);
+                                o.Rpayload = row_pay(Rs[pad16(q)]);
+                                o.Spayload = row_pay(Ss[pad16(j)]);
                                 a.out[pos] = o;
                             }
                             pos++;
