@@ -3,8 +3,8 @@
 // RSM (Joins/radix_sortmerge_join.c:102-105) shares RHO's radix partitioning
 // and swaps the build/probe kernel for a per-partition sort + merge-path join.
 // PSM (Joins/psm/parallel_sortmerge_join.h:61-111) sorts both relations by key
-// (LSD radix sort, 8-bit digits, stable one-sweep scatter; a pass whose digit
-// is the same for every row is skipped) and merges them.
+// (LSD radix sort, 8-bit digits, chunked stable passes; a pass whose digit is
+// the same for every row is skipped) and merges them.
 #include <algorithm>
 #include <cstring>
 
@@ -55,7 +55,47 @@ int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const 
     return TBG_OK;
 }
 
-// LSD sort of n rows by key; returns the buffer holding the sorted rows.
+cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, const uint32_t *pre,
+                             const uint32_t *totals, uint32_t shift, unsigned *err, cudaStream_t st);
+
+// LSD sort of n rows by key with chunked stable passes (per-chunk digit
+// histograms, column prefix, k_sort_pass): 24 B per row per pass and no
+// inter-CTA waits.  Passes whose digit is the same for every row (hhist:
+// the four digit histograms of the input) are skipped.
+int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, Workspace &w,
+                     cudaStream_t st, const Row **out, int *passes) {
+    const Row *src = in;
+    Row *bufs[2] = {a.as<Row>(), b.as<Row>()};
+    int which = 0;
+    *passes = 0;
+    const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)w.nsm * 4, (n + 32767) / 32768));
+    const uint64_t chunk = (n + G - 1) / G;
+    cudaError_t e = w.sorthist.ensure(((size_t)G + 1) * 256 * 4);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
+    uint32_t *hist = w.sorthist.as<uint32_t>(), *totals = hist + (size_t)G * 256;
+    unsigned *err = &w.ctrl.as<Ctrl>()->error;
+    for (int p = 0; p < 4; p++) {
+        bool trivial = false;
+        for (int d = 0; d < 256; d++)
+            if (hhist[p * 256 + d] == n) trivial = true;
+        if (trivial || n <= 1) continue;
+        const uint32_t shift = 8 * p;
+        if ((e = launch_hist_chunks(src, n, chunk, G, hist, 8, RadixF{0u, shift, 255u, 0u}, st)) != cudaSuccess ||
+            (e = launch_colscan(hist, G, 256, totals, st)) != cudaSuccess ||
+            (e = launch_sort_pass(src, bufs[which], n, chunk, G, hist, totals, shift, err, st)) != cudaSuccess)
+            return cuda_error(e, "sort pass");
+        src = bufs[which];
+        which ^= 1;
+        (*passes)++;
+    }
+    *out = src;
+    return TBG_OK;
+}
+
+// LSD sort of n rows by key with the one-sweep scatter (one launch per pass,
+// decoupled look-back): used for small inputs (LRN's sample), where launch
+// count matters more than bandwidth.  Returns the buffer holding the sorted
+// rows.
 int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist,
                     const uint64_t *dbases, int slot0, Workspace &w, cudaStream_t st, const Row **out,
                     int *passes) {
@@ -131,10 +171,10 @@ int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *d
     mark_ev(w, timing, 1, st);
     const Row *sR = nullptr, *sS = nullptr;
     int pr = 0, ps = 0;
-    int rc = lsd_sort(dR, nR, w.aux[0], w.aux[1], hh, bases, 0, w, st, &sR, &pr);
+    int rc = lsd_sort_chunked(dR, nR, w.aux[0], w.aux[1], hh, w, st, &sR, &pr);
     if (rc) return rc;
     mark_ev(w, timing, 2, st);
-    rc = lsd_sort(dS, nS, w.aux[2], w.aux[3], hh + 1024, bases + 1024, 4, w, st, &sS, &ps);
+    rc = lsd_sort_chunked(dS, nS, w.aux[2], w.aux[3], hh + 1024, w, st, &sS, &ps);
     if (rc) return rc;
     mark_ev(w, timing, 3, st);
     e = launch_merge_join(sR, nR, sS, nS, w.aux[6].as<uint64_t>(), &ctrl->matches, &ctrl->rows, d_rows,

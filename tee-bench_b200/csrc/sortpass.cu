@@ -1,0 +1,157 @@
+// One stable LSD radix-sort pass for the PSM sort (8-bit digit at `shift`),
+// built like the partitioning passes: CTA c owns chunk c of the input; its
+// digit cursors are base[d] + (rows of digit d in chunks before c), from the
+// per-chunk histograms (k_hist_chunks) and their column prefix (k_colscan),
+// so no CTA waits for another.  Tiles of 512 threads x 8 rows arrive by TMA
+// bulk copy; a row's rank within its tile counts the same-digit rows before
+// it in tile order (per-(digit, warp) counters advanced row slot by row slot,
+// __match_any_sync inside a slot); the tile is staged digit-sorted and
+// written out in slot order, so stores coalesce.  Chunk order, tile order
+// and tile-internal order all follow the input, so the pass is stable.
+#include "part_dev.cuh"
+
+namespace tbg {
+
+constexpr int SORT_THREADS = 512;
+
+struct SortSmem {
+    static constexpr int NW = SORT_THREADS / 32;
+    static constexpr int T = SORT_THREADS * PART_ITEMS;
+    Row buf[2][T + 2];               // input tile (bulk copy), then the same tile digit-sorted
+    uint16_t cnt[2][256 * NW];       // (digit, warp) counts, then offsets, double-buffered
+    uint32_t delta[256];             // output row - tile slot, per digit
+    uint32_t cursor[256];            // next output row of each digit
+    uint64_t scan[NW + 1];
+    uint64_t mbar[2];
+};
+
+template <bool FULL>
+__device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const TileGeo &g, uint32_t k, bool has_next,
+                                          const TileGeo &gnext, uint2 *__restrict__ out, uint32_t out_n,
+                                          uint32_t shift, SortSmem &sm, unsigned *err) {
+    constexpr int NW = SortSmem::NW, C = 256 * NW / SORT_THREADS;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int b = k & 1;
+    const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
+    const uint32_t cnt = g.cnt;
+    uint16_t *c = sm.cnt[b];
+    if (!mbar_wait(&sm.mbar[b], (k >> 1) & 1, SPIN_LIMIT * 16)) atomicCAS(err, 0u, (unsigned)TBG_ERR_TIMEOUT);
+    uint2 v[PART_ITEMS];
+    uint32_t rank[PART_ITEMS];
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < PART_ITEMS; i++) {
+        const uint32_t r = wbase + i * 32 + lane;
+        const bool valid = FULL || r < cnt;
+        if (valid) {
+            if (r >= g.a_lo && r < g.a_hi) {
+                const Row x = sm.buf[b][r + g.off];
+                v[i] = make_uint2(x.key, x.payload);
+            } else {
+                v[i] = reinterpret_cast<const uint2 *>(in)[g.t + r];
+            }
+        }
+        const uint32_t d = valid ? (v[i].x >> shift) & 255 : 256;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        uint32_t base = 0;
+        if (valid) base = c[d * NW + w];
+        __syncwarp();
+        if (valid && (peers & lt) == 0) c[d * NW + w] = (uint16_t)(base + __popc(peers));
+        __syncwarp();
+        rank[i] = base + __popc(peers & lt);
+    }
+    for (int i = tid; i < 256 * NW; i += SORT_THREADS) sm.cnt[b ^ 1][i] = 0;
+    __syncthreads();
+    // the other buffer is free (its tile was written out before this barrier)
+    if (tid == 0 && has_next) issue_tile(in, gnext, sm.buf[b ^ 1], &sm.mbar[b ^ 1]);
+    // exclusive scan over (digit, warp), digit-major; thread t owns C
+    // counters, all of digit t / 2 (two threads per digit)
+    uint32_t sum = 0;
+#pragma unroll
+    for (int q = 0; q < C; q++) sum += c[tid * C + q];
+    uint64_t dummy;
+    uint32_t run = (uint32_t)block_excl_scan<SORT_THREADS, false>(sum, &dummy, sm.scan);
+    const uint32_t dstart = __shfl_sync(0xffffffffu, run, lane & ~1);    // the digit's first offset
+    const uint32_t dtotal = sum + __shfl_xor_sync(0xffffffffu, sum, 1);  // the digit's rows in the tile
+#pragma unroll
+    for (int q = 0; q < C; q++) {
+        const uint32_t x = c[tid * C + q];
+        c[tid * C + q] = (uint16_t)run;
+        run += x;
+    }
+    if ((tid & 1) == 0) {
+        const int d = tid >> 1;
+        sm.delta[d] = sm.cursor[d] - dstart;
+        sm.cursor[d] += dtotal;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PART_ITEMS; i++) {
+        if (FULL || wbase + i * 32 + lane < cnt) {
+            const uint32_t d = (v[i].x >> shift) & 255;
+            sm.buf[b][c[d * NW + w] + rank[i]] = Row{v[i].x, v[i].y};
+        }
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < PART_ITEMS; kk++) {
+        const uint32_t j = kk * SORT_THREADS + tid;
+        if (FULL || j < cnt) {
+            const Row x = sm.buf[b][j];
+            const uint32_t pos = sm.delta[(x.key >> shift) & 255] + j;
+            if (pos < out_n) out[pos] = make_uint2(x.key, x.payload);
+            else atomicCAS(err, 0u, (unsigned)TBG_ERR_ARG);
+        }
+    }
+}
+
+// pre: per-chunk digit prefixes [G][256]; totals: digit totals [256].
+__global__ void __launch_bounds__(SORT_THREADS, 2) k_sort_pass(const Row *__restrict__ in, Row *__restrict__ out,
+                                                               uint64_t n, uint64_t chunk,
+                                                               const uint32_t *__restrict__ pre,
+                                                               const uint32_t *__restrict__ totals, uint32_t shift,
+                                                               unsigned *err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem &sm = *reinterpret_cast<SortSmem *>(smem_raw);
+    constexpr int T = SortSmem::T;
+    const int c = blockIdx.x, tid = threadIdx.x;
+    // digit bases: exclusive scan of the totals, plus this chunk's prefix
+    const uint32_t tot = tid < 256 ? totals[tid] : 0;
+    uint64_t dummy;
+    const uint32_t bse = (uint32_t)block_excl_scan<SORT_THREADS>(tot, &dummy, sm.scan);
+    if (tid < 256) sm.cursor[tid] = bse + pre[(uint64_t)c * 256 + tid];
+    for (int i = tid; i < 256 * SortSmem::NW; i += SORT_THREADS) sm.cnt[0][i] = 0;
+    if (tid == 0) {
+        mbar_init(&sm.mbar[0], 1);
+        mbar_init(&sm.mbar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const uint64_t lo = (uint64_t)c * chunk;
+    const uint64_t hi = umin64(n, lo + chunk);
+    if (lo >= hi) return;
+    const int ntiles = (int)((hi - lo + T - 1) / T);
+    uint2 *o = reinterpret_cast<uint2 *>(out);
+    TileGeo g = tile_geo(in, lo, (uint32_t)umin64(T, hi - lo));
+    if (tid == 0) issue_tile(in, g, sm.buf[0], &sm.mbar[0]);
+    for (int k = 0; k < ntiles; k++) {
+        const uint64_t t1 = g.t + T;
+        const bool more = k + 1 < ntiles;
+        const TileGeo gn = more ? tile_geo(in, t1, (uint32_t)umin64(T, hi - t1)) : g;
+        if (g.cnt == T) sort_tile<true>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sm, err);
+        else sort_tile<false>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sm, err);
+        g = gn;
+    }
+}
+
+cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, const uint32_t *pre,
+                             const uint32_t *totals, uint32_t shift, unsigned *err, cudaStream_t st) {
+    const size_t smem = sizeof(SortSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_sort_pass<<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace tbg

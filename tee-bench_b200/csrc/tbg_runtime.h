@@ -28,6 +28,7 @@ struct Workspace {
     DevBuf status, tmpR, tmpS, partR, partS, items, misc;
     DevBuf inR, inS, rows;      // drop-in layer: device copies of host inputs and output rows
     DevBuf sc, kept;            // learned path: compacted S and kept rows per chunk
+    DevBuf sorthist;            // PSM sort: per-chunk digit histograms and totals
     DevBuf aux[8];              // algorithm-specific scratch (sort, learned model)
     uint32_t epoch = 0;         // last look-back epoch used on `status`
     Ctrl *host_ctrl = nullptr;  // pinned mirror of the control block
@@ -93,6 +94,8 @@ int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row
                     int capR, Workspace &w, cudaStream_t st, JoinRun *run, int *join_grid_out);
 int radix_join_phase(const tbg_config &cfg, tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
                      JoinRun *run, int capR, int join_grid);
+int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, Workspace &w,
+                     cudaStream_t st, const Row **out, int *passes);
 int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, const uint64_t *dbases,
              int slot0, Workspace &w, cudaStream_t st, const Row **out, int *passes);
 cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_t *bases, int nsm,
