@@ -19,7 +19,7 @@ namespace tbg {
 template <bool MAT>
 __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_item[2];
     __shared__ uint64_t scan_scratch[JOIN_THREADS / 32 + 1];
     Table t;
     t.key = reinterpret_cast<uint32_t *>(smem);
@@ -33,11 +33,21 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     const unsigned nitems = *a.nitems;
     unsigned long long local = 0;
 
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.item_ctr, 1u);
-        __syncthreads();
-        const uint32_t it = s_item;
+    // an item is claimed one step ahead, and its R rows are prefetched into
+    // L2 while the current item is probed, so its table build reads L2
+    if (tid == 0) s_item[0] = atomicAdd(a.item_ctr, 1u);
+    __syncthreads();
+    for (uint32_t iter = 0;; iter++) {
+        const uint32_t it = s_item[iter & 1];
         if (it >= nitems) break;
+        if (tid == 0) {
+            const uint32_t nx = atomicAdd(a.item_ctr, 1u);
+            s_item[(iter + 1) & 1] = nx;  // read by all after this item's barriers
+            if (nx < nitems) {
+                const Item mn = a.items[nx];
+                prefetch_l2(a.R + mn.r_off, (uint64_t)mn.r_len * sizeof(Row));
+            }
+        }
         const Item m = a.items[it];
         build_table<JOIN_THREADS>(t, a.R, m.r_off, m.r_len, scan_scratch);
 

@@ -171,6 +171,17 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         : "memory");
 }
 // Bounded wait for phase `parity` of `bar`; false when the limit ran out.
+// Bulk prefetch of [p, p + bytes) into L2 (TMA, no destination); the range
+// is rounded inward to 16-byte bounds, so it never reaches past the rows.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint64_t bytes) {
+    const uintptr_t lo = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t hi = (reinterpret_cast<uintptr_t>(p) + bytes) & ~uintptr_t(15);
+    for (uintptr_t a = lo; a < hi; a += (1u << 20)) {  // at most 1 MB per instruction
+        const uint32_t n = (uint32_t)(hi - a < (1u << 20) ? hi - a : (1u << 20));
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+    }
+}
+
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
     const uint32_t a = smem_addr(bar);
     for (uint32_t it = 0; it < limit; it++) {
