@@ -35,7 +35,7 @@ __host__ __device__ constexpr uint32_t padded_rows(uint32_t n) { return n + n / 
 // inside the tile are sorted, 8 per pass.  In a pass, thread (w, lane) holds
 // rows e = w * 256 + i * 32 + lane (i < 8); a row's rank counts the rows of
 // the same digit before it in that order (per-warp counters advanced slot by
-// slot, __match_any_sync inside a slot), so every pass is stable.  `a` holds
+// slot, ballot-built peer masks inside a slot), so every pass is stable.  `a` holds
 // the rows, `b` is scratch for n rows, `cnt` 256 * THREADS / 32 counters,
 // `scratch` THREADS / 32 + 1 words, `red` 2 words.  `a` is read in plain
 // layout; the sorted rows are left in the skewed layout (pad16) in the
@@ -44,7 +44,8 @@ template <int THREADS>
 __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint16_t *cnt, uint64_t *scratch,
                                       uint32_t *red) {
     constexpr int NW = THREADS / 32, ITEMS = 8, C = 256 * NW / THREADS;
-    static_assert(THREADS * ITEMS <= 65535 && 256 * NW % THREADS == 0, "16-bit counters, even split");
+    static_assert(THREADS * ITEMS <= 65535 && 256 * NW % THREADS == 0 && NW % C == 0,
+                  "16-bit counters; a thread's counters belong to one digit");
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (tid == 0) {
         red[0] = 0;
@@ -87,35 +88,35 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
             const bool valid = e < n;
             x[i] = valid ? src[e] : 0;
             const uint32_t d = valid ? (row_key(x[i]) >> shift) & 255 : 256;
-            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const unsigned peers = warp_peers9(d);
             uint32_t base = 0;
-            if (valid) base = cnt[d * NW + w];
+            if (valid) base = cnt[w * 256 + d];  // warp-major: lanes with different digits hit different banks
             __syncwarp();
-            if (valid && (peers & lanemask_lt()) == 0) cnt[d * NW + w] = (uint16_t)(base + __popc(peers));
+            if (valid && (peers & lanemask_lt()) == 0) cnt[w * 256 + d] = (uint16_t)(base + __popc(peers));
             __syncwarp();
             r[i] = base + __popc(peers & lanemask_lt());
             dg[i] = d;
         }
         __syncthreads();
-        // exclusive scan over (digit, warp), digit-major: thread t owns C counters
-        uint32_t loc[C], sum = 0;
+        // exclusive scan over (digit, warp), digit-major: thread t owns the C
+        // counters of digit t * C / NW for warps (t * C) % NW ...
+        const int dgt = tid * C / NW, w0 = (tid * C) % NW;
+        uint32_t sum = 0;
 #pragma unroll
-        for (int c = 0; c < C; c++) {
-            loc[c] = cnt[tid * C + c];
-            sum += loc[c];
-        }
+        for (int c = 0; c < C; c++) sum += cnt[(w0 + c) * 256 + dgt];
         uint64_t tot;
         uint32_t run = (uint32_t)block_excl_scan<THREADS>(sum, &tot, scratch);
 #pragma unroll
         for (int c = 0; c < C; c++) {
-            cnt[tid * C + c] = (uint16_t)run;
-            run += loc[c];
+            const uint32_t x = cnt[(w0 + c) * 256 + dgt];
+            cnt[(w0 + c) * 256 + dgt] = (uint16_t)run;
+            run += x;
         }
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             if (dg[i] < 256) {
-                const uint32_t p = cnt[dg[i] * NW + w] + r[i];
+                const uint32_t p = cnt[w * 256 + dg[i]] + r[i];
                 dst[last ? pad16(p) : p] = x[i];
             }
         }

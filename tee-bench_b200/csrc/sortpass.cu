@@ -5,7 +5,7 @@
 // so no CTA waits for another.  Tiles of 512 threads x 8 rows arrive by TMA
 // bulk copy; a row's rank within its tile counts the same-digit rows before
 // it in tile order (per-(digit, warp) counters advanced row slot by row slot,
-// __match_any_sync inside a slot); the tile is staged digit-sorted and
+// ballot-built peer masks inside a slot); the tile is staged digit-sorted and
 // written out in slot order, so stores coalesce.  Chunk order, tile order
 // and tile-internal order all follow the input, so the pass is stable.
 #include "part_dev.cuh"
@@ -18,7 +18,7 @@ struct SortSmem {
     static constexpr int NW = SORT_THREADS / 32;
     static constexpr int T = SORT_THREADS * PART_ITEMS;
     Row buf[2][T + 2];               // input tile (bulk copy), then the same tile digit-sorted
-    uint16_t cnt[2][256 * NW];       // (digit, warp) counts, then offsets, double-buffered
+    uint16_t cnt[2][256 * NW];       // [warp][digit] counts, then offsets, double-buffered
     uint32_t delta[256];             // output row - tile slot, per digit
     uint32_t cursor[256];            // next output row of each digit
     uint64_t scan[NW + 1];
@@ -30,6 +30,7 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
                                           const TileGeo &gnext, uint2 *__restrict__ out, uint32_t out_n,
                                           uint32_t shift, SortSmem &sm, unsigned *err) {
     constexpr int NW = SortSmem::NW, C = 256 * NW / SORT_THREADS;
+    static_assert(NW == 2 * C, "two threads per digit");
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int b = k & 1;
     const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
@@ -52,11 +53,11 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
             }
         }
         const uint32_t d = valid ? (v[i].x >> shift) & 255 : 256;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned peers = warp_peers9(d);
         uint32_t base = 0;
-        if (valid) base = c[d * NW + w];
+        if (valid) base = c[w * 256 + d];  // warp-major: lanes with different digits hit different banks
         __syncwarp();
-        if (valid && (peers & lt) == 0) c[d * NW + w] = (uint16_t)(base + __popc(peers));
+        if (valid && (peers & lt) == 0) c[w * 256 + d] = (uint16_t)(base + __popc(peers));
         __syncwarp();
         rank[i] = base + __popc(peers & lt);
     }
@@ -64,19 +65,20 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
     __syncthreads();
     // the other buffer is free (its tile was written out before this barrier)
     if (tid == 0 && has_next) issue_tile(in, gnext, sm.buf[b ^ 1], &sm.mbar[b ^ 1]);
-    // exclusive scan over (digit, warp), digit-major; thread t owns C
-    // counters, all of digit t / 2 (two threads per digit)
+    // exclusive scan over (digit, warp), digit-major; thread t owns the C
+    // counters of digit t / 2 for warps (t & 1) * C ... (two threads per digit)
+    const int dgt = tid >> 1, w0 = (tid & 1) * C;
     uint32_t sum = 0;
 #pragma unroll
-    for (int q = 0; q < C; q++) sum += c[tid * C + q];
+    for (int q = 0; q < C; q++) sum += c[(w0 + q) * 256 + dgt];
     uint64_t dummy;
     uint32_t run = (uint32_t)block_excl_scan<SORT_THREADS, false>(sum, &dummy, sm.scan);
     const uint32_t dstart = __shfl_sync(0xffffffffu, run, lane & ~1);    // the digit's first offset
     const uint32_t dtotal = sum + __shfl_xor_sync(0xffffffffu, sum, 1);  // the digit's rows in the tile
 #pragma unroll
     for (int q = 0; q < C; q++) {
-        const uint32_t x = c[tid * C + q];
-        c[tid * C + q] = (uint16_t)run;
+        const uint32_t x = c[(w0 + q) * 256 + dgt];
+        c[(w0 + q) * 256 + dgt] = (uint16_t)run;
         run += x;
     }
     if ((tid & 1) == 0) {
@@ -89,7 +91,7 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
     for (int i = 0; i < PART_ITEMS; i++) {
         if (FULL || wbase + i * 32 + lane < cnt) {
             const uint32_t d = (v[i].x >> shift) & 255;
-            sm.buf[b][c[d * NW + w] + rank[i]] = Row{v[i].x, v[i].y};
+            sm.buf[b][c[w * 256 + d] + rank[i]] = Row{v[i].x, v[i].y};
         }
     }
     __syncthreads();

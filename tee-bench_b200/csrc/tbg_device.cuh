@@ -85,6 +85,20 @@ __device__ __forceinline__ void block_emit_positions(const uint32_t (&c)[NJ], ui
     __syncthreads();  // scratch is reused by the next round
 }
 
+// Lanes of the warp whose value d (< 512) equals this lane's: one ballot per
+// bit, so the cost does not depend on how many distinct values the warp
+// holds (unlike __match_any_sync).  Every lane of the warp must call it.
+__device__ __forceinline__ unsigned warp_peers9(uint32_t d) {
+    unsigned peers = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const bool bit = (d >> k) & 1;
+        const unsigned b = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? b : ~b;
+    }
+    return peers;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
