@@ -235,6 +235,21 @@ TBG_API int tbg_mlp_grad(const float *params, const float *x, const float *y, ui
 TBG_API int tbg_mlp_train(float *params, const float *x, const float *y, uint64_t n, int steps,
                           float lr, uint64_t seed);
 
+/* ---- chained joins on device-resident output --------------------------------
+ * to_relation (Enclave/TrustedJoins/secure_joins.cpp:277-301): materialised
+ * rows -> relation of (key, payload = R payload) tuples, on the device.     */
+TBG_API int tbg_rows_to_relation(const tbg_row_out *d_rows, uint64_t n, struct row_t *d_out,
+                                 void *stream);
+/* The reference's three-way chain (ecall_three_way_join_sealed_tables,
+ * secure_joins.cpp:348-399) without host round trips: out1 = R x S
+ * materialised into library memory, rel1 = to_relation(out1), then T x rel1
+ * (T on the build side) with cfg's algorithm; its rows go to d_rows2 when it
+ * is not NULL (else count only).  *matches1, *matches2: the two counts.    */
+TBG_API int tbg_join_three_way(const tbg_config *cfg, const struct row_t *dR, uint64_t nR,
+                               const struct row_t *dS, uint64_t nS, const struct row_t *dT,
+                               uint64_t nT, tbg_row_out *d_rows2, uint64_t rows2_cap,
+                               uint64_t *matches1, uint64_t *matches2, void *stream);
+
 /* ---- batched joins (many independent joins, one persistent launch) -------- *
  * No counterpart in the reference, whose driver runs one join per call
  * (native.cpp:125); each join's count equals RHO's on that join.     */

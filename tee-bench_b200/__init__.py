@@ -149,6 +149,11 @@ def lib():
         f.restype = I
     L.tbg_rows_checksum.argtypes = [P, U64, C.POINTER(U64), P]
     L.tbg_rows_checksum.restype = I
+    L.tbg_rows_to_relation.argtypes = [P, U64, P, P]
+    L.tbg_rows_to_relation.restype = I
+    L.tbg_join_three_way.argtypes = [C.POINTER(Config), P, U64, P, U64, P, U64, P, U64, C.POINTER(U64),
+                                     C.POINTER(U64), P]
+    L.tbg_join_three_way.restype = I
     L.tbg_batch_create.argtypes = [C.POINTER(BatchJoin), I, C.POINTER(Config), P, C.POINTER(P)]
     L.tbg_batch_create.restype = I
     L.tbg_batch_run.argtypes = [P, P, P]
@@ -288,6 +293,18 @@ def rows_checksum(d_rows: int, n: int, stream: int = 0) -> int:
     v = C.c_uint64(0)
     _check(lib().tbg_rows_checksum(d_rows, n, C.byref(v), stream or None))
     return int(v.value)
+
+
+def rows_to_relation(d_rows: int, n: int, d_out: int, stream: int = 0):
+    _check(lib().tbg_rows_to_relation(d_rows or None, n, d_out or None, stream or None))
+
+
+def join_three_way(cfg: Config, dR, nR, dS, nS, dT, nT, d_rows2=0, rows2_cap=0, stream=0):
+    """(matches of R x S, matches of T x to_relation(R x S))."""
+    m1, m2 = C.c_uint64(), C.c_uint64()
+    _check(lib().tbg_join_three_way(C.byref(cfg), dR, nR, dS, nS, dT, nT, d_rows2 or None, rows2_cap,
+                                    C.byref(m1), C.byref(m2), stream or None))
+    return int(m1.value), int(m2.value)
 
 
 def last_transfer_bytes():

@@ -29,6 +29,7 @@ struct Workspace {
     DevBuf inR, inS, rows;      // drop-in layer: device copies of host inputs and output rows
     DevBuf sc, kept;            // learned path: compacted S and kept rows per chunk
     DevBuf sorthist;            // PSM sort: per-chunk digit histograms and totals
+    DevBuf chain_rows, chain_rel;  // chained join: first join's rows and the relation made of them
     DevBuf aux[8];              // algorithm-specific scratch (sort, learned model)
     uint32_t epoch = 0;         // last look-back epoch used on `status`
     Ctrl *host_ctrl = nullptr;  // pinned mirror of the control block
