@@ -39,7 +39,7 @@ struct Choice {
     int B = 0;               // 0: direct join, > 0: radix bits of the single pass
     int layout = 0;          // table layout: 0 bucket chain, 1 histogram
     uint32_t capS = 65536;   // S rows per work item / direct slice
-    uint32_t chunk = 32768;  // rows per histogram and scatter chunk
+    uint32_t chunk = 262144;  // rows per histogram and scatter chunk
     double ms = 0;           // tuned time of the class sample (0: not tuned)
     int joins = 0;           // joins of the batch in this class
     int tuned = 0;
@@ -334,7 +334,7 @@ static int autotune(tbg_batch *b, const tbg_batch_join *joins, int njoins, int g
             rc = run(cand);
         }
         if (!rc && best.B > 0) {
-            for (uint32_t chunk : {16384u, 65536u}) {
+            for (uint32_t chunk : {65536u, 1048576u}) {
                 Choice cand = best;
                 cand.chunk = chunk;
                 if ((rc = run(cand))) break;

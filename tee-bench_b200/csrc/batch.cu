@@ -18,6 +18,8 @@
 // Each join's count equals the reference's RHO count on that join
 // (Joins/radix_join.c:1558-1561, join_init_run :1237-1396; bucket
 // chaining :187-244, histogram join :374-440).
+#include <algorithm>
+
 #include "batch.h"
 #include "join_dev.cuh"
 #include "part_dev.cuh"
@@ -66,7 +68,12 @@ __device__ __forceinline__ int ilog2(uint32_t p) { return 31 - __clz(p); }
 // ---------------------------------------------------------------------------
 // hist: chunk histogram over the join's partitions
 // ---------------------------------------------------------------------------
+// Per-warp sub-histograms (P <= 256 bins each): with so few bins nearly every
+// warp holds repeated digits, so each row pays one shared atomic on its
+// warp's own bins instead of a match-based aggregation; the warps' bins are
+// summed at the end of the chunk.
 __device__ void hist_chunk(const BatchArgs &a, uint32_t c, uint32_t *bins) {
+    constexpr int NW = BATCH_THREADS / 32;
     const uint2 ch = a.chunks[c];
     const BatchJoin &J = a.joins[ch.x];
     const int rel = ch.y >> 31;
@@ -75,7 +82,8 @@ __device__ void hist_chunk(const BatchArgs &a, uint32_t c, uint32_t *bins) {
     const uint64_t n = rel ? J.nS : J.nR;
     const uint32_t P = J.P, mask = P - 1;
     const int tid = threadIdx.x;
-    for (uint32_t i = tid; i < P; i += BATCH_THREADS) bins[i] = 0;
+    uint32_t *wb = bins + (tid >> 5) * BATCH_FMAX;  // this warp's bins
+    for (uint32_t i = tid; i < NW * BATCH_FMAX; i += BATCH_THREADS) bins[i] = 0;
     __syncthreads();
     const uint64_t lo = (uint64_t)idx * J.chunk;
     const uint64_t hi = umin64(n, lo + J.chunk);
@@ -84,7 +92,7 @@ __device__ void hist_chunk(const BatchArgs &a, uint32_t c, uint32_t *bins) {
     const uint64_t nv = body / 2;
     const uint4 *v = reinterpret_cast<const uint4 *>(in + lo + head);
     const uint64_t per = (uint64_t)BATCH_THREADS * 4;
-    for (uint64_t base = 0; base < nv; base += per) {  // warp-uniform trip count
+    for (uint64_t base = 0; base < nv; base += per) {
         uint4 x[4];
         bool ok[4];
 #pragma unroll
@@ -93,20 +101,26 @@ __device__ void hist_chunk(const BatchArgs &a, uint32_t c, uint32_t *bins) {
             ok[u] = i < nv;
             if (ok[u]) x[u] = ldg_stream(v + i);
         }
-        const bool dup = warp_has_dups(ok[0] ? (x[0].x & mask) : 0, ok[0]);
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            hist_add_warp(bins, ok[u] ? (x[u].x & mask) : 0, ok[u], dup);
-            hist_add_warp(bins, ok[u] ? (x[u].z & mask) : 0, ok[u], dup);
+            if (ok[u]) {
+                atomicAdd(&wb[x[u].x & mask], 1u);
+                atomicAdd(&wb[x[u].z & mask], 1u);
+            }
         }
     }
     if (tid == 0) {
-        if (head) atomicAdd(&bins[in[lo].key & mask], 1u);
-        if (body & 1) atomicAdd(&bins[in[hi - 1].key & mask], 1u);
+        if (head) atomicAdd(&wb[in[lo].key & mask], 1u);
+        if (body & 1) atomicAdd(&wb[in[hi - 1].key & mask], 1u);
     }
     __syncthreads();
     uint32_t *dst = (rel ? J.histS : J.histR) + (uint64_t)idx * P;
-    for (uint32_t i = tid; i < P; i += BATCH_THREADS) __stcg(dst + i, bins[i]);
+    for (uint32_t f = tid; f < P; f += BATCH_THREADS) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) t += bins[w * BATCH_FMAX + f];
+        __stcg(dst + f, t);
+    }
     cta_signal(&a.sync[ch.x].hist_done);
 }
 
@@ -326,7 +340,7 @@ size_t batch_smem_bytes() {
     size_t s = sizeof(BPart);
     const size_t j = join_smem_bytes(BATCH_CAPR);
     if (j > s) s = j;
-    const size_t sc = (BATCH_THREADS + 4 * BATCH_FMAX) * sizeof(uint32_t);
+    const size_t sc = std::max<size_t>(BATCH_THREADS + 4 * BATCH_FMAX, BATCH_THREADS / 32 * BATCH_FMAX) * sizeof(uint32_t);
     if (sc > s) s = sc;
     return s;
 }
