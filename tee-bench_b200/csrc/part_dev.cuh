@@ -12,7 +12,7 @@ namespace tbg {
 // ---------------------------------------------------------------------------
 
 // True when neighbouring lanes of the warp hold the same digit: a sign of
-// skew, for which ranks are aggregated with __match_any_sync.
+// skew, for which the hot values' rows are aggregated (see hot_peers).
 __device__ __forceinline__ bool warp_has_dups(uint32_t d, bool valid) {
     const int lane = threadIdx.x & 31;
     const uint32_t key = valid ? d : 0xFFFFFFFFu;
@@ -20,34 +20,50 @@ __device__ __forceinline__ bool warp_has_dups(uint32_t d, bool valid) {
     return __any_sync(0xffffffffu, valid && lane > 0 && up == key);
 }
 
+// Under skew a warp holds a few hot values among many distinct ones.  The
+// lanes equal to lane 0's or lane 16's value (the likely hot ones) form a
+// group: returns its lane mask for this lane, or 0 if this lane is in
+// neither group.  Two shuffles and two ballots, whatever the spread.
+__device__ __forceinline__ unsigned hot_peers(uint32_t key) {
+    const uint32_t c0 = __shfl_sync(0xffffffffu, key, 0);
+    const uint32_t c1 = __shfl_sync(0xffffffffu, key, 16);
+    const unsigned g0 = __ballot_sync(0xffffffffu, key == c0);
+    const unsigned g1 = __ballot_sync(0xffffffffu, key == c1 && key != c0);
+    return key == c0 ? g0 : (key == c1 ? g1 : 0u);
+}
+
 // Adds one row's bin to a shared histogram; every lane of the warp calls it
 // (valid = false for lanes without a row).  With `dup` (the warp showed
-// repeated bins: skew), lanes sharing a bin are merged by __match_any_sync
-// into one atomic; otherwise each row pays one shared atomic.
+// repeated bins: skew), the hot groups add once per group; other rows pay
+// one shared atomic each.
 __device__ __forceinline__ void hist_add_warp(uint32_t *h, uint32_t f, bool valid, bool dup) {
     if (!dup) {
         if (valid) atomicAdd(&h[f], 1u);
     } else {
-        const unsigned peers = __match_any_sync(0xffffffffu, valid ? f : 0xFFFFFFFFu);
-        if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&h[f], (uint32_t)__popc(peers));
+        const unsigned peers = hot_peers(valid ? f : 0xFFFFFFFFu);
+        if (!valid) return;
+        if (!peers) atomicAdd(&h[f], 1u);
+        else if ((peers & lanemask_lt()) == 0) atomicAdd(&h[f], (uint32_t)__popc(peers));
     }
 }
 
 // Rank of a row on a shared digit counter (returns the old count).
 // Correct either way; `dup` only picks the faster path.
 __device__ __forceinline__ uint32_t rank_warp(uint32_t *cnt, uint32_t d, bool valid, bool dup) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t key = valid ? d : 0xFFFFFFFFu;
     uint32_t r = 0;
     if (!dup) {
         if (valid) r = atomicAdd(&cnt[d], 1u);
     } else {
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(peers) - 1;
+        const unsigned peers = hot_peers(valid ? d : 0xFFFFFFFFu);
+        const int leader = peers ? __ffs(peers) - 1 : 0;
         uint32_t b = 0;
-        if (valid && lane == leader) b = atomicAdd(&cnt[d], (uint32_t)__popc(peers));
-        b = __shfl_sync(0xffffffffu, b, leader);
-        r = b + __popc(peers & lanemask_lt());
+        if (valid) {
+            if (!peers) r = atomicAdd(&cnt[d], 1u);
+            else if ((int)(threadIdx.x & 31) == leader) b = atomicAdd(&cnt[d], (uint32_t)__popc(peers));
+        }
+        // every lane joins both shuffles; group members take their leader's base
+        const uint32_t b0 = __shfl_sync(0xffffffffu, b, leader);
+        if (valid && peers) r = b0 + __popc(peers & lanemask_lt());
     }
     return r;
 }
