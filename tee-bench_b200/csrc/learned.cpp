@@ -73,7 +73,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     } while (0)
     ENSURE(w.aux[0], m * 8);                     // sample, sort ping
     ENSURE(w.aux[1], m * 8);                     // sort pong
-    ENSURE(w.aux[4], 4 * 256 * 4);               // digit histograms of the sample
+    ENSURE(w.aux[4], 8192);                      // digit histograms of the sample, then candidate counts
     ENSURE(w.aux[5], 4 * 256 * 8);
     ENSURE(w.aux[2], (size_t)16384 * 8);         // training set x, y
     ENSURE(w.aux[3], (size_t)MLP_PARAMS_PAD * 4 * 2 + sizeof(LearnCounters));
@@ -118,7 +118,8 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
                        &npass)))
         return rc;
     // 2. candidates (distinct sampled keys) and the frequency model
-    if ((e = launch_candidates(sorted, m, (double)nS, cand, &lc->ncand, kCandCap, s2)) != cudaSuccess)
+    if ((e = launch_candidates(sorted, m, (double)nS, cand, &lc->ncand, kCandCap, w.aux[4].as<unsigned>(), s2)) !=
+        cudaSuccess)
         return cuda_error(e, "candidates");
     unsigned ncand_raw = 0;
     if ((e = cudaMemcpyAsync(&ncand_raw, &lc->ncand, 4, cudaMemcpyDeviceToHost, s2)) != cudaSuccess ||

@@ -286,26 +286,67 @@ cudaError_t launch_sample(const Row *in, uint64_t n, Row *out, uint64_t m, uint6
 // ---------------------------------------------------------------------------
 // Candidates: each distinct key of the sorted sample, with the sample's
 // estimate of its S rows (nS * run / m).
-__global__ void __launch_bounds__(256) k_candidates(const Row *__restrict__ sorted, uint64_t m, double nS,
-                                                    HeavyCand *cand, unsigned *ncand, unsigned cand_cap) {
-    for (uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x; i < m; i += (uint64_t)gridDim.x * 256) {
-        const uint32_t k = sorted[i].key;
-        if ((i > 0 && sorted[i - 1].key == k) || k == 0xFFFFFFFFu) continue;
-        uint64_t lo = i + 1, hi = m;  // run end: first index with a larger key
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (sorted[mid].key == k) lo = mid + 1;
-            else hi = mid;
+// Candidates: the distinct keys of the sorted sample with their sample
+// estimate of S rows, written in key order (so the training points, and the
+// trained model, do not depend on scheduling).  CTA c owns a contiguous range
+// of the sample; k_cand_count counts the run starts in each range, then every
+// CTA places its run starts after those of the ranges before it.
+constexpr int CAND_THREADS = 256;
+
+__device__ __forceinline__ bool run_start(const Row *sorted, uint64_t i) {
+    const uint32_t k = sorted[i].key;
+    return k != 0xFFFFFFFFu && (i == 0 || sorted[i - 1].key != k);
+}
+
+__global__ void __launch_bounds__(CAND_THREADS) k_cand_count(const Row *__restrict__ sorted, uint64_t m,
+                                                            uint64_t chunk, unsigned *cnt) {
+    __shared__ uint64_t scratch[CAND_THREADS / 32 + 1];
+    const uint64_t lo = (uint64_t)blockIdx.x * chunk, hi = umin64(m, lo + chunk);
+    uint64_t c = 0;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += CAND_THREADS) c += run_start(sorted, i);
+    uint64_t tot;
+    block_excl_scan<CAND_THREADS>(c, &tot, scratch);
+    if (threadIdx.x == 0) cnt[blockIdx.x] = (unsigned)tot;
+}
+
+__global__ void __launch_bounds__(CAND_THREADS) k_candidates(const Row *__restrict__ sorted, uint64_t m,
+                                                            uint64_t chunk, const unsigned *__restrict__ cnt,
+                                                            double nS, HeavyCand *cand, unsigned *ncand,
+                                                            unsigned cand_cap) {
+    __shared__ uint64_t scratch[CAND_THREADS / 32 + 1];
+    const uint64_t lo = (uint64_t)blockIdx.x * chunk, hi = umin64(m, lo + chunk);
+    uint64_t before = 0;  // run starts in the ranges before this one
+    for (unsigned c = threadIdx.x; c < blockIdx.x; c += CAND_THREADS) before += cnt[c];
+    uint64_t base;
+    block_excl_scan<CAND_THREADS>(before, &base, scratch);
+    for (uint64_t t = lo; t < hi; t += CAND_THREADS) {  // block-uniform trip count
+        const uint64_t i = t + threadIdx.x;
+        const bool start = i < hi && run_start(sorted, i);
+        uint64_t tile;
+        const uint64_t pos = base + block_excl_scan<CAND_THREADS>(start ? 1 : 0, &tile, scratch);
+        if (start) {
+            const uint32_t k = sorted[i].key;
+            uint64_t a = i + 1, b = m;  // run end: first index with a larger key
+            while (a < b) {
+                const uint64_t mid = (a + b) >> 1;
+                if (sorted[mid].key == k) a = mid + 1;
+                else b = mid;
+            }
+            if (pos < cand_cap) cand[pos] = HeavyCand{k, (float)(nS * (double)(a - i) / (double)m)};
         }
-        const unsigned slot = atomicAdd(ncand, 1u);
-        if (slot < cand_cap) cand[slot] = HeavyCand{k, (float)(nS * (double)(lo - i) / (double)m)};
+        base += tile;
     }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *ncand = (unsigned)base;
 }
 
 cudaError_t launch_candidates(const Row *sorted, uint64_t m, double nS, HeavyCand *cand, unsigned *ncand,
-                              unsigned cand_cap, cudaStream_t st) {
-    k_candidates<<<(unsigned)umin64((m + 255) / 256, 148 * 8), 256, 0, st>>>(sorted, m, nS, cand, ncand, cand_cap);
-    count_launch();
+                              unsigned cand_cap, unsigned *scratch_cnt, cudaStream_t st) {
+    if (!m) return cudaMemsetAsync(ncand, 0, sizeof(unsigned), st);
+    const unsigned g = (unsigned)umin64((m + 4095) / 4096, 148 * 8);
+    const uint64_t chunk = (m + g - 1) / g;
+    k_cand_count<<<g, CAND_THREADS, 0, st>>>(sorted, m, chunk, scratch_cnt);
+    k_candidates<<<g, CAND_THREADS, 0, st>>>(sorted, m, chunk, scratch_cnt, nS, cand, ncand, cand_cap);
+    count_launch(2);
     return cudaGetLastError();
 }
 

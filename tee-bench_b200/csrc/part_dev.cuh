@@ -11,13 +11,15 @@ namespace tbg {
 // shared helpers
 // ---------------------------------------------------------------------------
 
-// True when neighbouring lanes of the warp hold the same digit: a sign of
-// skew, for which the hot values' rows are aggregated (see hot_peers).
+// True when at least four neighbouring lane pairs of the warp hold the same
+// digit: a sign of skew, for which the hot values' rows are aggregated (see
+// hot_peers).  Fewer repeats (uniform keys over 128-256 digits give a pair
+// in about one warp in five) cost less as plain atomics.
 __device__ __forceinline__ bool warp_has_dups(uint32_t d, bool valid) {
     const int lane = threadIdx.x & 31;
     const uint32_t key = valid ? d : 0xFFFFFFFFu;
     const uint32_t up = __shfl_up_sync(0xffffffffu, key, 1);
-    return __any_sync(0xffffffffu, valid && lane > 0 && up == key);
+    return __popc(__ballot_sync(0xffffffffu, valid && lane > 0 && up == key)) >= 4;
 }
 
 // Under skew a warp holds a few hot values among many distinct ones.  The

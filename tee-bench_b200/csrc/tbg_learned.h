@@ -69,7 +69,7 @@ cudaError_t launch_mlp_train(const float *xs, const float *ys, uint32_t n, float
                              uint64_t seed, cudaStream_t st);
 cudaError_t launch_sample(const Row *in, uint64_t n, Row *out, uint64_t m, uint64_t seed, cudaStream_t st);
 cudaError_t launch_candidates(const Row *sorted, uint64_t m, double nS, HeavyCand *cand, unsigned *ncand,
-                              unsigned cand_cap, cudaStream_t st);
+                              unsigned cand_cap, unsigned *scratch_cnt, cudaStream_t st);
 cudaError_t launch_freq_points(const HeavyCand *cand, unsigned ncand, float *xs, float *ys, uint32_t T,
                                cudaStream_t st);
 cudaError_t launch_heavy_score(HeavyCand *cand, unsigned ncand, const float *params, int use_model, double tau_min,
