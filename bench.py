@@ -53,6 +53,8 @@ WORKLOADS = {
     "plain_c3_z15": ("RHO", 26, 29, "zipf", 1.5, {"skew_split": 0}),
     "lrn_c3_z15": ("LRN", 26, 29, "zipf", 1.5),
     "rho_c1": ("RHO", 21, 21, "fk", 100),
+    # one 2^27 / 2^30 join sharded over the ranks (S split, R broadcast from rank 0)
+    "rho_c2_sharded": ("RHO", 27, 30, "fk", 100, {"sharded": 1}),
     # 2^28 / 2^31 Zipf z = 1.0, materialised (2^31 output rows, 25.8 GB)
     "lrn_c5_mat": ("LRN", 28, 31, "zipf", 1.0, {"materialize": 1}),
     "radix_c5_mat": ("RHO", 28, 31, "zipf", 1.0, {"materialize": 1}),
@@ -114,6 +116,27 @@ def max_over_ranks(x, dist, device):
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def shard_rows(n, world, rank):
+    """[lo, hi): the rows rank owns when n rows are split evenly over world."""
+    base, rem = divmod(n, world)
+    lo = rank * base + min(rank, rem)
+    return lo, lo + base + (1 if rank < rem else 0)
+
+
+def sharded_count(dist, R, S_local, join_count, root=0):
+    """One equi-join of R with S split across the ranks: R (a tensor of rows,
+    valid on root) is broadcast from root, the exchange step; every rank joins
+    its shard of S; the counts are summed on every rank."""
+    import torch
+    multi = dist is not None and dist.is_initialized() and dist.get_world_size() > 1
+    if multi:
+        dist.broadcast(R, src=root)
+    t = torch.tensor([int(join_count(R, S_local))], dtype=torch.int64, device=R.device)
+    if multi:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item())
 
 
 def job_mtuples(world, rows_per_rank, steps, seconds):
@@ -275,6 +298,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload in BATCH_WORKLOADS:
         return batch_main(args, rank, world, local)
+    if wl_spec(args.workload)[5].get("sharded"):
+        return sharded_main(args, rank, world, local)
     algo, lr, ls, kind, param, over = wl_spec(args.workload)
     lr = args.log2_r if args.log2_r is not None else lr
     ls = args.log2_s if args.log2_s is not None else ls
@@ -315,10 +340,10 @@ def main():
     import torch
     import torch.distributed as dist
     tbg = importlib.import_module("tee-bench_b200")
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if world > 1:  # the rank's GPU is current before NCCL binds to it
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300), device_id=dev)
     stream = torch.cuda.Stream(device=dev)
     sh = stream.cuda_stream
 
@@ -525,6 +550,138 @@ def main():
     return 0
 
 
+# ------------------------------------------------------------------ sharded
+def sharded_main(args, rank, world, local):
+    """One |R| = 2^27, |S| = 2^30 join over all ranks (strong scaling): S is
+    split evenly, R lives on rank 0 and is broadcast (NCCL) every step, each
+    rank joins its shard, the counts are all-reduced."""
+    algo, lr, ls, kind, param, _ = wl_spec(args.workload)
+    lr = args.log2_r if args.log2_r is not None else lr
+    ls = args.log2_s if args.log2_s is not None else ls
+    nR, nS = 1 << lr, 1 << ls
+    lo, hi = shard_rows(nS, world, rank)
+    nSl = hi - lo
+    workload_name = (f"{algo} |R|=2^{lr} |S|=2^{ls} uniform FK, count only, one join sharded over {world} GPU(s): "
+                     f"S split evenly, R broadcast from rank 0 each step, counts all-reduced")
+    metric = "input Mtuples/s (|R|+|S|)/t of one sharded count-only equi-join, bit-exact"
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = host_threads()
+        res, why = cpu_reference_run("rho_c2", 1 << args.cpu_sample_log2, max(1, args.steps), 1, threads)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        print(json.dumps({"impl": "reference", "metric": metric, "value": res["value"], "unit": "Mtuples/s",
+                          "n_gpus": world, "steps": max(1, args.steps), "warmup": 1,
+                          "ms_per_step": res["seconds_per_step"] * 1e3, "higher_is_better": True,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                          "config": {"workload": workload_name, "global_batch": res["nR"] + res["nS"]},
+                          "cpu_baseline": {"value": res["value"], "unit": "Mtuples/s", "cores": threads,
+                                           "kind": "reference",
+                                           "sample": f"reference RHO (oracle/_ref) on |R|={res['nR']}, "
+                                                     f"|S|={res['nS']} rows, {threads} threads, its own timer"},
+                          "e2e": {"value": res["value"], "unit": "Mtuples/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+    import torch.distributed as dist
+    tbg = importlib.import_module("tee-bench_b200")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300), device_id=dev)
+    # one stream (the current one) orders the broadcast, the join and the reduction
+    sh = torch.cuda.current_stream().cuda_stream
+    tR = torch.zeros(nR, dtype=torch.int64, device=dev)
+    tS = torch.empty(max(nSl, 1), dtype=torch.int64, device=dev)
+    if rank == 0:
+        tbg.gen_pk(tR.data_ptr(), nR, 11111, sh)
+    tbg.gen_fk(tS.data_ptr(), nSl, nR, 22222 + rank, sh)
+    torch.cuda.synchronize()
+    cfg = tbg.config(algo)
+
+    def join_count(R, S):
+        return tbg.join_device(cfg, R.data_ptr(), nR, S.data_ptr(), nSl, stream=sh)[1]
+
+    for _ in range(args.warmup):
+        m = sharded_count(dist, tR, tS, join_count)
+    if m != nS:
+        raise SystemExit(f"wrong match count {m} != {nS}")
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = tbg.kernel_launches()
+    with ClockSampler(local) as clocks:
+        ev0.record()
+        for _ in range(args.steps):
+            m = sharded_count(dist, tR, tS, join_count)
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = tbg.kernel_launches() - l0
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
+    K = args.steps
+    value = (nR + nS) * K / (ms / 1e3) / 1e6
+    e2e = None
+    if args.e2e_steps > 0:  # every step: the shard (and R on rank 0) copied from pinned host memory
+        hS = torch.empty_like(tS, device="cpu", pin_memory=True)
+        hS.copy_(tS)
+        hR = torch.empty_like(tR, device="cpu", pin_memory=True) if rank == 0 else None
+        if hR is not None:
+            hR.copy_(tR)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.e2e_steps):
+            tS.copy_(hS, non_blocking=True)
+            if hR is not None:
+                tR.copy_(hR, non_blocking=True)
+            m = sharded_count(dist, tR, tS, join_count)  # the count is read back to the host
+        e1.record()
+        torch.cuda.synchronize()
+        el = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, dev)
+        e2e = {"value": (nR + nS) * args.e2e_steps / el / 1e6, "unit": "Mtuples/s",
+               "h2d_bytes_per_step": (nR + nS) * 8, "d2h_bytes_per_step": 8 * world,
+               "api": "tbg_join_device per shard, R broadcast over NCCL, count all-reduced; inputs copied from "
+                      "pinned host memory each step", "count": int(m)}
+    peak, peak_kind = read_peaks()
+    alg = 48 * (nR + nSl)  # this rank's pipeline: histogram 8 + 2 passes x 16 + build/probe 8 B per row
+    line = {
+        "metric": metric, "value": value, "unit": "Mtuples/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": workload_name, "global_batch": nR + nS, "nR": nR, "nS": nS,
+                   "shard_rows_S": nSl, "exchange_bytes_per_step": nR * 8 * (world > 1),
+                   "parallelism": f"S sharded over {world} rank(s), R broadcast (NCCL), count all-reduce",
+                   "l2": "inputs larger than the 126 MB L2; no flush needed"},
+        "gpu_launches": int(launches),
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "kernel": "all kernels of one shard's RHO join (pipeline)",
+                     "achieved": alg / (ms / K / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (ms / K / 1e3) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_shard": alg},
+        "clocks": clocks.summary(),
+        "matches": int(m),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        res, why = cpu_reference_run("rho_c2", 1 << args.cpu_sample_log2, 1, 0, threads)
+        line["cpu_baseline"] = ({"value": res["value"], "unit": "Mtuples/s", "cores": threads, "kind": "reference",
+                                 "sample": f"reference RHO (oracle/_ref) on |R|={res['nR']}, |S|={res['nS']} rows"}
+                                if res else {"value": None, "unavailable": why})
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------------ batch
 def batch_algorithmic_bytes(dj, desc):
     """Bytes each join must move under the plan's choices: partitioned joins
@@ -615,10 +772,10 @@ def batch_main(args, rank, world, local):
     import torch
     import torch.distributed as dist
     tbg = importlib.import_module("tee-bench_b200")
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if world > 1:  # the rank's GPU is current before NCCL binds to it
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300), device_id=dev)
     stream = torch.cuda.Stream(device=dev)
     sh = stream.cuda_stream
     with torch.cuda.stream(stream):
