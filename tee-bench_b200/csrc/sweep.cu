@@ -9,7 +9,7 @@ namespace tbg {
 //
 //  1. rows are loaded warp-striped: warp w owns a contiguous sub-tile, so the
 //     order (warp, item, lane) is the input order (needed for stability);
-//  2. each row is ranked inside its warp with __match_any_sync against a
+//  2. each row is ranked inside its warp (ballot-built peer masks) against a
 //     warp-private digit counter; a column scan over warps and a scan over
 //     digits give every row its slot in the digit-sorted tile;
 //  3. the tile publishes its digit counts and looks back over predecessor
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(ScatterArgs a) {
     uint32_t *myc = wcnt + w * SCATTER_FMAX;
 #pragma unroll
     for (int i = 0; i < SCATTER_ITEMS; i++) {
-        unsigned peers = __match_any_sync(0xffffffffu, d[i]);
+        unsigned peers = warp_peers9(d[i]);  // d < 512: digit or the sentinel
         unsigned lt = peers & lanemask_lt();
         uint32_t c = d[i] < SCATTER_FMAX ? myc[d[i]] : 0;
         rank[i] = c + __popc(lt);
