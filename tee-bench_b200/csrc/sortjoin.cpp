@@ -7,6 +7,7 @@
 // the same for every row is skipped) and merges them.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "tbg_internal.h"
 #include "tbg_runtime.h"
@@ -56,12 +57,14 @@ int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const 
 }
 
 cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, const uint32_t *pre,
-                             const uint32_t *totals, uint32_t shift, unsigned *err, cudaStream_t st);
+                             const uint32_t *totals, uint32_t shift, int digit_bits, unsigned *err, cudaStream_t st);
 
 // LSD sort of n rows by key with chunked stable passes (per-chunk digit
 // histograms, column prefix, k_sort_pass): 24 B per row per pass and no
-// inter-CTA waits.  Passes whose digit is the same for every row (hhist:
-// the four digit histograms of the input) are skipped.
+// inter-CTA waits.  hhist holds the four 8-bit digit histograms of the input:
+// 8-bit digits that are the same for every row are skipped, and when the key
+// bits that vary fit fewer 9-bit digits than the remaining 8-bit passes, the
+// sort uses 9-bit digits instead (e.g. 3 passes for 27-bit keys, not 4).
 int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, Workspace &w,
                      cudaStream_t st, const Row **out, int *passes) {
     const Row *src = in;
@@ -70,19 +73,44 @@ int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint
     *passes = 0;
     const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)w.nsm * 4, (n + 32767) / 32768));
     const uint64_t chunk = (n + G - 1) / G;
-    cudaError_t e = w.sorthist.ensure(((size_t)G + 1) * 256 * 4);
+    cudaError_t e = w.sorthist.ensure(((size_t)G + 1) * 512 * 4);
     if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
-    uint32_t *hist = w.sorthist.as<uint32_t>(), *totals = hist + (size_t)G * 256;
+    uint32_t *hist = w.sorthist.as<uint32_t>(), *totals = hist + (size_t)G * 512;
     unsigned *err = &w.ctrl.as<Ctrl>()->error;
+    if (n <= 1) {
+        *out = src;
+        return TBG_OK;
+    }
+    // the passes: (shift, digit bits)
+    std::vector<std::pair<uint32_t, int>> plan;
+    int lo_bit = -1, hi_bit = -1;
     for (int p = 0; p < 4; p++) {
         bool trivial = false;
-        for (int d = 0; d < 256; d++)
+        int top = 0;
+        for (int d = 0; d < 256; d++) {
             if (hhist[p * 256 + d] == n) trivial = true;
-        if (trivial || n <= 1) continue;
-        const uint32_t shift = 8 * p;
-        if ((e = launch_hist_chunks(src, n, chunk, G, hist, 8, RadixF{0u, shift, 255u, 0u}, st)) != cudaSuccess ||
-            (e = launch_colscan(hist, G, 256, totals, st)) != cudaSuccess ||
-            (e = launch_sort_pass(src, bufs[which], n, chunk, G, hist, totals, shift, err, st)) != cudaSuccess)
+            if (hhist[p * 256 + d]) top = d;
+        }
+        if (trivial) continue;
+        plan.push_back({8u * p, 8});
+        if (lo_bit < 0) lo_bit = 8 * p;
+        hi_bit = 8 * p + (top ? 31 - __builtin_clz((unsigned)top) : 0);
+    }
+    if (lo_bit >= 0) {
+        const int bits = hi_bit - lo_bit + 1;
+        const int p9 = (bits + 8) / 9;
+        if (p9 < (int)plan.size()) {
+            plan.clear();
+            for (int i = 0; i < p9; i++) plan.push_back({(uint32_t)(lo_bit + 9 * i), 9});
+        }
+    }
+    for (const auto &pp : plan) {
+        const uint32_t shift = pp.first;
+        const int db = pp.second;
+        const uint32_t m2 = (1u << db) - 1;
+        if ((e = launch_hist_chunks(src, n, chunk, G, hist, db, RadixF{0u, shift, m2, 0u}, st)) != cudaSuccess ||
+            (e = launch_colscan(hist, G, 1 << db, totals, st)) != cudaSuccess ||
+            (e = launch_sort_pass(src, bufs[which], n, chunk, G, hist, totals, shift, db, err, st)) != cudaSuccess)
             return cuda_error(e, "sort pass");
         src = bufs[which];
         which ^= 1;
