@@ -132,6 +132,14 @@ TBG_API extern const algorithm_t tbg_algorithms[];
 TBG_API extern const int tbg_num_algorithms;
 TBG_API const algorithm_t *tbg_find(const char *name); /* NULL when unknown */
 
+/* S slices that RHO and RHT (and their _mat forms) copy to the GPU and join
+ * one after another, each slice's join overlapping the next slice's copy;
+ * the result is the whole join's.  0 (the default): one slice per 2^26 S
+ * rows, at most 16; 1: copy everything, then join.  Returns the previous
+ * setting.  No counterpart in the reference (its relations are in host
+ * memory already). */
+TBG_API int tbg_set_dropin_slices(int k);
+
 /* Host<->device bytes the last drop-in call moved (inputs in, result out). */
 TBG_API void tbg_last_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
 

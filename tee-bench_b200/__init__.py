@@ -164,6 +164,8 @@ def lib():
     L.tbg_batch_describe.restype = I
     L.tbg_batch_destroy.argtypes = [P]
     L.tbg_last_transfer_bytes.argtypes = [C.POINTER(U64), C.POINTER(U64)]
+    L.tbg_set_dropin_slices.argtypes = [I]
+    L.tbg_set_dropin_slices.restype = I
     L.tbg_mlp_param_count.restype = I
     L.tbg_mlp_feature.argtypes = [C.c_uint32]
     L.tbg_mlp_feature.restype = C.c_float
@@ -305,6 +307,12 @@ def join_three_way(cfg: Config, dR, nR, dS, nS, dT, nT, d_rows2=0, rows2_cap=0, 
     _check(lib().tbg_join_three_way(C.byref(cfg), dR, nR, dS, nS, dT, nT, d_rows2 or None, rows2_cap,
                                     C.byref(m1), C.byref(m2), stream or None))
     return int(m1.value), int(m2.value)
+
+
+def set_dropin_slices(k: int) -> int:
+    """S slices the drop-in RHO/RHT copy and join one by one (0: automatic,
+    1: copy all, then join).  Returns the previous setting."""
+    return lib().tbg_set_dropin_slices(int(k))
 
 
 def last_transfer_bytes():

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -358,6 +359,58 @@ int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row 
     int rc = radix_partition(cfg, dR, nR, dS, nS, capR, w, st, run, &join_grid);
     if (rc) return rc;
     return radix_join_phase(cfg, d_rows, cap, w, st, run, capR, join_grid);
+}
+
+// RHO / RHT with S arriving in slices, for callers that copy S from the host
+// on another stream: slice k is [s_lo[k], s_lo[k+1]) of dS.  issue(-1)
+// starts R's copy and issue(k) slice k's; each records r_ready / s_ready[k]
+// when its copy is done.  Slice k + 1's copy is issued before slice k's work
+// is queued, so copies from pageable memory (which block the host) still
+// overlap the work.  R is
+// partitioned once; each slice is partitioned with R's radix geometry
+// (which depends on |R| only), planned against R's partitions and joined.
+// Matches and output rows accumulate in the control block across slices,
+// so the count and the row multiset equal the whole join's, and slice k's
+// work overlaps the copy of slice k + 1.
+int run_radix_join_sliced(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, const uint64_t *s_lo,
+                          int nslices, const std::function<int(int)> &issue, cudaEvent_t r_ready,
+                          const cudaEvent_t *s_ready, tbg_row_out *d_rows, uint64_t cap, Workspace &w,
+                          cudaStream_t st, JoinRun *run) {
+    const int capR = join_capacity(nR);
+    uint64_t smax = 1;
+    for (int k = 0; k < nslices; k++) smax = std::max(smax, s_lo[k + 1] - s_lo[k]);
+    const RadixGeom gmax = radix_geometry(cfg, nR, smax, capR, w);
+    run->B = gmax.B;
+    run->passes = gmax.passes;
+    run->P = gmax.P;
+    int rc = ensure_radix_buffers(gmax, false, w);
+    if (rc) return rc;
+    Ctrl *ctrl = w.ctrl.as<Ctrl>();
+    if ((rc = issue(-1)) || (nslices > 0 && (rc = issue(0)))) return rc;
+    cudaError_t e = cudaMemsetAsync(w.ctrl.p, 0, sizeof(Ctrl), st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, r_ready, 0);
+    if (e != cudaSuccess) return cuda_error(e, "sliced join: setup");
+    // R: histogram, bases and both passes, while S is still arriving
+    if ((rc = part_histogram(0, gmax, dR, cfg, w, st, nullptr))) return rc;
+    if ((rc = part_pass(0, 1, gmax, dR, w, st, false))) return rc;
+    if ((rc = part_pass(0, 2, gmax, dR, w, st, false))) return rc;
+    for (int k = 0; k < nslices; k++) {
+        if (k + 1 < nslices && (rc = issue(k + 1))) return rc;
+        const uint64_t n = s_lo[k + 1] - s_lo[k];
+        if (!n) continue;
+        const Row *d = dS + s_lo[k];
+        const RadixGeom g = radix_geometry(cfg, nR, n, capR, w);
+        if ((e = cudaStreamWaitEvent(st, s_ready[k], 0)) != cudaSuccess) return cuda_error(e, "sliced join: wait");
+        if ((rc = part_histogram(1, g, d, cfg, w, st, nullptr))) return rc;
+        if ((rc = plan_items(g, w, st))) return rc;
+        if ((rc = part_pass(1, 1, g, d, w, st, false))) return rc;
+        if ((rc = part_pass(1, 2, g, d, w, st, false))) return rc;
+        // the join's work-item ticket restarts for every slice
+        if ((e = cudaMemsetAsync(&ctrl->item_ctr[0], 0, sizeof(unsigned), st)) != cudaSuccess)
+            return cuda_error(e, "memset");
+        if ((rc = radix_join_phase(cfg, d_rows, cap, w, st, run, capR, g.join_grid))) return rc;
+    }
+    return TBG_OK;
 }
 
 // Build/probe over the partitions radix_partition left in partR / partS.

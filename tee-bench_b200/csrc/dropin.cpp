@@ -25,6 +25,32 @@ static uint64_t g_last_h2d = 0, g_last_d2h = 0;  // bytes the last call moved
 
 extern int dropin_errmode();
 
+// RHO and RHT copy large S in slices on a second stream and join each slice
+// as it lands (run_radix_join_sliced), so only the last slice's work follows
+// the last copy.
+constexpr int MAX_SLICES = 16;
+constexpr uint64_t SLICE_ROWS = 1ull << 26;  // 512 MiB of S per slice
+static int g_slices = 0;                     // 0: SLICE_ROWS per slice, up to MAX_SLICES
+static cudaStream_t g_copy = nullptr;
+static cudaEvent_t g_ready[MAX_SLICES + 1];  // [0]: R copied; [1 + k]: slice k copied
+static cudaEvent_t g_idle;                   // the join stream reached the copies
+
+static int slice_count(int algo, uint64_t nR, uint64_t nS) {
+    if (algo != TBG_RHO && algo != TBG_RHT) return 1;
+    if (nR == 0 || nR > 0xFFFFFFFFull || nS > 0xFFFFFFFFull) return 1;
+    const uint64_t k = g_slices > 0 ? (uint64_t)g_slices : nS / SLICE_ROWS;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(std::min<uint64_t>(k, MAX_SLICES), nS));
+}
+
+static cudaError_t slice_streams() {
+    if (g_copy) return cudaSuccess;
+    cudaError_t e = cudaStreamCreateWithFlags(&g_copy, cudaStreamNonBlocking);
+    for (auto &ev : g_ready)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g_idle, cudaEventDisableTiming);
+    return e;
+}
+
 static cudaError_t h2d(void *dst, const void *src, size_t bytes, cudaStream_t st) {
     if (!bytes) return cudaSuccess;
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
@@ -92,8 +118,17 @@ static result_t *dropin(int algo, struct table_t *relR, struct table_t *relS, in
     cudaError_t e;
     if ((e = w->inR.ensure(std::max<uint64_t>(nR, 1) * 8)) != cudaSuccess) return fail(cuda_error(e, "cudaMalloc"));
     if ((e = w->inS.ensure(std::max<uint64_t>(nS, 1) * 8)) != cudaSuccess) return fail(cuda_error(e, "cudaMalloc"));
-    if ((e = h2d(w->inR.p, relR->tuples, nR * 8, g_stream)) != cudaSuccess) return fail(cuda_error(e, "H2D R"));
-    if ((e = h2d(w->inS.p, relS->tuples, nS * 8, g_stream)) != cudaSuccess) return fail(cuda_error(e, "H2D S"));
+    const int K = slice_count(algo, nR, nS);
+    if (K == 1) {
+        if ((e = h2d(w->inR.p, relR->tuples, nR * 8, g_stream)) != cudaSuccess) return fail(cuda_error(e, "H2D R"));
+        if ((e = h2d(w->inS.p, relS->tuples, nS * 8, g_stream)) != cudaSuccess) return fail(cuda_error(e, "H2D S"));
+    } else {
+        if ((e = slice_streams()) != cudaSuccess) return fail(cuda_error(e, "copy stream"));
+        // the copies overwrite the inputs only after the join stream's earlier work
+        if ((e = cudaEventRecord(g_idle, g_stream)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(g_copy, g_idle, 0)) != cudaSuccess)
+            return fail(cuda_error(e, "copy stream"));
+    }
 
     g_last_h2d = (nR + nS) * 8;
     g_last_d2h = sizeof(Ctrl);
@@ -104,15 +139,38 @@ static result_t *dropin(int algo, struct table_t *relR, struct table_t *relS, in
     uint64_t matches = 0;
     uint64_t cap = 0;
     tbg_row_out *d_rows = nullptr;
+    const Row *dR = w->inR.as<Row>(), *dS = w->inS.as<Row>();
+    bool resident = K == 1;
     for (int attempt = 0; attempt < 2; attempt++) {
         if (mat) {
             cap = attempt == 0 ? std::max<uint64_t>(nS, 1024) : std::max<uint64_t>(matches, 1);
             if ((e = w->rows.ensure(cap * sizeof(tbg_row_out))) != cudaSuccess) return fail(cuda_error(e, "cudaMalloc rows"));
             d_rows = w->rows.as<tbg_row_out>();
         }
-        int rc = tbg_join_device(&cfg, reinterpret_cast<const row_t *>(w->inR.p), nR,
-                                 reinterpret_cast<const row_t *>(w->inS.p), nS, d_rows, cap, &matches,
-                                 nullptr, g_stream);
+        int rc;
+        if (resident) {
+            rc = tbg_join_device(&cfg, reinterpret_cast<const row_t *>(dR), nR, reinterpret_cast<const row_t *>(dS),
+                                 nS, d_rows, cap, &matches, nullptr, g_stream);
+        } else {
+            uint64_t lo[MAX_SLICES + 1];
+            for (int k = 0; k <= K; k++) lo[k] = nS * (uint64_t)k / (uint64_t)K;
+            auto issue = [&](int k) -> int {
+                const bool isR = k < 0;
+                const uint64_t off = isR ? 0 : lo[k] * 8, bytes = isR ? nR * 8 : (lo[k + 1] - lo[k]) * 8;
+                const void *src = static_cast<const char *>(isR ? (const void *)relR->tuples : (const void *)relS->tuples) + off;
+                void *dst = static_cast<char *>(isR ? w->inR.p : w->inS.p) + off;
+                cudaError_t ce = h2d(dst, src, bytes, g_copy);
+                if (ce == cudaSuccess) ce = cudaEventRecord(g_ready[isR ? 0 : 1 + k], g_copy);
+                return ce == cudaSuccess ? TBG_OK : cuda_error(ce, isR ? "H2D R" : "H2D S slice");
+            };
+            JoinRun run;
+            rc = run_radix_join_sliced(cfg, dR, nR, dS, lo, K, issue, g_ready[0], g_ready + 1, d_rows, cap, *w,
+                                       g_stream, &run);
+            if (rc == TBG_OK) rc = finish_join(cfg, *w, g_stream, run, nR, nS, cap, &matches, nullptr);
+            cudaError_t ce = cudaStreamSynchronize(g_copy);  // no copy outlives the call, even on error
+            if (rc == TBG_OK && ce != cudaSuccess) rc = cuda_error(ce, "H2D");
+            resident = true;
+        }
         if (rc == TBG_OK) break;
         if (!(rc == TBG_ERR_CAPACITY && attempt == 0)) return fail(rc);
     }
@@ -169,6 +227,13 @@ const algorithm_t *tbg_find(const char *name) {
         if (strcmp(name, tbg_algorithms[i].name) == 0) return &tbg_algorithms[i];
     set_error(TBG_ERR_UNKNOWN_ALGO, "unknown algorithm '%s'", name);
     return nullptr;
+}
+
+int tbg_set_dropin_slices(int k) {
+    std::lock_guard<std::mutex> g(g_dropin_mu);
+    const int prev = g_slices;
+    g_slices = std::max(0, std::min(k, MAX_SLICES));
+    return prev;
 }
 
 void tbg_last_transfer_bytes(uint64_t *h2d, uint64_t *d2h) {

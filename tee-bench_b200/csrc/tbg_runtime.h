@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <cuda_runtime.h>
 
 #include "tbg_internal.h"
@@ -103,6 +104,10 @@ cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_
                               cudaStream_t st);
 int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                    tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
+int run_radix_join_sliced(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, const uint64_t *s_lo,
+                          int nslices, const std::function<int(int)> &issue, cudaEvent_t r_ready,
+                          const cudaEvent_t *s_ready, tbg_row_out *d_rows, uint64_t cap, Workspace &w,
+                          cudaStream_t st, JoinRun *run);
 int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                        tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
 int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,

@@ -48,6 +48,34 @@ def test_dropin_matches_reference_default_config(tbg, oracle, golden, cuda, algo
     assert sha(oracle.sort_rows(rows)) == j["RHO_mat_sorted_sha256"]
 
 
+@pytest.mark.parametrize("algo", ["RHO", "RHT"])
+@pytest.mark.parametrize("slices", [1, 3, 16])
+def test_dropin_sliced_copies(tbg, oracle, cuda, algo, slices):
+    """The drop-in copies S in slices and joins each as it lands: same count
+    and row multiset as the oracle, including the materialising retry when
+    the output outgrows |S| (duplicate R keys) and a slice count that does
+    not divide |S|."""
+    rng = np.random.default_rng(slices)
+    R = np.zeros(300007, dtype=oracle.ROW)
+    S = np.zeros(1000003, dtype=oracle.ROW)
+    R["key"] = rng.integers(1, 100000, len(R))  # about 3 rows per key: more matches than |S|
+    S["key"] = np.minimum(rng.zipf(1.2, len(S)), 250000)
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    assert ref > len(S)
+    prev = tbg.set_dropin_slices(slices)
+    try:
+        assert tbg.find(algo).join(R, S, 2) == ref
+        c, rows = tbg.find(algo).join(R, S, 3, materialize=True)
+    finally:
+        tbg.set_dropin_slices(prev)
+    assert c == ref == len(rows)
+    assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+    h2d, _ = tbg.last_transfer_bytes()
+    assert h2d == 8 * (len(R) + len(S))
+
+
 @pytest.mark.parametrize("bits,passes", [(1, 1), (4, 1), (8, 1), (9, 2), (12, 2), (14, 2), (15, 2)])
 def test_radix_geometry(tbg, oracle, cuda, bits, passes):
     rng = np.random.default_rng(bits * 10 + passes)
