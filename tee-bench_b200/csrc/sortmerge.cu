@@ -328,11 +328,12 @@ cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_
 // Merge join of sorted R (nr) and sorted S (ns).  k_merge_splits finds, for
 // every CTA boundary c * D, the merge-path split (one thread per boundary);
 // CTA c then loads R[i_c, i_c+1) and S[j_c, j_c+1) (D rows together) into
-// shared memory, splits its D diagonals evenly over threads and walks them.
+// one shared array, each thread issuing all of its loads before its first
+// shared store, splits its D diagonals evenly over threads and walks them.
 // A run of equal R keys that continues past the tile is finished in global
 // memory.
 constexpr int MERGE_THREADS = 256;
-constexpr int MERGE_PER_THREAD = 8;
+constexpr int MERGE_PER_THREAD = 16;
 constexpr int MERGE_TILE = MERGE_THREADS * MERGE_PER_THREAD;
 
 __global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row *__restrict__ S, uint64_t ns,
@@ -352,7 +353,11 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_join(const Row *__restr
                                                                unsigned long long *matches,
                                                                unsigned long long *rows_ctr, tbg_row_out *out,
                                                                uint64_t cap) {
-    __shared__ uint64_t Rt[MERGE_TILE], St[MERGE_TILE];
+    // keys (and payloads when materialising) of the tile's R rows [0, nrt),
+    // then of its S rows; one spare slot so a walk may read one row past
+    // either side without a guard
+    __shared__ uint32_t K[MERGE_TILE + 1];
+    __shared__ uint32_t Pay[MAT ? MERGE_TILE : 1];
     __shared__ unsigned long long s_base;
     __shared__ uint64_t scan_scratch[MERGE_THREADS / 32 + 1];
     const uint64_t L = nr + ns;
@@ -361,44 +366,65 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_join(const Row *__restr
     const uint64_t ic0 = splits[c], ic1 = splits[c + 1];
     const uint64_t jc0 = dc0 - ic0, jc1 = dc1 - ic1;
     const uint32_t nrt = (uint32_t)(ic1 - ic0), nst = (uint32_t)(jc1 - jc0);
-    for (uint32_t t = threadIdx.x; t < nrt; t += MERGE_THREADS) {
-        const uint2 x = reinterpret_cast<const uint2 *>(R)[ic0 + t];
-        Rt[t] = pack_row(x.x, x.y);
-    }
-    for (uint32_t t = threadIdx.x; t < nst; t += MERGE_THREADS) {
-        const uint2 x = reinterpret_cast<const uint2 *>(S)[jc0 + t];
-        St[t] = pack_row(x.x, x.y);
+    const uint32_t Lt = nrt + nst;
+    {
+        const uint2 *Rv = reinterpret_cast<const uint2 *>(R) + ic0;
+        const uint2 *Sv = reinterpret_cast<const uint2 *>(S) + jc0;
+        uint2 x[MERGE_PER_THREAD];
+#pragma unroll
+        for (int q = 0; q < MERGE_PER_THREAD; q++) {
+            const uint32_t t = q * MERGE_THREADS + threadIdx.x;
+            if (t < Lt) x[q] = *(t < nrt ? Rv + t : Sv + (t - nrt));
+        }
+#pragma unroll
+        for (int q = 0; q < MERGE_PER_THREAD; q++) {
+            const uint32_t t = q * MERGE_THREADS + threadIdx.x;
+            if (t < Lt) {
+                K[t] = x[q].x;
+                if (MAT) Pay[t] = x[q].y;
+            }
+        }
+        if (threadIdx.x == 0) K[Lt] = 0;
     }
     __syncthreads();
-    const uint32_t Lt = nrt + nst;
+    const uint32_t *Ks = K + nrt;
     const uint32_t d0 = min(Lt, threadIdx.x * MERGE_PER_THREAD), d1 = min(Lt, d0 + MERGE_PER_THREAD);
-    auto kr = [&](uint64_t i) { return row_key(Rt[i]); };
-    auto ks = [&](uint64_t j) { return row_key(St[j]); };
-    const uint32_t i0 = (uint32_t)merge_split(d0, nrt, nst, kr, ks);
+    // merge-path split of diagonal d0 inside the tile (32-bit indices)
+    uint32_t i0;
+    {
+        uint32_t lo = d0 > nst ? d0 - nst : 0, hi = min(d0, nrt);
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (K[mid] < Ks[d0 - mid - 1]) lo = mid + 1;
+            else hi = mid;
+        }
+        i0 = lo;
+    }
     const uint32_t j0 = d0 - i0;
-    // matches of S row with key k taken at tile R position i: the run of k
+    // rows of R equal to k from tile position i on (continuing past the tile)
     auto run_len = [&](uint32_t i, uint32_t k) {
-        uint32_t n = 0;
         uint32_t q = i;
-        for (; q < nrt && row_key(Rt[q]) == k; q++) n++;
+        while (q < nrt && K[q] == k) q++;
+        uint32_t n = q - i;
         if (q == nrt)
             for (uint64_t g = ic0 + q; g < nr && R[g].key == k; g++) n++;
         return n;
     };
     uint32_t i = i0, j = j0, cnt = 0, last_key = 0, last_cnt = 0;
+    uint32_t rk = K[i], sk = Ks[j];  // current keys (a spare or foreign slot past a side's end)
     bool have = false;
     for (uint32_t d = d0; d < d1; d++) {
-        if (i < nrt && (j >= nst || row_key(Rt[i]) < row_key(St[j]))) {
-            i++;
+        if (i < nrt && (j >= nst || rk < sk)) {
+            rk = K[++i];
         } else {
-            const uint32_t k = row_key(St[j]);
-            if (!have || k != last_key) {
-                last_cnt = run_len(i, k);
-                last_key = k;
+            if (!have || sk != last_key) {
+                // i == nrt: the run may continue in the R rows past the tile
+                last_cnt = (i == nrt || rk == sk) ? run_len(i, sk) : 0;
+                last_key = sk;
                 have = true;
             }
             cnt += last_cnt;
-            j++;
+            sk = Ks[++j];
         }
     }
     if (MAT) {
@@ -410,13 +436,13 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_join(const Row *__restr
         i = i0;
         j = j0;
         for (uint32_t d = d0; d < d1; d++) {
-            if (i < nrt && (j >= nst || row_key(Rt[i]) < row_key(St[j]))) {
+            if (i < nrt && (j >= nst || K[i] < Ks[j])) {
                 i++;
             } else {
-                const uint32_t k = row_key(St[j]), sp = row_pay(St[j]);
+                const uint32_t k = Ks[j], sp = Pay[nrt + j];
                 uint32_t q = i;
-                for (; q < nrt && row_key(Rt[q]) == k; q++, pos++)
-                    if (pos < cap) out[pos] = tbg_row_out{k, row_pay(Rt[q]), sp};
+                for (; q < nrt && K[q] == k; q++, pos++)
+                    if (pos < cap) out[pos] = tbg_row_out{k, Pay[q], sp};
                 if (q == nrt)
                     for (uint64_t g = ic0 + q; g < nr && R[g].key == k; g++, pos++)
                         if (pos < cap) out[pos] = tbg_row_out{k, R[g].payload, sp};
