@@ -1,9 +1,10 @@
 // Sort-merge joins for sm_100a.
 //
 // RSM (Joins/radix_sortmerge_join.c:74-100): the radix partitions of RHO,
-// then per partition pair both sides are sorted in shared memory (a stable
-// LSD radix sort of packed (key, payload) words over the key bits that vary
-// inside the tile) and merged.  PSM
+// then per partition pair both sides are sorted in shared memory over the
+// key bits that vary inside the tile (one counting pass, or a stable LSD
+// radix sort of packed (key, payload) words when they span more than 12
+// bits) and merged.  PSM
 // (Joins/psm/parallel_sortmerge_join.h:61-111): R and S are sorted globally
 // (LSD radix sort with the one-sweep scatter of sweep.cu) and merged.
 //
@@ -17,7 +18,7 @@
 // misses; this merge counts exactly the equi-join.
 #include <algorithm>
 
-#include "tbg_device.cuh"
+#include "part_dev.cuh"
 
 namespace tbg {
 
@@ -80,14 +81,14 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
         const bool last = shift + 8 > hi;
         for (int i = tid; i < 256 * NW; i += THREADS) cnt[i] = 0;
         __syncthreads();
-        uint64_t x[ITEMS];
-        uint32_t r[ITEMS], dg[ITEMS];
+        // only the ranks stay in registers across the scan; rows and digits
+        // are read again from src for the scatter
+        uint32_t r[ITEMS];
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t e = (uint32_t)w * 32 * ITEMS + i * 32 + lane;
             const bool valid = e < n;
-            x[i] = valid ? src[e] : 0;
-            const uint32_t d = valid ? (row_key(x[i]) >> shift) & 255 : 256;
+            const uint32_t d = valid ? (row_key(src[e]) >> shift) & 255 : 256;
             const unsigned peers = warp_peers9(d);
             uint32_t base = 0;
             if (valid) base = cnt[w * 256 + d];  // warp-major: lanes with different digits hit different banks
@@ -95,7 +96,6 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
             if (valid && (peers & lanemask_lt()) == 0) cnt[w * 256 + d] = (uint16_t)(base + __popc(peers));
             __syncwarp();
             r[i] = base + __popc(peers & lanemask_lt());
-            dg[i] = d;
         }
         __syncthreads();
         // exclusive scan over (digit, warp), digit-major: thread t owns the C
@@ -115,9 +115,11 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
-            if (dg[i] < 256) {
-                const uint32_t p = cnt[w * 256 + dg[i]] + r[i];
-                dst[last ? pad16(p) : p] = x[i];
+            const uint32_t e = (uint32_t)w * 32 * ITEMS + i * 32 + lane;
+            if (e < n) {
+                const uint64_t x = src[e];
+                const uint32_t p = cnt[w * 256 + ((row_key(x) >> shift) & 255)] + r[i];
+                dst[last ? pad16(p) : p] = x;
             }
         }
         __syncthreads();
@@ -128,18 +130,107 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
     return src;
 }
 
-// Loads rows [off, off + n) (n <= THREADS * 8) into s packed and sorts them
-// by key with `tmp` as scratch; returns the buffer holding the sorted rows
-// (skewed layout).
+// Widest key field (bits) that load_sorted sorts in one counting pass.
+constexpr int COUNT_SORT_BITS = 12;
+
+// Loads rows [off, off + n) (n <= THREADS * 8) and sorts them by key; returns
+// the buffer holding the sorted rows in the skewed layout (s, or tmp after a
+// multi-pass sort).  Every thread issues its 8 loads before the first use.
+// When the key bits that vary in the tile span at most COUNT_SORT_BITS
+// (12 at the 2^27-key, 15-bit radix workloads), one counting pass sorts
+// them: ranks from shared atomics on 2^span bins kept in tmp, an exclusive
+// scan of the bins, then each row goes straight from registers to its
+// place.  Rows with equal keys then sit in no particular order, which the
+// merge does not need (a join's rows are a multiset).  Wider spans take
+// block_radix_sort.
 template <int THREADS>
 __device__ uint64_t *load_sorted(const Row *__restrict__ src, uint64_t off, uint32_t n, uint64_t *s, uint64_t *tmp,
                                  uint16_t *cnt, uint64_t *scratch, uint32_t *red) {
-    for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
-        const uint2 x = reinterpret_cast<const uint2 *>(src)[off + i];
-        s[i] = pack_row(x.x, x.y);
+    constexpr int ITEMS = 8;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint2 *v = reinterpret_cast<const uint2 *>(src) + off;
+    if (tid == 0) {
+        red[0] = 0;
+        red[1] = ~0u;
+    }
+    // tmp (sized for THREADS * 8 skewed rows) holds the payloads, parked
+    // there to free registers, and the counting pass's 2^span <= 4096 bins
+    uint32_t *c32 = reinterpret_cast<uint32_t *>(tmp);
+    uint32_t *pay = c32 + (1u << COUNT_SORT_BITS);
+    uint32_t key[ITEMS];
+    uint32_t vor = 0, vand = ~0u;
+    {
+        uint2 x[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t e = i * THREADS + tid;
+            if (e < n) x[i] = v[e];
+        }
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t e = i * THREADS + tid;
+            key[i] = x[i].x;
+            if (e < n) {
+                pay[e] = x[i].y;
+                vor |= x[i].x;
+                vand &= x[i].x;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        vor |= __shfl_xor_sync(0xffffffffu, vor, o);
+        vand &= __shfl_xor_sync(0xffffffffu, vand, o);
+    }
+    __syncthreads();  // red initialised
+    if (lane == 0) {
+        atomicOr(&red[0], vor);
+        atomicAnd(&red[1], vand);
     }
     __syncthreads();
-    return block_radix_sort<THREADS>(s, tmp, n, cnt, scratch, red);
+    const uint32_t varying = red[0] & ~red[1];
+    const int lo = varying ? __ffs(varying) - 1 : 0;
+    const int span = varying ? 32 - __clz(varying) - lo : 0;
+    if (span > COUNT_SORT_BITS) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t e = i * THREADS + tid;
+            if (e < n) s[e] = pack_row(key[i], pay[e]);
+        }
+        __syncthreads();  // also: red is reused by the sort
+        return block_radix_sort<THREADS>(s, tmp, n, cnt, scratch, red);
+    }
+    const uint32_t bins = 1u << span;
+    for (uint32_t b = tid; b < bins; b += THREADS) c32[b] = 0;
+    __syncthreads();
+    uint32_t r[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const bool valid = i * THREADS + tid < n;
+        const uint32_t d = valid ? (key[i] >> lo) & (bins - 1) : 0;
+        r[i] = rank_warp(c32, d, valid, warp_has_dups(d, valid));
+    }
+    __syncthreads();
+    {
+        // exclusive scan of the bins; thread t owns bins [t * per, (t + 1) * per)
+        const uint32_t per = (bins + THREADS - 1) / THREADS;
+        const uint32_t b0 = min(bins, tid * per), b1 = min(bins, b0 + per);
+        uint32_t sum = 0;
+        for (uint32_t b = b0; b < b1; b++) sum += c32[b];
+        uint64_t tot;
+        uint32_t run = (uint32_t)block_excl_scan<THREADS>(sum, &tot, scratch);
+        for (uint32_t b = b0; b < b1; b++) {
+            const uint32_t c = c32[b];
+            c32[b] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+        if (i * THREADS + tid < n)
+            s[pad16(c32[(key[i] >> lo) & (bins - 1)] + r[i])] = pack_row(key[i], pay[i * THREADS + tid]);
+    __syncthreads();
+    return s;
 }
 
 // Merge-path split of diagonal d over sorted arrays A (na) and B (nb):
@@ -201,29 +292,41 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
             const uint32_t L = nr + ns;
             const uint32_t per = (L + RSM_THREADS - 1) / RSM_THREADS;
             const uint32_t d0 = min(L, tid * per), d1 = min(L, d0 + per);
-            auto kr = [&](uint64_t i) { return row_key(Rs[pad16((uint32_t)i)]); };
-            auto ks = [&](uint64_t j) { return row_key(Ss[pad16((uint32_t)j)]); };
-            uint32_t i = (uint32_t)merge_split(d0, nr, ns, kr, ks);
+            auto kr = [&](uint32_t i) { return row_key(Rs[pad16(i)]); };
+            auto ks = [&](uint32_t j) { return row_key(Ss[pad16(j)]); };
+            uint32_t i;
+            {
+                uint32_t lo = d0 > ns ? d0 - ns : 0, hi = min(d0, nr);
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (kr(mid) < ks(d0 - mid - 1)) lo = mid + 1;
+                    else hi = mid;
+                }
+                i = lo;
+            }
             uint32_t j = d0 - i;
-            // pass 1: count this thread's matches
+            // pass 1: count this thread's matches.  The current keys stay in
+            // registers; at a side's end they read the padded slot past its
+            // last row (inside the buffer, never used).
             uint32_t cnt = 0;
             {
                 uint32_t ii = i, jj = j;
+                uint32_t rk = kr(ii), sk = ks(jj);
                 uint32_t last_key = 0, last_cnt = 0;
                 bool have = false;
                 for (uint32_t d = d0; d < d1; d++) {
-                    if (ii < nr && (jj >= ns || kr(ii) < ks(jj))) {
-                        ii++;
+                    if (ii < nr && (jj >= ns || rk < sk)) {
+                        rk = kr(++ii);
                     } else {
-                        const uint32_t k = ks(jj);
-                        if (!have || k != last_key) {
+                        if (!have || sk != last_key) {
                             last_cnt = 0;
-                            for (uint32_t q = ii; q < nr && kr(q) == k; q++) last_cnt++;
-                            last_key = k;
+                            if (ii < nr && rk == sk)
+                                for (uint32_t q = ii; q < nr && kr(q) == sk; q++) last_cnt++;
+                            last_key = sk;
                             have = true;
                         }
                         cnt += last_cnt;
-                        jj++;
+                        sk = ks(++jj);
                     }
                 }
             }
