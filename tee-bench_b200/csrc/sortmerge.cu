@@ -6,7 +6,7 @@
 // radix sort of packed (key, payload) words when they span more than 12
 // bits) and merged.  PSM
 // (Joins/psm/parallel_sortmerge_join.h:61-111): R and S are sorted globally
-// (LSD radix sort with the one-sweep scatter of sweep.cu) and merged.
+// (LSD radix sort with the chunked stable passes of sortpass.cu) and merged.
 //
 // The merge is a merge path (Green, McColl, Bader 2012): the merged order
 // takes R[i] before S[j] iff R[i].key < S[j].key, so when S[j] is taken every

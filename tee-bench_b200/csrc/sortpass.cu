@@ -69,7 +69,8 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
             }
         }
         const uint32_t d = valid ? (v[i].x >> shift) & (NB - 1) : NB;  // NB: the no-row sentinel
-        const unsigned peers = warp_peers_bits<DB + 1>(d);
+        // a full tile has no sentinel, so its digits need one ballot less
+        const unsigned peers = FULL ? warp_peers_bits<DB>(d) : warp_peers_bits<DB + 1>(d);
         uint32_t base = 0;
         if (valid) base = c[w * NB + d];  // warp-major: lanes with different digits hit different banks
         __syncwarp();
