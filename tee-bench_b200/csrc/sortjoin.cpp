@@ -15,7 +15,7 @@
 namespace tbg {
 
 cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaStream_t st);
-int rsm_ctas_per_sm(int capR);
+int rsm_ctas_per_sm(int capR, bool materialize);
 cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t ns, uint64_t *splits,
                               unsigned long long *matches, unsigned long long *rows_ctr, tbg_row_out *out,
                               uint64_t cap, bool mat, cudaStream_t st);
@@ -49,7 +49,8 @@ int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const 
     ja.out = d_rows;
     ja.cap = d_rows ? cap : 0;
     ja.err = &ctrl->error;
-    cudaError_t e = launch_join_rsm(ja, cfg.materialize != 0, w.nsm * rsm_ctas_per_sm(capR), st);
+    cudaError_t e =
+        launch_join_rsm(ja, cfg.materialize != 0, w.nsm * rsm_ctas_per_sm(capR, cfg.materialize != 0), st);
     if (e != cudaSuccess) return cuda_error(e, "rsm join");
     mark_ev(w, cfg.timing != 0, 4, st);
     run->timed = cfg.timing != 0;

@@ -31,19 +31,32 @@ __device__ __forceinline__ uint32_t row_pay(uint64_t x) { return (uint32_t)x; }
 __device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
 __host__ __device__ constexpr uint32_t padded_rows(uint32_t n) { return n + n / 16 + 1; }
 
-// Block-wide stable LSD radix sort of n <= THREADS * 8 packed rows by key
-// (their high 32 bits) in shared memory.  Only the key bits that differ
+// The sorts below run on packed rows (key in the high 32 bits) or on bare
+// keys (count-only RSM).  Bare keys are 4 bytes, one bank each, so their
+// skewed layout puts key i at i + i / 8 for the same effect.
+__device__ __forceinline__ uint32_t elem_key(uint64_t x) { return row_key(x); }
+__device__ __forceinline__ uint32_t elem_key(uint32_t x) { return x; }
+template <typename T>
+__device__ __forceinline__ uint32_t skew(uint32_t i) {
+    return sizeof(T) == 8 ? pad16(i) : i + (i >> 3);
+}
+template <typename T>
+__host__ __device__ constexpr uint32_t skewed_size(uint32_t n) {
+    return sizeof(T) == 8 ? padded_rows(n) : n + n / 8 + 1;
+}
+
+// Block-wide stable LSD radix sort of n <= THREADS * 8 packed rows (by their
+// high 32 bits) or bare keys in shared memory.  Only the key bits that differ
 // inside the tile are sorted, 8 per pass.  In a pass, thread (w, lane) holds
 // rows e = w * 256 + i * 32 + lane (i < 8); a row's rank counts the rows of
 // the same digit before it in that order (per-warp counters advanced slot by
 // slot, ballot-built peer masks inside a slot), so every pass is stable.  `a` holds
 // the rows, `b` is scratch for n rows, `cnt` 256 * THREADS / 32 counters,
 // `scratch` THREADS / 32 + 1 words, `red` 2 words.  `a` is read in plain
-// layout; the sorted rows are left in the skewed layout (pad16) in the
-// returned buffer, a or b, each sized padded_rows(n).
-template <int THREADS>
-__device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint16_t *cnt, uint64_t *scratch,
-                                      uint32_t *red) {
+// layout; the sorted rows are left in the skewed layout (skew<T>) in the
+// returned buffer, a or b, each sized skewed_size<T>(n).
+template <int THREADS, typename T>
+__device__ T *block_radix_sort(T *a, T *b, uint32_t n, uint16_t *cnt, uint64_t *scratch, uint32_t *red) {
     constexpr int NW = THREADS / 32, ITEMS = 8, C = 256 * NW / THREADS;
     static_assert(THREADS * ITEMS <= 65535 && 256 * NW % THREADS == 0 && NW % C == 0,
                   "16-bit counters; a thread's counters belong to one digit");
@@ -55,7 +68,7 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
     __syncthreads();
     uint32_t vor = 0, vand = ~0u;
     for (uint32_t e = tid; e < n; e += THREADS) {
-        const uint32_t k = row_key(a[e]);
+        const uint32_t k = elem_key(a[e]);
         vor |= k;
         vand &= k;
     }
@@ -70,9 +83,9 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
     __syncthreads();
     const uint32_t varying = red[0] & ~red[1];
     __syncthreads();  // red is reused by the next call
-    uint64_t *src = a, *dst = b;
+    T *src = a, *dst = b;
     if (!varying) {  // every key equal: already sorted, only the layout changes
-        for (uint32_t e = tid; e < n; e += THREADS) b[pad16(e)] = a[e];
+        for (uint32_t e = tid; e < n; e += THREADS) b[skew<T>(e)] = a[e];
         __syncthreads();
         return b;
     }
@@ -88,7 +101,7 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t e = (uint32_t)w * 32 * ITEMS + i * 32 + lane;
             const bool valid = e < n;
-            const uint32_t d = valid ? (row_key(src[e]) >> shift) & 255 : 256;
+            const uint32_t d = valid ? (elem_key(src[e]) >> shift) & 255 : 256;
             const unsigned peers = warp_peers9(d);
             uint32_t base = 0;
             if (valid) base = cnt[w * 256 + d];  // warp-major: lanes with different digits hit different banks
@@ -117,13 +130,13 @@ __device__ uint64_t *block_radix_sort(uint64_t *a, uint64_t *b, uint32_t n, uint
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t e = (uint32_t)w * 32 * ITEMS + i * 32 + lane;
             if (e < n) {
-                const uint64_t x = src[e];
-                const uint32_t p = cnt[w * 256 + ((row_key(x) >> shift) & 255)] + r[i];
-                dst[last ? pad16(p) : p] = x;
+                const T x = src[e];
+                const uint32_t p = cnt[w * 256 + ((elem_key(x) >> shift) & 255)] + r[i];
+                dst[last ? skew<T>(p) : p] = x;
             }
         }
         __syncthreads();
-        uint64_t *t = src;
+        T *t = src;
         src = dst;
         dst = t;
     }
@@ -197,7 +210,7 @@ __device__ uint64_t *load_sorted(const Row *__restrict__ src, uint64_t off, uint
             if (e < n) s[e] = pack_row(key[i], pay[e]);
         }
         __syncthreads();  // also: red is reused by the sort
-        return block_radix_sort<THREADS>(s, tmp, n, cnt, scratch, red);
+        return block_radix_sort<THREADS, uint64_t>(s, tmp, n, cnt, scratch, red);
     }
     const uint32_t bins = 1u << span;
     for (uint32_t b = tid; b < bins; b += THREADS) c32[b] = 0;
@@ -363,21 +376,216 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
     if ((tid & 31) == 0 && ws) atomicAdd(a.matches, ws);
 }
 
-int rsm_ctas_per_sm(int capR) {
+// Count-only RSM works on bare keys (4 bytes in shared memory instead of 8),
+// which leaves room to load the next S tile's keys into registers while the
+// current tile is merged.
+
+// Keys of rows [off, off + n) (n <= THREADS * 8): key[i] is row i * THREADS +
+// tid.  All loads are issued before the first use.
+template <int THREADS>
+__device__ __forceinline__ void load_keys(const Row *__restrict__ src, uint64_t off, uint32_t n, uint32_t (&key)[8]) {
+    const uint2 *v = reinterpret_cast<const uint2 *>(src) + off;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint32_t e = i * THREADS + threadIdx.x;
+        if (e < n) key[i] = __ldcs(v + e).x;
+    }
+}
+
+// Sorts the n keys held as load_keys left them into `out` (skewed 4-byte
+// layout): one counting pass when the varying bits span at most
+// COUNT_SORT_BITS, else the stable LSD sort through `tmp`.  `out` and `tmp`
+// hold skewed_size<uint32_t>(THREADS * 8) keys.
+template <int THREADS>
+__device__ void sort_keys(const uint32_t (&key)[8], uint32_t n, uint32_t *out, uint32_t *tmp, uint16_t *cnt,
+                          uint64_t *scratch, uint32_t *red) {
+    constexpr int ITEMS = 8;
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) {
+        red[0] = 0;
+        red[1] = ~0u;
+    }
+    uint32_t vor = 0, vand = ~0u;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        if (i * THREADS + tid < n) {
+            vor |= key[i];
+            vand &= key[i];
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        vor |= __shfl_xor_sync(0xffffffffu, vor, o);
+        vand &= __shfl_xor_sync(0xffffffffu, vand, o);
+    }
+    __syncthreads();  // red initialised
+    if (lane == 0) {
+        atomicOr(&red[0], vor);
+        atomicAnd(&red[1], vand);
+    }
+    __syncthreads();
+    const uint32_t varying = red[0] & ~red[1];
+    const int lo = varying ? __ffs(varying) - 1 : 0;
+    const int span = varying ? 32 - __clz(varying) - lo : 0;
+    if (span > COUNT_SORT_BITS) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++)
+            if (i * THREADS + tid < n) tmp[i * THREADS + tid] = key[i];
+        __syncthreads();  // also: red is reused by the sort
+        const uint32_t *res = block_radix_sort<THREADS, uint32_t>(tmp, out, n, cnt, scratch, red);
+        if (res != out) {
+            for (uint32_t q = tid; q < skewed_size<uint32_t>(n); q += THREADS) out[q] = res[q];
+            __syncthreads();
+        }
+        return;
+    }
+    const uint32_t bins = 1u << span;
+    uint32_t *c32 = tmp;
+    for (uint32_t b = tid; b < bins; b += THREADS) c32[b] = 0;
+    __syncthreads();
+    uint32_t r[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const bool valid = i * THREADS + tid < n;
+        const uint32_t d = valid ? (key[i] >> lo) & (bins - 1) : 0;
+        r[i] = rank_warp(c32, d, valid, warp_has_dups(d, valid));
+    }
+    __syncthreads();
+    {
+        const uint32_t per = (bins + THREADS - 1) / THREADS;
+        const uint32_t b0 = min(bins, tid * per), b1 = min(bins, b0 + per);
+        uint32_t sum = 0;
+        for (uint32_t b = b0; b < b1; b++) sum += c32[b];
+        uint64_t tot;
+        uint32_t run = (uint32_t)block_excl_scan<THREADS>(sum, &tot, scratch);
+        for (uint32_t b = b0; b < b1; b++) {
+            const uint32_t c = c32[b];
+            c32[b] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+        if (i * THREADS + tid < n) out[skew<uint32_t>(c32[(key[i] >> lo) & (bins - 1)] + r[i])] = key[i];
+    __syncthreads();
+}
+
+// Matches of this thread's share of the merge path of sorted keys A (na)
+// and B (nb), skewed 4-byte layout: B's rows count the run of equal A keys.
+template <int THREADS>
+__device__ __forceinline__ uint32_t merge_count(const uint32_t *A, uint32_t na, const uint32_t *B, uint32_t nb) {
+    const uint32_t L = na + nb;
+    const uint32_t per = (L + THREADS - 1) / THREADS;
+    const uint32_t d0 = min(L, threadIdx.x * per), d1 = min(L, d0 + per);
+    auto ka = [&](uint32_t i) { return A[skew<uint32_t>(i)]; };
+    auto kb = [&](uint32_t j) { return B[skew<uint32_t>(j)]; };
+    uint32_t lo = d0 > nb ? d0 - nb : 0, hi = min(d0, na);
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (ka(mid) < kb(d0 - mid - 1)) lo = mid + 1;
+        else hi = mid;
+    }
+    // the current keys stay in registers; at a side's end they read the
+    // padding slot past its last key (inside the buffer, never used)
+    uint32_t i = lo, j = d0 - lo;
+    uint32_t ak = ka(i), bk = kb(j);
+    uint32_t cnt = 0, last_key = 0, last_cnt = 0;
+    bool have = false;
+    for (uint32_t d = d0; d < d1; d++) {
+        if (i < na && (j >= nb || ak < bk)) {
+            ak = ka(++i);
+        } else {
+            if (!have || bk != last_key) {
+                last_cnt = 0;
+                if (i < na && ak == bk)
+                    for (uint32_t q = i; q < na && ka(q) == bk; q++) last_cnt++;
+                last_key = bk;
+                have = true;
+            }
+            cnt += last_cnt;
+            bk = kb(++j);
+        }
+    }
+    return cnt;
+}
+
+constexpr uint32_t RSM_KEYS = skewed_size<uint32_t>(RSM_STILE);
+
+size_t rsm_count_smem_bytes() { return (size_t)3 * RSM_KEYS * 4 + 256 * (RSM_THREADS / 32) * 2; }
+
+// Count-only RSM for items with r_len <= RSM_STILE: the R chunk's keys are
+// sorted once, then S tiles of RSM_STILE keys are sorted and merged against
+// them; tile k + 1's keys load while tile k merges.
+__global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t *Rk = reinterpret_cast<uint32_t *>(smem);
+    uint32_t *Sk = Rk + RSM_KEYS;
+    uint32_t *tmp = Sk + RSM_KEYS;
+    uint16_t *cnt = reinterpret_cast<uint16_t *>(tmp + RSM_KEYS);
+    __shared__ uint32_t s_item;
+    __shared__ uint64_t scan_scratch[RSM_THREADS / 32 + 1];
+    __shared__ uint32_t red[2];
+    const int tid = threadIdx.x;
+    const unsigned nitems = *a.nitems;
+    unsigned long long local = 0;
+    uint32_t key[8];
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(a.item_ctr, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= nitems) break;
+        const Item m = a.items[it];
+        const uint32_t nr = min(m.r_len, (uint32_t)RSM_STILE);  // the planner's capR is RSM_STILE
+        load_keys<RSM_THREADS>(a.R, m.r_off, nr, key);
+        sort_keys<RSM_THREADS>(key, nr, Rk, tmp, cnt, scan_scratch, red);
+        uint32_t ns = (uint32_t)umin64(RSM_STILE, m.s_len);
+        load_keys<RSM_THREADS>(a.S, m.s_off, ns, key);
+        for (uint64_t s0 = 0; s0 < m.s_len;) {
+            sort_keys<RSM_THREADS>(key, ns, Sk, tmp, cnt, scan_scratch, red);
+            const uint64_t s1 = s0 + ns;
+            const uint32_t ns_next = (uint32_t)umin64(RSM_STILE, m.s_len - s1);
+            if (ns_next) load_keys<RSM_THREADS>(a.S, m.s_off + s1, ns_next, key);  // in flight during the merge
+            local += merge_count<RSM_THREADS>(Rk, nr, Sk, ns);
+            __syncthreads();  // Sk and tmp are rewritten by the next tile
+            s0 = s1;
+            ns = ns_next;
+        }
+    }
+    const unsigned long long ws = warp_sum_u64(local);
+    if ((tid & 31) == 0 && ws) atomicAdd(a.matches, ws);
+}
+
+// Resident CTAs per SM of the RSM join kernel a launch would use.
+int rsm_ctas_per_sm(int capR, bool materialize) {
     int n = 0;
-    const size_t smem = rsm_smem_bytes(capR);
-    cudaFuncSetAttribute(k_join_rsm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_join_rsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join_rsm<false>, RSM_THREADS, smem);
+    const bool keys = !materialize && capR <= RSM_STILE;
+    const size_t smem = keys ? rsm_count_smem_bytes() : rsm_smem_bytes(capR);
+    if (keys) {
+        cudaFuncSetAttribute(k_join_rsm_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join_rsm_count, RSM_THREADS, smem);
+    } else {
+        auto kern = materialize ? k_join_rsm<true> : k_join_rsm<false>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, RSM_THREADS, smem);
+    }
     return n < 1 ? 1 : n;
 }
 
 cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaStream_t st) {
-    const size_t smem = rsm_smem_bytes(a.capR);
-    auto kern = materialize ? k_join_rsm<true> : k_join_rsm<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<grid, RSM_THREADS, smem, st>>>(a);
+    cudaError_t e;
+    if (!materialize && a.capR <= RSM_STILE) {
+        const size_t smem = rsm_count_smem_bytes();
+        if ((e = cudaFuncSetAttribute(k_join_rsm_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+            return e;
+        k_join_rsm_count<<<grid, RSM_THREADS, smem, st>>>(a);
+    } else {
+        const size_t smem = rsm_smem_bytes(a.capR);
+        auto kern = materialize ? k_join_rsm<true> : k_join_rsm<false>;
+        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return e;
+        kern<<<grid, RSM_THREADS, smem, st>>>(a);
+    }
     count_launch();
     return cudaGetLastError();
 }

@@ -212,6 +212,29 @@ def test_generators_contract(tbg, cuda):
     assert np.allclose(freq[:8], expect, rtol=0.02)
 
 
+@pytest.mark.parametrize("materialize", [False, True])
+def test_rsm_wide_key_spans(tbg, oracle, cuda, materialize):
+    """Full-range 32-bit keys: inside a radix partition the varying key bits
+    span more than the 12 a single counting pass sorts, so every tile takes
+    the stable multi-pass sort (count-only on bare keys, materialising on
+    packed rows).  Both sides hold duplicate keys."""
+    rng = np.random.default_rng(29)
+    R = np.zeros(200003, dtype=oracle.ROW)
+    S = np.zeros(700001, dtype=oracle.ROW)
+    R["key"] = rng.integers(0, 1 << 32, len(R), dtype=np.uint64).astype(np.uint32)
+    R["key"][:5000] = R["key"][5000:10000]  # duplicates in R
+    pick = R["key"][rng.integers(0, len(R), len(S))]
+    S["key"] = np.where(rng.random(len(S)) < 0.6, pick,
+                        rng.integers(0, 1 << 32, len(S), dtype=np.uint64).astype(np.uint32))
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    m, rows, _ = run_join(tbg, cuda, "RSM", R, S, materialize=materialize, cap=ref)
+    assert m == ref
+    if materialize:
+        assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+
+
 @pytest.mark.parametrize("algo", ["RSM", "PSM"])
 def test_sortmerge_duplicates_both_sides(tbg, oracle, cuda, algo):
     """Runs of equal keys on both sides, spanning merge tiles and partitions."""
