@@ -273,6 +273,11 @@ __device__ void join_ticket(const BatchArgs &a, uint32_t q, unsigned char *smem,
     t.pay = t.key + capR;
     t.heads = t.pay + capR;
     t.next = reinterpret_cast<uint16_t *>(t.heads + capR + 2);
+    t.head64 = nullptr;
+    if (J.layout == 0) {  // counts only: keys, packed heads (capR * 4 is a multiple of 8), links
+        t.head64 = reinterpret_cast<uint64_t *>(t.key + capR);
+        t.next = reinterpret_cast<uint16_t *>(t.head64 + floor_pow2(capR + 2));
+    }
     t.hs = (int)J.B;
     t.layout = (int)J.layout;
     t.hcap = floor_pow2(capR + 2);

@@ -26,6 +26,11 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     t.pay = t.key + a.capR;
     t.heads = t.pay + a.capR;
     t.next = reinterpret_cast<uint16_t *>(t.heads + a.capR + 2);
+    t.head64 = nullptr;
+    if (!MAT && a.layout == 0) {  // count only: keys, packed heads (capR * 4 is a multiple of 8), links
+        t.head64 = reinterpret_cast<uint64_t *>(t.key + a.capR);
+        t.next = reinterpret_cast<uint16_t *>(t.head64 + floor_pow2((uint32_t)a.capR + 2));
+    }
     t.hs = a.hash_shift;
     t.layout = a.layout;
     t.hcap = floor_pow2((uint32_t)a.capR + 2);

@@ -14,11 +14,19 @@ __host__ __device__ __forceinline__ uint32_t floor_pow2(uint32_t x) {
     return p;
 }
 
+// Packed bucket head of a count-only bucket-chain table: the head entry's
+// key, its 1-based row and its 1-based next link in one 64-bit word, so a
+// probe whose chain has one entry costs one shared load.
+__device__ __forceinline__ uint64_t pack_head(uint32_t key, uint32_t row1, uint32_t next1) {
+    return ((uint64_t)key << 32) | (row1 << 16) | next1;
+}
+
 struct Table {
     uint32_t *key;    // [capR]
-    uint32_t *pay;    // [capR]
+    uint32_t *pay;    // [capR] (unused with head64)
     uint32_t *heads;  // layout 0: [N] 1-based chain heads; layout 1: [Nb+1] starts, then cursors
     uint16_t *next;   // layout 0: [capR] 1-based next links
+    uint64_t *head64; // layout 0, count only (else null): [N] packed heads instead of heads
     uint32_t mask;    // bucket mask
     uint32_t hcap;    // head slots available (a power of two <= capR + 2)
     int hs;           // hash shift (radix bits already consumed)
@@ -40,7 +48,11 @@ struct Table {
     __device__ __forceinline__ uint32_t count(uint32_t k) const {
         uint32_t c = 0;
         const uint32_t b = bucket(k);
-        if (layout == 0) {
+        if (head64) {
+            const uint64_t x = head64[b];
+            c = ((x >> 16) & 0xFFFF) != 0 && (uint32_t)(x >> 32) == k;
+            for (uint32_t h = (uint32_t)x & 0xFFFF; h; h = next[h - 1]) c += (key[h - 1] == k);
+        } else if (layout == 0) {
             for (uint32_t h = heads[b]; h; h = next[h - 1]) c += (key[h - 1] == k);
         } else {
             for (uint32_t j = heads[b], e = heads[b + 1]; j < e; j++) c += (key[j] == k);
@@ -68,7 +80,29 @@ template <int THREADS, bool CG = false>
 __device__ void build_table(Table &t, const Row *__restrict__ R, uint64_t r_off, uint32_t r_len,
                             uint64_t *scan_scratch) {
     const int tid = threadIdx.x;
-    if (t.layout == 0) {
+    if (t.head64) {
+        // the same buckets and chains with packed heads: a row enters at
+        // the head of its chain by compare-and-swap, its next link being the
+        // head it displaced
+        const uint32_t N = min(next_pow2(r_len), t.hcap);
+        t.mask = N - 1;
+        for (uint32_t i = tid; i < r_len; i += THREADS) t.key[i] = ld_row<CG>(R, r_off + i).x;
+        for (uint32_t i = tid; i < N; i += THREADS) t.head64[i] = 0;
+        __syncthreads();
+        for (uint32_t i = tid; i < r_len; i += THREADS) {
+            const uint32_t k = t.key[i];
+            unsigned long long *slot = reinterpret_cast<unsigned long long *>(&t.head64[t.bucket(k)]);
+            unsigned long long old = *slot;
+            for (;;) {  // ends: each failed swap means another row entered this chain
+                const unsigned long long seen =
+                    atomicCAS(slot, old, (unsigned long long)pack_head(k, i + 1, (uint32_t)(old >> 16) & 0xFFFF));
+                if (seen == old) break;
+                old = seen;
+            }
+            t.next[i] = (uint16_t)((old >> 16) & 0xFFFF);
+        }
+        __syncthreads();
+    } else if (t.layout == 0) {
         // next_pow2(|R_p|) buckets as in the reference, at most hcap (a
         // longer average chain when capR is not a power of two)
         const uint32_t N = min(next_pow2(r_len), t.hcap);
