@@ -48,7 +48,12 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     }
     cudaError_t e;
     if (!w.side) {
-        if ((e = cudaStreamCreateWithFlags(&w.side, cudaStreamNonBlocking)) != cudaSuccess ||
+        // the learning stream gets the highest priority: its small kernels
+        // are on the critical path and would otherwise queue behind R's
+        // partitioning grids, which fill every SM
+        int least = 0, greatest = 0;
+        if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess ||
+            (e = cudaStreamCreateWithPriority(&w.side, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&w.joined, cudaEventDisableTiming)) != cudaSuccess)
             return cuda_error(e, "stream");
