@@ -65,7 +65,9 @@ cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk
 // inter-CTA waits.  hhist holds the four 8-bit digit histograms of the input:
 // 8-bit digits that are the same for every row are skipped, and when the key
 // bits that vary fit fewer 9-bit digits than the remaining 8-bit passes, the
-// sort uses 9-bit digits instead (e.g. 3 passes for 27-bit keys, not 4).
+// sort uses 9-bit digits instead (e.g. 3 passes for 27-bit keys, not 4); at
+// an equal pass count narrower digits win (4 passes of 7 bits for 28-bit
+// keys).
 int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, Workspace &w,
                      cudaStream_t st, const Row **out, int *passes) {
     const Row *src = in;
@@ -98,11 +100,16 @@ int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint
         hi_bit = 8 * p + (top ? 31 - __builtin_clz((unsigned)top) : 0);
     }
     if (lo_bit >= 0) {
+        // the fewest passes of at most 9 bits over the varying span, with the
+        // bits spread evenly (at least 7 per pass); taken when it saves a
+        // pass, or at equal passes when its digits are narrower (cheaper
+        // ranking, longer runs per digit)
         const int bits = hi_bit - lo_bit + 1;
-        const int p9 = (bits + 8) / 9;
-        if (p9 < (int)plan.size()) {
+        const int np = (bits + 8) / 9;
+        const int db = std::max(7, (bits + np - 1) / np);
+        if (np < (int)plan.size() || (np == (int)plan.size() && db < 8)) {
             plan.clear();
-            for (int i = 0; i < p9; i++) plan.push_back({(uint32_t)(lo_bit + 9 * i), 9});
+            for (int i = 0; i < np; i++) plan.push_back({(uint32_t)(lo_bit + db * i), db});
         }
     }
     for (const auto &pp : plan) {

@@ -1,4 +1,4 @@
-// One stable LSD radix-sort pass for the PSM sort (8- or 9-bit digit at
+// One stable LSD radix-sort pass for the PSM sort (7-, 8- or 9-bit digit at
 // `shift`),
 // built like the partitioning passes: CTA c owns chunk c of the input; its
 // digit cursors are base[d] + (rows of digit d in chunks before c), from the
@@ -15,7 +15,7 @@ namespace tbg {
 
 constexpr int SORT_THREADS = 512;
 
-template <int NB>  // digits per pass: 256 or 512
+template <int NB>  // digits per pass: 128, 256 or 512
 struct SortSmem {
     static constexpr int NW = SORT_THREADS / 32;
     static constexpr int T = SORT_THREADS * PART_ITEMS;
@@ -46,7 +46,8 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
                                           const TileGeo &gnext, uint2 *__restrict__ out, uint32_t out_n,
                                           uint32_t shift, SortSmem<NB> &sm, unsigned *err) {
     constexpr int NW = SortSmem<NB>::NW, C = NB * NW / SORT_THREADS, TPD = NW / C;  // TPD threads per digit
-    static_assert(NW % C == 0 && (TPD == 1 || TPD == 2), "a thread's counters belong to one digit");
+    static_assert(C >= 1 && NW % C == 0 && (TPD & (TPD - 1)) == 0 && TPD <= 32,
+                  "a thread's counters belong to one digit; a digit's threads share a warp");
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int b = k & 1;
     const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
@@ -92,7 +93,8 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
     uint32_t run = (uint32_t)block_excl_scan<SORT_THREADS, false>(sum, &dummy, sm.scan);
     const uint32_t dstart = __shfl_sync(0xffffffffu, run, lane & ~(TPD - 1));  // the digit's first offset
     uint32_t dtotal = sum;                                                     // the digit's rows in the tile
-    if (TPD == 2) dtotal += __shfl_xor_sync(0xffffffffu, sum, 1);
+#pragma unroll
+    for (int o = 1; o < TPD; o <<= 1) dtotal += __shfl_xor_sync(0xffffffffu, dtotal, o);
 #pragma unroll
     for (int q = 0; q < C; q++) {
         const uint32_t x = c[(w0 + q) * NB + dgt];
@@ -166,11 +168,17 @@ __global__ void __launch_bounds__(SORT_THREADS, 2) k_sort_pass(const Row *__rest
     }
 }
 
-// digit_bits: 8 or 9
+// digit_bits: 7, 8 or 9
 cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, const uint32_t *pre,
                              const uint32_t *totals, uint32_t shift, int digit_bits, unsigned *err, cudaStream_t st) {
     cudaError_t e;
-    if (digit_bits == 9) {
+    if (digit_bits == 7) {
+        const size_t smem = sizeof(SortSmem<128>);
+        if ((e = cudaFuncSetAttribute(k_sort_pass<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+            return e;
+        k_sort_pass<7><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);
+    } else if (digit_bits == 9) {
         const size_t smem = sizeof(SortSmem<512>);
         if ((e = cudaFuncSetAttribute(k_sort_pass<9>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
             cudaSuccess)

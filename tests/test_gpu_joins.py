@@ -212,6 +212,30 @@ def test_generators_contract(tbg, cuda):
     assert np.allclose(freq[:8], expect, rtol=0.02)
 
 
+@pytest.mark.parametrize("span", [12, 20, 21, 27, 28, 32])
+def test_psm_digit_plans(tbg, oracle, cuda, span):
+    """PSM's LSD sort picks its digits from the key bits that vary: 8-bit
+    digits, 9-bit digits when they save a pass (27 bits: 3 passes), 7-bit
+    digits at an equal pass count (20, 21, 28 bits).  Every plan must give the
+    oracle's count and rows."""
+    rng = np.random.default_rng(span)
+    hi = 1 << span
+    R = np.zeros(150001, dtype=oracle.ROW)
+    S = np.zeros(400003, dtype=oracle.ROW)
+    R["key"] = rng.integers(0, hi, len(R), dtype=np.uint64).astype(np.uint32)
+    R["key"][0] = hi - 1  # the span's top bit is set
+    pick = R["key"][rng.integers(0, len(R), len(S))]
+    S["key"] = np.where(rng.random(len(S)) < 0.7, pick, rng.integers(0, hi, len(S), dtype=np.uint64).astype(np.uint32))
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    m, _, _ = run_join(tbg, cuda, "PSM", R, S)
+    assert m == ref
+    m, rows, _ = run_join(tbg, cuda, "PSM", R, S, materialize=True, cap=ref)
+    assert m == ref
+    assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+
+
 @pytest.mark.parametrize("materialize", [False, True])
 def test_rsm_wide_key_spans(tbg, oracle, cuda, materialize):
     """Full-range 32-bit keys: inside a radix partition the varying key bits
