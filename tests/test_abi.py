@@ -97,6 +97,19 @@ def test_device_api_argument_errors(tbg):
     assert L.tbg_join_device(None, 8, 1, 8, 1, None, 0, C.byref(m), None, None) == tbg.ERR_ARG
 
 
+def test_dropin_slice_setting(tbg):
+    """tbg_set_dropin_slices returns the previous setting and clamps to
+    0 (automatic) .. 16; it needs no device."""
+    prev = tbg.set_dropin_slices(3)
+    try:
+        assert tbg.set_dropin_slices(40) == 3
+        assert tbg.set_dropin_slices(-5) == 16
+        assert tbg.set_dropin_slices(1) == 0
+        assert tbg.set_dropin_slices(0) == 1
+    finally:
+        tbg.set_dropin_slices(prev)
+
+
 def test_dropin_without_gpu_returns_status(tbg):
     try:
         import torch
