@@ -431,7 +431,28 @@ int radix_join_phase(const tbg_config &cfg, tbg_row_out *d_rows, uint64_t cap, W
     ja.out = d_rows;
     ja.cap = d_rows ? cap : 0;
     ja.err = &ctrl->error;
-    cudaError_t e = launch_join(ja, cfg.materialize != 0, join_grid, st);
+    ja.gate = nullptr;
+    ja.gate_max = 0;
+    ja.gate_le = 0;
+    cudaError_t e;
+    if (!cfg.materialize && capR == JOIN_CAPR_DEFAULT) {
+        // Counting with 4096-row tables takes less shared memory per CTA and
+        // is faster, but only fits when no R partition is larger; that size
+        // is known on the device only (the planner's max_part_R).  So both
+        // table sizes are launched, each gated on it: one does the join, the
+        // other returns at once, and no host read-back is needed.
+        JoinArgs small = ja;
+        small.capR = JOIN_CAPR_SMALL;
+        small.gate = &ctrl->max_part_R;
+        small.gate_max = JOIN_CAPR_SMALL;
+        small.gate_le = 1;
+        if ((e = launch_join(small, false, w.nsm * join_ctas_per_sm(JOIN_CAPR_SMALL), st)) != cudaSuccess)
+            return cuda_error(e, "join");
+        ja.gate = small.gate;
+        ja.gate_max = JOIN_CAPR_SMALL;
+        ja.gate_le = 0;
+    }
+    e = launch_join(ja, cfg.materialize != 0, join_grid, st);
     if (e != cudaSuccess) return cuda_error(e, "join");
     mark(w, cfg.timing != 0, 4, st);
     run->timed = cfg.timing != 0;

@@ -21,6 +21,10 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t s_item[2];
     __shared__ uint64_t scan_scratch[JOIN_THREADS / 32 + 1];
+    if (a.gate) {  // the same value for every thread: the whole launch steps aside
+        const unsigned long long v = *a.gate;
+        if (a.gate_le ? v > a.gate_max : v <= a.gate_max) return;
+    }
     Table t;
     t.key = reinterpret_cast<uint32_t *>(smem);
     t.pay = t.key + a.capR;

@@ -55,6 +55,7 @@ constexpr int PART_ITEMS = 8;
 // Shared-memory table capacity of the build/probe kernels (rows of R_p).
 constexpr int JOIN_THREADS = 512;
 constexpr int JOIN_CAPR_DEFAULT = 5120;
+constexpr int JOIN_CAPR_SMALL = 4096;  // count-only tables when every R partition fits it
 
 // Bounded device waits: iterations before a wait gives up with TBG_ERR_TIMEOUT.
 constexpr unsigned int SPIN_LIMIT = 1u << 21;
@@ -116,6 +117,11 @@ struct JoinArgs {
     int capR;
     int hash_shift;
     int layout;                // 0 bucket chain, 1 histogram (RHT)
+    // Launch gate: with `gate` set, the launch does its work only when
+    // *gate <= gate_max (gate_le != 0) or *gate > gate_max (gate_le == 0).
+    const unsigned long long *gate;
+    unsigned long long gate_max;
+    int gate_le;
     unsigned long long *matches;
     unsigned long long *rows_ctr;
     tbg_row_out *out;

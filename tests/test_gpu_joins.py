@@ -212,6 +212,27 @@ def test_generators_contract(tbg, cuda):
     assert np.allclose(freq[:8], expect, rtol=0.02)
 
 
+@pytest.mark.parametrize("algo", ["RHO", "RHT"])
+@pytest.mark.parametrize("bits", [3, 4])
+def test_join_table_size_gate(tbg, oracle, cuda, algo, bits):
+    """Counting joins launch a 4096-row and a 5120-row table kernel, each
+    gated on the largest R partition: 3 radix bits over 36000 keys give
+    partitions of about 4500 rows (the 5120-row kernel runs), 4 bits about
+    2250 (the 4096-row kernel runs).  Both running would double the count."""
+    rng = np.random.default_rng(bits)
+    R = np.zeros(36000, dtype=oracle.ROW)
+    S = np.zeros(300007, dtype=oracle.ROW)
+    R["key"] = rng.integers(0, 1 << 30, len(R), dtype=np.uint64).astype(np.uint32)
+    S["key"] = np.where(rng.random(len(S)) < 0.8, R["key"][rng.integers(0, len(R), len(S))],
+                        rng.integers(0, 1 << 30, len(S), dtype=np.uint64).astype(np.uint32))
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref = oracle.rho(R, S)
+    m, _, st = run_join(tbg, cuda, algo, R, S, radix_bits=bits)
+    assert m == ref
+    assert (st.max_part_R > 4096) == (bits == 3)
+
+
 @pytest.mark.parametrize("span", [12, 20, 21, 27, 28, 32])
 def test_psm_digit_plans(tbg, oracle, cuda, span):
     """PSM's LSD sort picks its digits from the key bits that vary: 8-bit
