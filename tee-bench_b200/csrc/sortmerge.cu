@@ -556,24 +556,26 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
 }
 
 // Resident CTAs per SM of the RSM join kernel a launch would use.
+// RSM's planner caps R chunks at RSM_STILE rows, so counting joins always
+// take the bare-key kernel and k_join_rsm runs materialising only.
 int rsm_ctas_per_sm(int capR, bool materialize) {
     int n = 0;
-    const bool keys = !materialize && capR <= RSM_STILE;
-    const size_t smem = keys ? rsm_count_smem_bytes() : rsm_smem_bytes(capR);
-    if (keys) {
+    if (!materialize) {
+        const size_t smem = rsm_count_smem_bytes();
         cudaFuncSetAttribute(k_join_rsm_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join_rsm_count, RSM_THREADS, smem);
     } else {
-        auto kern = materialize ? k_join_rsm<true> : k_join_rsm<false>;
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, RSM_THREADS, smem);
+        const size_t smem = rsm_smem_bytes(capR);
+        cudaFuncSetAttribute(k_join_rsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join_rsm<true>, RSM_THREADS, smem);
     }
     return n < 1 ? 1 : n;
 }
 
 cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaStream_t st) {
+    if (a.capR > RSM_STILE) return cudaErrorInvalidValue;  // one shared-memory tile of R per item
     cudaError_t e;
-    if (!materialize && a.capR <= RSM_STILE) {
+    if (!materialize) {
         const size_t smem = rsm_count_smem_bytes();
         if ((e = cudaFuncSetAttribute(k_join_rsm_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
             cudaSuccess)
@@ -581,10 +583,10 @@ cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaS
         k_join_rsm_count<<<grid, RSM_THREADS, smem, st>>>(a);
     } else {
         const size_t smem = rsm_smem_bytes(a.capR);
-        auto kern = materialize ? k_join_rsm<true> : k_join_rsm<false>;
-        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        if ((e = cudaFuncSetAttribute(k_join_rsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
             return e;
-        kern<<<grid, RSM_THREADS, smem, st>>>(a);
+        k_join_rsm<true><<<grid, RSM_THREADS, smem, st>>>(a);
     }
     count_launch();
     return cudaGetLastError();
