@@ -2,7 +2,7 @@
  * tbg.h -- C ABI of tee-bench-b200, a B200 (sm_100a) implementation of the
  * TEEbench equi-join hot path: the radix hash join RHO, its histogram sibling
  * RHT, the sort-merge joins RSM and PSM, and LRN, a learned skew-aware
- * range-partitioned join.
+ * join whose model picks heavy keys that bypass radix partitioning.
  *
  * Two layers:
  *
@@ -99,7 +99,8 @@ enum {
  *   RHT  Joins/radix_join.h:23-24      (radix join, histogram table)
  *   RSM  Joins/radix_sortmerge_join.h:4 (radix partitions, sort-merge join)
  *   PSM  Joins/psm/parallel_sortmerge_join.h:61 (global sort, merge join)
- *   LRN  new: learned range partitioning with heavy-key handling, same result
+ *   LRN  new: radix join whose learned model picks heavy keys that skip
+ *        partitioning (joined during S's histogram read), same result
  * totalresults is the exact equi-join cardinality for every algorithm.  The
  * *_mat variants also fill resultlist[t].results with nresults rows each (the
  * JOIN_MATERIALIZE layout of Joins/radix_join.c:1195-1199), NULL-terminated.

@@ -28,6 +28,20 @@ namespace tbg {
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(unsigned n) { g_launches += n; }
 
+cudaError_t smem_limit(const void *func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> set;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(mu);
+    size_t &cur = set[std::make_pair(dev, func)];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 // ---------------------------------------------------------------- errors
 static thread_local int t_err = TBG_OK;
 static thread_local char t_msg[512] = "";

@@ -350,12 +350,20 @@ size_t batch_smem_bytes() {
     return s;
 }
 
-int batch_ctas_per_sm() {
-    int n = 0;
+cudaError_t batch_occupancy(int *per_sm) {
     const size_t smem = batch_smem_bytes();
-    cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch, BATCH_THREADS, smem);
-    return n < 1 ? 1 : n;
+    int n = 0;
+    cudaError_t e = smem_limit((const void *)k_batch, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch, BATCH_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    *per_sm = n < 1 ? 1 : n;
+    return cudaSuccess;
+}
+
+int batch_ctas_per_sm() {
+    int n = 1;
+    if (batch_occupancy(&n) != cudaSuccess) cudaGetLastError();
+    return n;
 }
 
 // batch_ctas_per_sm() (called when a plan is made, outside any stream

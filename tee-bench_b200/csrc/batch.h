@@ -65,6 +65,9 @@ struct BatchArgs {
 
 size_t batch_smem_bytes();
 int batch_ctas_per_sm();
+// Sets k_batch's shared-memory limit on the current device and returns its
+// resident CTAs per SM; the status of both CUDA calls is returned.
+cudaError_t batch_occupancy(int *per_sm);
 cudaError_t launch_batch(const BatchArgs &a, int grid, cudaStream_t st);
 
 }  // namespace tbg

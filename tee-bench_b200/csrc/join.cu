@@ -12,6 +12,9 @@
 // JOIN_THREADS * 8 probe rows) and places them in (row slot, lane) order, so
 // consecutive lanes store consecutive rows (the reference's insert_output,
 // Include/util.c:20-29, mallocs one node per row).
+#include <map>
+#include <mutex>
+
 #include "join_dev.cuh"
 
 namespace tbg {
@@ -131,19 +134,32 @@ size_t join_smem_bytes(int capR) {
     return (size_t)capR * 4 * 2 + ((size_t)capR + 2) * 4 + (size_t)capR * 2 + 16;
 }
 
+// Resident CTAs per SM at a table of capR rows, cached per (device, capR):
+// the occupancy query runs once per size.
 int join_ctas_per_sm(int capR) {
-    int n = 0;
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find(std::make_pair(dev, capR));
+    if (it != cache.end()) return it->second;
     const size_t smem = join_smem_bytes(capR);
-    cudaFuncSetAttribute(k_join<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_join<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join<false>, JOIN_THREADS, smem);
-    return n < 1 ? 1 : n;
+    int n = 0;
+    if (smem_limit((const void *)k_join<false>, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join<false>, JOIN_THREADS, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;  // not cached: a later call retries
+    }
+    n = n < 1 ? 1 : n;
+    cache[std::make_pair(dev, capR)] = n;
+    return n;
 }
 
 cudaError_t launch_join(const JoinArgs &a, bool materialize, int grid, cudaStream_t st) {
     const size_t smem = join_smem_bytes(a.capR);
     auto kern = materialize ? k_join<true> : k_join<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     kern<<<grid, JOIN_THREADS, smem, st>>>(a);
     count_launch();

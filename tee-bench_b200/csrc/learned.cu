@@ -247,7 +247,7 @@ cudaError_t launch_mlp_grad(const float *params, const float *xs, const float *y
     if (e == cudaSuccess) e = cudaMemsetAsync(loss_sum, 0, 4, st);
     if (e != cudaSuccess || n == 0) return e;
     const size_t smem = mlp_grad_smem();
-    e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = smem_limit((const void *)k_mlp_grad, smem);
     if (e != cudaSuccess) return e;
     k_mlp_grad<<<(n + MLP_BATCH_CTA - 1) / MLP_BATCH_CTA, MLP_BATCH_CTA, smem, st>>>(params, xs, ys, n, grad, loss_sum);
     count_launch();
@@ -258,7 +258,7 @@ cudaError_t launch_mlp_train(const float *xs, const float *ys, uint32_t n, float
                              uint64_t seed, cudaStream_t st) {
     if (n == 0 || steps <= 0) return cudaSuccess;
     const size_t smem = mlp_train_smem();
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_mlp_train, smem);
     if (e != cudaSuccess) return e;
     k_mlp_train<<<MLP_CLUSTER, MLP_BATCH_CTA, smem, st>>>(xs, ys, n, params, steps, lr, seed);
     count_launch();
@@ -516,8 +516,8 @@ cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const
     if (!n) return cudaSuccess;
     const unsigned g = (unsigned)umin64((n + 511) / 512, (uint64_t)nsm * 4);
     const size_t smem = (size_t)HEAVY_CAP * 8 + (1 << FILTER_LOG2) / 8;
-    cudaError_t e = cudaFuncSetAttribute(k_heavy_r<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_heavy_r<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_heavy_r<0>, smem);
+    if (e == cudaSuccess) e = smem_limit((const void *)k_heavy_r<1>, smem);
     if (e != cudaSuccess) return e;
     if (stage == 0) {
         k_heavy_r<0><<<g, 512, smem, st>>>(R, n, keys, filter, cnt, nullptr, nullptr, nullptr);
@@ -651,7 +651,7 @@ size_t bypass_smem(int nbins, bool mat) {
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st) {
     const size_t smem = bypass_smem(a.nbins, mat);
     auto kern = mat ? k_hist_bypass<true> : k_hist_bypass<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     kern<<<a.G, 1024, smem, st>>>(a);
     count_launch();

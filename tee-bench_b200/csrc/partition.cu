@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass2(PartArgs a) {
 int hist_ctas_per_sm(int P_log2) {
     const size_t smem = ((size_t)1 << P_log2) * 4;
     int n = 0;
-    cudaFuncSetAttribute(k_hist_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_limit((const void *)k_hist_chunks, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_hist_chunks, HIST_THREADS, smem);
     return n < 1 ? 1 : n;
 }
@@ -345,7 +345,7 @@ cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G,
                                int P_log2, RadixF rf, cudaStream_t st) {
     const int nbins = 1 << P_log2;
     const size_t smem = (size_t)nbins * 4;
-    cudaError_t e = cudaFuncSetAttribute(k_hist_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_hist_chunks, smem);
     if (e != cudaSuccess) return e;
     k_hist_chunks<<<G, HIST_THREADS, smem, st>>>(in, n, chunk, hist, nbins, rf);
     count_launch();
@@ -362,7 +362,7 @@ cudaError_t launch_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2
                               cudaStream_t st) {
     const int P = 1 << P_log2;
     const size_t smem = (size_t)(P + P / 32 + 1) * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute(k_plan_bases, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_plan_bases, smem);
     if (e != cudaSuccess) return e;
     k_plan_bases<<<1, PLAN_THREADS, smem, st>>>(totals, base, P_log2, maxp);
     count_launch();
@@ -377,7 +377,7 @@ cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st) {
 
 cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st) {
     const size_t smem = sizeof(PartSmem<PART_THREADS>);
-    cudaError_t e = cudaFuncSetAttribute(k_part_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_part_pass1, smem);
     if (e != cudaSuccess) return e;
     k_part_pass1<<<a.G, PART_THREADS, smem, st>>>(a);
     count_launch();
@@ -386,7 +386,7 @@ cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st) {
 
 cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st) {
     const size_t smem = sizeof(PartSmem<PART_THREADS>);
-    cudaError_t e = cudaFuncSetAttribute(k_part_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_part_pass2, smem);
     if (e != cudaSuccess) return e;
     const uint64_t units = (uint64_t)((a.G + a.group - 1) / a.group) << a.b1;
     k_part_pass2<<<(unsigned)units, PART_THREADS, smem, st>>>(a);

@@ -562,11 +562,11 @@ int rsm_ctas_per_sm(int capR, bool materialize) {
     int n = 0;
     if (!materialize) {
         const size_t smem = rsm_count_smem_bytes();
-        cudaFuncSetAttribute(k_join_rsm_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        smem_limit((const void *)k_join_rsm_count, smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join_rsm_count, RSM_THREADS, smem);
     } else {
         const size_t smem = rsm_smem_bytes(capR);
-        cudaFuncSetAttribute(k_join_rsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        smem_limit((const void *)k_join_rsm<true>, smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join_rsm<true>, RSM_THREADS, smem);
     }
     return n < 1 ? 1 : n;
@@ -577,13 +577,13 @@ cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaS
     cudaError_t e;
     if (!materialize) {
         const size_t smem = rsm_count_smem_bytes();
-        if ((e = cudaFuncSetAttribute(k_join_rsm_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        if ((e = smem_limit((const void *)k_join_rsm_count, smem)) !=
             cudaSuccess)
             return e;
         k_join_rsm_count<<<grid, RSM_THREADS, smem, st>>>(a);
     } else {
         const size_t smem = rsm_smem_bytes(a.capR);
-        if ((e = cudaFuncSetAttribute(k_join_rsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        if ((e = smem_limit((const void *)k_join_rsm<true>, smem)) !=
             cudaSuccess)
             return e;
         k_join_rsm<true><<<grid, RSM_THREADS, smem, st>>>(a);

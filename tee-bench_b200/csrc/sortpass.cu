@@ -174,19 +174,19 @@ cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk
     cudaError_t e;
     if (digit_bits == 7) {
         const size_t smem = sizeof(SortSmem<128>);
-        if ((e = cudaFuncSetAttribute(k_sort_pass<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        if ((e = smem_limit((const void *)k_sort_pass<7>, smem)) !=
             cudaSuccess)
             return e;
         k_sort_pass<7><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);
     } else if (digit_bits == 9) {
         const size_t smem = sizeof(SortSmem<512>);
-        if ((e = cudaFuncSetAttribute(k_sort_pass<9>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        if ((e = smem_limit((const void *)k_sort_pass<9>, smem)) !=
             cudaSuccess)
             return e;
         k_sort_pass<9><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);
     } else {
         const size_t smem = sizeof(SortSmem<256>);
-        if ((e = cudaFuncSetAttribute(k_sort_pass<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        if ((e = smem_limit((const void *)k_sort_pass<8>, smem)) !=
             cudaSuccess)
             return e;
         k_sort_pass<8><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);

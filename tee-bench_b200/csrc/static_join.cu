@@ -113,29 +113,33 @@ __global__ void __launch_bounds__(256) k_static_plan(StaticPlan p) {
 }
 
 struct StaticDevice {
-    std::once_flag once;
-    cudaError_t setup = cudaSuccess;
+    bool ok = false;
     unsigned char *scratch = nullptr;
     int grid = 0;
 };
+std::mutex g_static_mu;
 StaticDevice g_static_dev[64];
 
-// Once per device, with that device current: the scratch's device address
-// and the persistent kernel's grid.
-StaticDevice *static_device(int dev) {
-    if (dev < 0 || dev >= 64) return nullptr;
+// With device `dev` current: the scratch's device address (from
+// cudaGetSymbolAddress) and the persistent kernel's grid, whose set-up also
+// raises k_batch's shared-memory limit on this device.  Only a successful
+// set-up is kept; after a failure the next call on the device tries again.
+cudaError_t static_device(int dev, StaticDevice *out) {
+    std::lock_guard<std::mutex> g(g_static_mu);
     StaticDevice &d = g_static_dev[dev];
-    std::call_once(d.once, [&d, dev] {
+    if (!d.ok) {
         void *ptr = nullptr;
-        d.setup = cudaGetSymbolAddress(&ptr, g_static_scratch);
-        if (d.setup != cudaSuccess) return;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess) return e;
+        int nsm = 0, per_sm = 0;
+        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = batch_occupancy(&per_sm)) != cudaSuccess) return e;
         d.scratch = static_cast<unsigned char *>(ptr);
-        int nsm = 0;
-        d.setup = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (d.setup != cudaSuccess) return;
-        d.grid = nsm * batch_ctas_per_sm();
-    });
-    return &d;
+        d.grid = nsm * per_sm;
+        d.ok = true;
+    }
+    *out = d;
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -159,9 +163,13 @@ extern "C" TBG_API int tbg_join_count_static(const row_t *dR, uint64_t nR, const
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
-    StaticDevice *sd = static_device(dev);
-    if (!sd) return set_error(TBG_ERR_ARG, "tbg_join_count_static: device index %d out of range", dev);
-    if (sd->setup != cudaSuccess) return cuda_error(sd->setup, "tbg_join_count_static: set-up");
+    if (dev < 0 || dev >= 64) return set_error(TBG_ERR_ARG, "tbg_join_count_static: device index %d out of range", dev);
+    StaticDevice sdev;
+    if ((e = static_device(dev, &sdev)) != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_error(e, "tbg_join_count_static: set-up");
+    }
+    const StaticDevice *sd = &sdev;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned char *b = sd->scratch;
     if (nR == 0 || nS == 0) {

@@ -192,7 +192,7 @@ cudaError_t launch_scatter(const ScatterArgs &a, uint64_t max_tiles, cudaStream_
     static bool attr_done = false;
     const size_t smem = scatter_smem_bytes();
     if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = smem_limit((const void *)k_scatter, smem);
         if (e != cudaSuccess) return e;
         attr_done = true;
     }

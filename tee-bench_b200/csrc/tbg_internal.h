@@ -165,4 +165,12 @@ cudaError_t launch_checksum(const tbg_row_out *rows, uint64_t n, unsigned long l
 // Counts kernel launches made by this library (reported by tbg_kernel_launches).
 void count_launch(unsigned n = 1);
 
+// Makes `bytes` of dynamic shared memory launchable for kernel `func` on the
+// current device.  The limit is process-wide and shared by every host thread,
+// so it is only ever raised (under a lock, to the largest size asked for so
+// far): a launch that asks for less than the limit stays valid, and one
+// thread's smaller launch never lowers the limit under another thread's
+// larger one.
+cudaError_t smem_limit(const void *func, size_t bytes);
+
 }  // namespace tbg

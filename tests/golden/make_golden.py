@@ -90,7 +90,7 @@ def isolated_join(algo, R, S, nt):
 
 def main():
     if O.ref() is None:
-        raise SystemExit("oracle/_ref/libtbref.so missing: run `make -C oracle` where the reference tree exists")
+        raise SystemExit("oracle/_ref/libtbref.so missing: run `make -C oracle REF=<reference source tree>`")
     out = {"payload_policy": "R.payload = i*2654435761 mod 2^32, S.payload = i",
            "generators": [], "joins": []}
     for kind, n, maxid, z, seed in GEN_CASES:

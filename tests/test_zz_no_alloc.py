@@ -1,6 +1,7 @@
 """tbg_join_count_static, the join count that allocates no device memory:
-checked against the existing device entry point (tbg_join_device, RHO) on
-the same relations, over consecutive calls that share its static scratch.
+checked against the existing device entry point (tbg_join_device, RHO) and
+against the equi-join count computed on the host (numpy) on the same
+relations, over consecutive calls that share its static scratch.
 The file name makes pytest collect it last; it also passes alone in a fresh
 process."""
 from __future__ import annotations
@@ -30,6 +31,16 @@ def _rel(keys, rs):
     return r
 
 
+def host_count(R, S):
+    """Equi-join cardinality: for every S row, the R rows with its key."""
+    keys, mult = np.unique(R["key"], return_counts=True)
+    if len(keys) == 0:
+        return 0
+    pos = np.minimum(np.searchsorted(keys, S["key"]), len(keys) - 1)
+    hit = keys[pos] == S["key"]
+    return int(mult[pos][hit].sum())
+
+
 def _cases():
     rs = np.random.RandomState(2024)
     out = []
@@ -42,6 +53,18 @@ def _cases():
     # the largest accepted input
     nR = 1 << 20
     out.append((_rel(rs.permutation(nR) + 1, rs), _rel(rs.randint(1, nR + 5000, MAX_ROWS - nR), rs)))
+    # 2^21 / 2^21: 256 radix partitions of about 8192 R rows, about half of
+    # them larger than one shared-memory table, so R is built in slices and
+    # S probed once per slice
+    n = 1 << 21
+    out.append((_rel(rs.permutation(n) + 1, rs), _rel(rs.randint(1, n + 1, n), rs)))
+    # skewed R: one key repeated 12000 times (its partition alone exceeds a
+    # table) and S hitting it often
+    kR = rs.randint(1, 300000, 400000)
+    kR[:12000] = 4242
+    kS = rs.randint(1, 320000, 600000)
+    kS[:64] = 4242
+    out.append((_rel(kR, rs), _rel(kS, rs)))
     return out
 
 
@@ -57,6 +80,7 @@ def test_static_join_matches_device_join(tbg, cuda):
         tS, pS = to_dev(torch, S)
         rc, want, _ = tbg.join_device(tbg.config("RHO"), pR, len(R), pS, len(S), stream=st)
         assert rc == tbg.OK
+        assert want == host_count(R, S)
         for _ in range(2):  # two calls in a row on the same inputs
             cnt.fill_(-1)
             status.fill_(77)
