@@ -185,6 +185,10 @@ class ClockSampler:
                  "-lms", str(self.interval_ms)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._th = threading.Thread(target=self._read, daemon=True)
             self._th.start()
+            # the timed region starts once nvidia-smi streams (at most 3 s)
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 3.0 and self._proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self._proc = None
         return self
@@ -212,60 +216,6 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- CPU
-def host_workload(wl, nS_sample, seed=1):
-    """Host copy of the workload for the CPU reference: R a permutation of
-    1..|R|, S a bounded sample drawn like the GPU generator's S."""
-    algo, lr, ls, kind, param, _ = wl_spec(wl)
-    nR = 1 << lr
-    rng = np.random.default_rng(seed)
-    R = np.zeros(nR, dtype=[("key", "<u4"), ("payload", "<u4")])
-    R["key"] = rng.permutation(nR).astype(np.uint32) + 1
-    R["payload"] = np.arange(nR, dtype=np.uint32)
-    S = np.zeros(nS_sample, dtype=R.dtype)
-    if kind == "fk":
-        maxid = nR * 100 // int(param)
-        S["key"] = (rng.permutation(maxid)[:nS_sample] % (1 << 32)).astype(np.uint32) + 1 \
-            if nS_sample <= maxid else rng.integers(1, maxid + 1, nS_sample).astype(np.uint32)
-    else:
-        ranks = rng.zipf(param, nS_sample * 2) if param > 1 else None
-        if ranks is None:  # numpy's zipf needs a > 1: inverse-CDF over the alphabet
-            w = 1.0 / np.arange(1, nR + 1) ** param
-            c = np.cumsum(w)
-            c /= c[-1]
-            S["key"] = (np.searchsorted(c, rng.random(nS_sample)) + 1).astype(np.uint32)
-        else:
-            r = ranks[ranks <= nR][:nS_sample]
-            S["key"][: len(r)] = r.astype(np.uint32)
-    S["payload"] = np.arange(nS_sample, dtype=np.uint32)
-    return R, S
-
-
-def cpu_reference_run(wl, nS_sample, steps, warmup, threads):
-    """Times the reference's own RHO (oracle/_ref) on the host."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    if O.ref() is None:
-        return None, "oracle/_ref/libtbref.so not built"
-    algo, _, _, _, _, over = wl_spec(wl)
-    mat = bool(over.get("materialize"))
-    if mat:  # the reference materialises one malloc'd node per row: keep the sample modest
-        nS_sample = min(nS_sample, 1 << 26)
-    R, S = host_workload(wl, nS_sample)
-    ref_algo = algo if algo in ("RHO", "RHT", "RSM", "PSM") else "RHO"
-    times = []
-    counts = []
-    for i in range(warmup + steps):
-        t0 = time.perf_counter()
-        c, _, rt_us = O.ref_join(ref_algo, R, S, nthreads=threads, materialize=mat)
-        wall = time.perf_counter() - t0
-        if i >= warmup:
-            times.append(rt_us * 1e-6 if rt_us and rt_us > 0 else wall)
-            counts.append(c)
-    t = statistics.median(times)
-    return {"value": (len(R) + len(S)) / t / 1e6, "seconds_per_step": t, "count": counts[-1],
-            "nR": len(R), "nS": len(S), "algo": ref_algo + ("_mat" if mat else "")}, None
-
-
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -273,7 +223,206 @@ def host_threads():
         return os.cpu_count() or 1
 
 
+def host_cpu():
+    """lscpu model, physical cores and logical CPUs this process may use."""
+    info = {"model": None, "physical_cores": None, "logical_cpus": host_threads()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=30).stdout
+        kv = {}
+        for line in out.splitlines():
+            if ":" in line:
+                k, v = line.split(":", 1)
+                kv[k.strip()] = v.strip()
+        info["model"] = kv.get("Model name")
+        cps, sockets = int(kv.get("Core(s) per socket", "0")), int(kv.get("Socket(s)", "0"))
+        tpc = int(kv.get("Thread(s) per core", "1") or 1)
+        phys = cps * sockets
+        if phys:  # cores whose threads this process may use
+            info["physical_cores"] = max(1, min(phys, info["logical_cpus"] // max(tpc, 1)))
+    except (OSError, ValueError, subprocess.SubprocessError):
+        pass
+    if not info["physical_cores"]:
+        info["physical_cores"] = info["logical_cpus"]
+    return info
+
+
+def reference_inputs(wl, nR, nS, zipf_sample):
+    """Inputs of the reference arm, made by the reference's own generators
+    (oracle/_ref, App/Lib/generator.cpp): R = create_relation_pk(|R|) with
+    seed 11111, S = create_relation_fk(|S|, maxid) or create_relation_fk_sel
+    with seed 22222 (native.cpp:63-64, :113), payloads = row index.  Zipf S
+    is drawn by inverse CDF over R's keys (rank = key) on a bounded sample
+    of zipf_sample rows: the reference's own Zipf generator needs minutes at
+    these sizes.  Returns (R, S, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    _, _, _, kind, param, _ = wl_spec(wl)
+    O.ref_seed(11111)
+    R = O.ref_gen("pk", nR)
+    R["payload"] = np.arange(nR, dtype=np.uint32)
+    if kind == "fk":
+        O.ref_seed(22222)
+        if int(param) == 100:
+            S = O.ref_gen("fk", nS, nR)
+            how = f"create_relation_fk(|S|={nS}, maxid={nR})"
+        else:
+            maxid = nR * 100 // int(param)
+            S = O.ref_gen("fk_sel", nS, maxid)
+            how = f"create_relation_fk_sel(|S|={nS}, maxid={maxid})"
+    else:
+        n = min(nS, zipf_sample)
+        rng = np.random.default_rng(22222)
+        w = 1.0 / np.arange(1, nR + 1, dtype=np.float64) ** float(param)
+        cdf = np.cumsum(w)
+        cdf /= cdf[-1]
+        S = np.zeros(n, dtype=R.dtype)
+        S["key"] = (np.searchsorted(cdf, rng.random(n)) + 1).astype(np.uint32)
+        how = f"Zipf z={param} over R's keys by inverse CDF, a sample of {n} rows"
+    S["payload"] = np.arange(len(S), dtype=np.uint32)
+    return R, S, f"create_relation_pk(|R|={nR}) + " + how + " (the reference's generators, seeds 11111 / 22222)"
+
+
+def cpu_reference_run(R, S, algo, steps, warmup, threads, materialize=False):
+    """Times the reference's own join (oracle/_ref) on the host: warm-up
+    calls, then `steps` calls; each call joins fresh private copies of R and
+    S (the reference clobbers its inputs), timed by its own Total Runtime.
+    Returns the median seconds per join, every timing and the last count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    times, count = [], None
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        c, _, rt_us = O.ref_join(algo, R, S, nthreads=threads, materialize=materialize)
+        wall = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(rt_us * 1e-6 if rt_us and rt_us > 0 else wall)
+        count = c
+    return statistics.median(times), times, count
+
+
+def reference_available():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O.ref() is not None
+
+
+def cpu_baseline_leg(R, S, algo, materialize, reps=3):
+    """The reference's join on this host's cores at the physical core count
+    and at the logical CPU count, median of `reps` calls each (plus one
+    warm-up).  R and S are the workload's own rows (or a stated sample)."""
+    cpu = host_cpu()
+    runs = {}
+    for label, th in (("physical", cpu["physical_cores"]), ("logical", cpu["logical_cpus"])):
+        if label == "logical" and th == cpu["physical_cores"] and "physical" in runs:
+            runs[label] = dict(runs["physical"])
+            continue
+        t, ts, c = cpu_reference_run(R, S, algo, reps, 1, th, materialize)
+        runs[label] = {"threads": th, "median_s": t, "runs_s": ts, "count": c,
+                       "Mtuples_s": (len(R) + len(S)) / t / 1e6}
+    best = max(runs.values(), key=lambda r: r["Mtuples_s"])
+    return best, runs, cpu
+
+
+def reference_main(args, metric, base_config, world, mat, scaling="weak"):
+    """The reference arm: the reference's own join (oracle/_ref, compiled from
+    its sources) timed on this host's cores, all logical CPUs, on the
+    workload's configuration; `warmup` untimed calls, then `steps` timed ones
+    (each on fresh copies of R and S), the median of its Total Runtime."""
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtbref.so not built"}))
+        return 0
+    algo = wl_spec(args.workload)[0]
+    ref_algo = algo if algo in ("RHO", "RHT", "RSM", "PSM") else "RHO"
+    nR, nS = base_config["nR"], base_config["nS"]
+    t0 = time.perf_counter()
+    R, S, how = reference_inputs(args.workload, nR, nS, 1 << 27)
+    if mat and len(S) > (1 << 26):  # one malloc'd list node per output row: keep it bounded
+        S = S[: 1 << 26].copy()
+        how += f"; materialising: the first {len(S)} S rows"
+    gen_s = time.perf_counter() - t0
+    cpu = host_cpu()
+    threads = cpu["logical_cpus"]
+    steps, warm = max(1, args.steps), max(0, args.warmup)
+    t, ts, count = cpu_reference_run(R, S, ref_algo, steps, warm, threads, mat)
+    value = (len(R) + len(S)) / t / 1e6
+    sample = (f"reference {ref_algo}{'_mat' if mat else ''} (oracle/_ref, built from the reference's sources) on "
+              f"|R|={len(R)}, |S|={len(S)}: {how}; {threads} threads (all logical CPUs of "
+              f"{cpu['model']}, {cpu['physical_cores']} physical cores); median of {steps} calls after {warm} "
+              f"warm-up calls, its own Total Runtime (us)")
+    config = dict(base_config)
+    if len(S) != nS:
+        config["sampled_nS"] = len(S)
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": "Mtuples/s", "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": scaling, "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": config,
+            "matches": int(count),
+            "cpu_baseline": {"value": value, "unit": "Mtuples/s", "cores": threads, "kind": "reference",
+                             "sample": sample, "host": cpu, "runs_ms": [x * 1e3 for x in ts],
+                             "input_generation_s": gen_s},
+            "e2e": {"value": value, "unit": "Mtuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 # --------------------------------------------------------------------- GPU
+# Learned vs radix partitioning on the skewed configuration: |R| = 2^26
+# unique keys, |S| = 2^29 Zipf over R's keys, hot keys at small ranks (rank =
+# key) or scattered over the key range by a seeded permutation.
+LVR_CASES = [("z1", 1.0, 0), ("z1_scattered", 1.0, 1)]
+LVR_VARIANTS = [("lrn", "LRN", {}), ("rho_skew_split", "RHO", {}), ("rho_plain", "RHO", {"skew_split": 0})]
+
+
+def learned_vs_radix(tbg, torch, dev, stream, steps, warmup, lr=26, ls=29, cases=LVR_CASES):
+    """Times LRN, RHO with its S-side skew split (the library default) and RHO
+    without it (the reference's behaviour) on the same device-resident
+    inputs, CUDA events on the join stream, the clock sampler running."""
+    sh = stream.cuda_stream
+    nR, nS = 1 << lr, 1 << ls
+    tR = torch.empty(nR, dtype=torch.int64, device=dev)
+    tS = torch.empty(nS, dtype=torch.int64, device=dev)
+    pR, pS = tR.data_ptr(), tS.data_ptr()
+    tbg.gen_pk(pR, nR, 11111, sh)
+    out = {"workload": f"|R|=2^{lr} unique keys, |S|=2^{ls} Zipf over R's keys (rank = key, or ranks scattered "
+                       f"over the keys by a seeded permutation), count only",
+           "steps": steps, "warmup": warmup, "timing": "CUDA events around the timed joins on their stream",
+           "cases": {}}
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    for label, z, scatter in cases:
+        tbg.gen_zipf(pS, nS, nR, z, scatter, 22222, sh)
+        stream.synchronize()
+        entry = {"z": z, "scattered": bool(scatter)}
+        with ClockSampler(dev.index) as clk:
+            for name, algo, over in LVR_VARIANTS:
+                cfg = tbg.config(algo, **over)
+                for _ in range(warmup):
+                    _, m, st = tbg.join_device(cfg, pR, nR, pS, nS, stream=sh)
+                torch.cuda.synchronize()
+                ev0.record(stream)
+                for _ in range(steps):
+                    _, m, st = tbg.join_device(cfg, pR, nR, pS, nS, stream=sh)
+                ev1.record(stream)
+                torch.cuda.synchronize()
+                ms = ev0.elapsed_time(ev1) / steps
+                part_rows = nS - int(st.heavy_rows_S)
+                mean_s = part_rows / st.partitions if st.partitions else 0.0
+                entry[name] = {"ms": ms, "Mtuples_s": (nR + nS) / ms / 1e3, "matches": int(m),
+                               "radix_bits": st.radix_bits, "max_part_S": int(st.max_part_S),
+                               "mean_part_S": mean_s,
+                               "max_over_mean_S": int(st.max_part_S) / mean_s if mean_s else None,
+                               "used_fallback": st.used_fallback, "heavy_keys": int(st.heavy_keys),
+                               "heavy_rows_S": int(st.heavy_rows_S), "train_steps": st.train_steps,
+                               "train_loss": st.train_loss}
+        entry["clocks"] = clk.summary()
+        counts = {entry[n]["matches"] for n, _, _ in LVR_VARIANTS}
+        entry["identical_counts"] = len(counts) == 1 and counts == {nS}
+        entry["lrn_speedup_vs_plain"] = entry["rho_plain"]["ms"] / entry["lrn"]["ms"]
+        entry["lrn_speedup_vs_skew_split"] = entry["rho_skew_split"]["ms"] / entry["lrn"]["ms"]
+        out["cases"][label] = entry
+    del tR, tS
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -283,7 +432,9 @@ def main():
     ap.add_argument("--workload", default="rho_c2", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-log2", type=int, default=29)
+    ap.add_argument("--no-learned-block", action="store_true",
+                    help="skip the learned-vs-radix comparison the headline line carries")
+    ap.add_argument("--cpu-sample-log2", type=int, default=30, help="S rows (log2) of the CPU baseline's sample")
     # smaller cases of the same workload (profiling captures); never the reported configuration
     ap.add_argument("--log2-r", type=int, default=None)
     ap.add_argument("--log2-s", type=int, default=None)
@@ -312,30 +463,11 @@ def main():
     metric = ("input Mtuples/s (|R|+|S|)/t, " + ("materialising" if mat else "count-only") +
               " equi-join, bit-exact")
 
+    base_config = {"workload": workload_name, "global_batch": world * (nR + nS), "nR": nR, "nS": nS}
     if args.impl == "reference":
         if rank != 0:
             return 0
-        threads = host_threads()
-        steps = max(1, args.steps)
-        warm = max(0, min(args.warmup, 1))
-        res, why = cpu_reference_run(args.workload, 1 << args.cpu_sample_log2, steps, warm, threads)
-        if res is None:
-            print(json.dumps({"impl": "reference", "unavailable": why}))
-            return 0
-        line = {"impl": "reference", "metric": metric, "value": res["value"], "unit": "Mtuples/s",
-                "n_gpus": world, "steps": steps, "warmup": warm,
-                "ms_per_step": res["seconds_per_step"] * 1e3, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-                "config": {"workload": workload_name, "global_batch": res["nR"] + res["nS"]},
-                "cpu_baseline": {"value": res["value"], "unit": "Mtuples/s", "cores": threads,
-                                 "kind": "reference",
-                                 "sample": f"reference {res['algo']} (oracle/_ref, its own sources) on "
-                                           f"|R|={res['nR']}, |S|={res['nS']} rows of the workload, "
-                                           f"{threads} threads, its own Total Runtime (us)"},
-                "e2e": {"value": res["value"], "unit": "Mtuples/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return 0
+        return reference_main(args, metric, base_config, world, mat)
 
     import torch
     import torch.distributed as dist
@@ -358,6 +490,10 @@ def main():
         else:
             tbg.gen_zipf(pS, nS, nR, float(param), 0, 22222 + rank, sh)
     stream.synchronize()
+    host_rows = None  # the workload's rows for the CPU baseline (rank 0, one GPU)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and reference_available():
+        nS_cpu = min(nS, 1 << (26 if mat else args.cpu_sample_log2))
+        host_rows = (host_copy_rows(tR, nR), host_copy_rows(tS, nS_cpu), nS)
 
     cfg = tbg.config(algo, **over)
     cfg.timing = 1
@@ -532,22 +668,40 @@ def main():
         "clocks": clocks.summary(),
         "matches": int(m),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = host_threads()
-        res, why = cpu_reference_run(args.workload, 1 << args.cpu_sample_log2, 1, 0, threads)
-        if res:
-            line["cpu_baseline"] = {"value": res["value"], "unit": "Mtuples/s", "cores": threads,
-                                    "kind": "reference",
-                                    "sample": f"reference {res['algo']} (oracle/_ref) on |R|={res['nR']}, "
-                                              f"|S|={res['nS']} rows of the workload, its own timer"}
-        else:
-            line["cpu_baseline"] = {"value": None, "unavailable": why}
+    if args.workload == "rho_c2" and world == 1 and not args.no_learned_block and args.log2_r is None:
+        line["learned_vs_radix"] = learned_vs_radix(tbg, torch, dev, stream, args.steps, args.warmup)
+    if host_rows is not None:
+        line["cpu_baseline"] = cpu_baseline_line(host_rows, algo, mat)
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = {"value": None, "unavailable": "oracle/_ref/libtbref.so not built"}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def host_copy_rows(t, n):
+    """The first n rows of a device relation as a host ROW array."""
+    return t[:n].cpu().numpy().view(np.dtype([("key", "<u4"), ("payload", "<u4")]))
+
+
+def cpu_baseline_line(host_rows, algo, mat):
+    """cpu_baseline: the reference's own join on the rows the GPU joined (R
+    whole, S whole or its stated prefix), at the physical core count and at
+    the logical CPU count, median of 3 calls each."""
+    R, S, nS_full = host_rows
+    ref_algo = algo if algo in ("RHO", "RHT", "RSM", "PSM") else "RHO"
+    best, runs, cpu = cpu_baseline_leg(R, S, ref_algo, mat)
+    part = "all" if len(S) == nS_full else f"the first {len(S)} of {nS_full}"
+    return {"value": best["Mtuples_s"], "unit": "Mtuples/s", "cores": best["threads"], "kind": "reference",
+            "sample": f"reference {ref_algo}{'_mat' if mat else ''} (oracle/_ref, built from the reference's sources) "
+                      f"on the workload's own rows copied from the GPU: R all {len(R)}, S {part} rows; median of 3 "
+                      f"calls after 1 warm-up at {runs['physical']['threads']} threads (physical cores) and at "
+                      f"{runs['logical']['threads']} threads (logical CPUs), its own Total Runtime; value = the "
+                      f"faster",
+            "host": cpu, "runs": runs}
 
 
 # ------------------------------------------------------------------ sharded
@@ -567,23 +721,8 @@ def sharded_main(args, rank, world, local):
     if args.impl == "reference":
         if rank != 0:
             return 0
-        threads = host_threads()
-        res, why = cpu_reference_run("rho_c2", 1 << args.cpu_sample_log2, max(1, args.steps), 1, threads)
-        if res is None:
-            print(json.dumps({"impl": "reference", "unavailable": why}))
-            return 0
-        print(json.dumps({"impl": "reference", "metric": metric, "value": res["value"], "unit": "Mtuples/s",
-                          "n_gpus": world, "steps": max(1, args.steps), "warmup": 1,
-                          "ms_per_step": res["seconds_per_step"] * 1e3, "higher_is_better": True,
-                          "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-                          "config": {"workload": workload_name, "global_batch": res["nR"] + res["nS"]},
-                          "cpu_baseline": {"value": res["value"], "unit": "Mtuples/s", "cores": threads,
-                                           "kind": "reference",
-                                           "sample": f"reference RHO (oracle/_ref) on |R|={res['nR']}, "
-                                                     f"|S|={res['nS']} rows, {threads} threads, its own timer"},
-                          "e2e": {"value": res["value"], "unit": "Mtuples/s", "h2d_bytes_per_step": 0,
-                                  "d2h_bytes_per_step": 0}}))
-        return 0
+        return reference_main(args, metric, {"workload": workload_name, "global_batch": nR + nS, "nR": nR,
+                                             "nS": nS}, world, False, scaling="strong")
     import torch
     import torch.distributed as dist
     tbg = importlib.import_module("tee-bench_b200")
@@ -668,12 +807,9 @@ def sharded_main(args, rank, world, local):
         "clocks": clocks.summary(),
         "matches": int(m),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = host_threads()
-        res, why = cpu_reference_run("rho_c2", 1 << args.cpu_sample_log2, 1, 0, threads)
-        line["cpu_baseline"] = ({"value": res["value"], "unit": "Mtuples/s", "cores": threads, "kind": "reference",
-                                 "sample": f"reference RHO (oracle/_ref) on |R|={res['nR']}, |S|={res['nS']} rows"}
-                                if res else {"value": None, "unavailable": why})
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and reference_available():
+        host_rows = (host_copy_rows(tR, nR), host_copy_rows(tS, min(nSl, 1 << args.cpu_sample_log2)), nSl)
+        line["cpu_baseline"] = cpu_baseline_line(host_rows, "RHO", False)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -158,9 +158,10 @@ enum { TBG_RHO = 0, TBG_RHT = 1, TBG_RSM = 2, TBG_PSM = 3, TBG_LRN = 4 };
 /* LRN model choices: how the heavy (frequent) S keys that bypass
  * partitioning are picked from the 1% sample's candidate keys */
 enum {
-    TBG_MODEL_MLP = 0,        /* FP32 MLP 1->32->32->1, trained on the GPU,
-                                 predicts each candidate's S rows            */
-    TBG_MODEL_SAMPLE = 1,     /* ablation: rank by raw sample counts, no model */
+    TBG_MODEL_MLP = 0,        /* FP32 MLP 1->32->32->1, trained on the GPU on
+                                 the sample's frequency-by-rank curve; predicts
+                                 the S rows of the top ranks                 */
+    TBG_MODEL_SAMPLE = 1,     /* ablation: raw sample counts, no model         */
     TBG_MODEL_UNTRAINED = 2,  /* ablation: the MLP at its initialisation       */
     TBG_MODEL_UNIFORM = 3     /* ablation: no heavy keys (plain radix, RHO)    */
 };
@@ -202,6 +203,8 @@ typedef struct tbg_stats {
     float train_loss;
     uint32_t kernel_launches;   /* kernels this call launched                */
     float ms_hist, ms_pass1, ms_pass2, ms_join, ms_learn, ms_total;
+    double heavy_rows_predicted; /* LRN: S rows the model predicts for the top ranks it flags */
+    double heavy_rows_sampled;   /* LRN: the sample's own estimate for the heavy keys taken   */
 } tbg_stats;
 
 TBG_API void tbg_config_init(tbg_config *cfg); /* defaults: RHO, automatic, count only */
@@ -231,10 +234,11 @@ TBG_API uint64_t tbg_kernel_launches(void);
 /* ---- learned partitioner model (LRN) --------------------------------------
  * The FP32 MLP 1->32->32->1 (tanh) that LRN trains per join, exposed for
  * inspection and tests.  params: W1[32], b1[32], W2[32][32], b2[32], W3[32],
- * b3 (host arrays of tbg_mlp_param_count() floats); x is the key feature
- * tbg_mlp_feature(key), y the target CDF value. */
+ * b3 (host arrays of tbg_mlp_param_count() floats).  LRN fits the frequency
+ * curve of S's keys: x = tbg_mlp_feature(r) for sample rank r (1 = the key
+ * the sample saw most often), y = log2(that key's sample count) / 32. */
 TBG_API int tbg_mlp_param_count(void);
-TBG_API float tbg_mlp_feature(uint32_t key);
+TBG_API float tbg_mlp_feature(uint32_t rank);
 /* seeded initialisation, as LRN uses before training */
 TBG_API int tbg_mlp_init(float *params, uint64_t seed);
 /* mean squared error over n points and its gradient (the GPU backward pass) */
@@ -243,6 +247,23 @@ TBG_API int tbg_mlp_grad(const float *params, const float *x, const float *y, ui
 /* `steps` Adam steps on the GPU trainer (batches drawn from the n points) */
 TBG_API int tbg_mlp_train(float *params, const float *x, const float *y, uint64_t n, int steps,
                           float lr, uint64_t seed);
+
+/* ---- joins split over several GPUs: the exchange step ----------------------
+ * The reference splits one join over threads by contiguous chunks of R and S
+ * (Joins/radix_join.c:1285-1306).  Across GPUs the split is by key: every
+ * rank splits its rows of R and of S by destination shard, an all-to-all
+ * (NCCL, in the caller) moves each piece to its shard's rank, every rank joins
+ * what it received with tbg_join_device, and the counts are summed (equal keys
+ * always meet on one rank).
+ *
+ * tbg_shard_split writes the n device rows of d_in to d_out grouped by shard:
+ * shard d's rows at d_out[offsets[d] .. offsets[d + 1]) (offsets: a host array
+ * of nshards + 1 entries, filled; waits for the stream).  1 <= nshards <= 256.
+ * tbg_shard_of(key, nshards) is the shard of a key: a multiplicative hash of
+ * the key, so shards get even shares of skewed keys too.                    */
+TBG_API int tbg_shard_split(const struct row_t *d_in, uint64_t n, int nshards, struct row_t *d_out,
+                            uint64_t *offsets, void *stream);
+TBG_API uint32_t tbg_shard_of(uint32_t key, int nshards);
 
 /* ---- chained joins on device-resident output --------------------------------
  * to_relation (Enclave/TrustedJoins/secure_joins.cpp:277-301): materialised

@@ -85,7 +85,8 @@ class Stats(C.Structure):
                 ("train_steps", C.c_int), ("train_loss", C.c_float),
                 ("kernel_launches", C.c_uint32),
                 ("ms_hist", C.c_float), ("ms_pass1", C.c_float), ("ms_pass2", C.c_float),
-                ("ms_join", C.c_float), ("ms_learn", C.c_float), ("ms_total", C.c_float)]
+                ("ms_join", C.c_float), ("ms_learn", C.c_float), ("ms_total", C.c_float),
+                ("heavy_rows_predicted", C.c_double), ("heavy_rows_sampled", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -175,6 +176,10 @@ def lib():
     L.tbg_mlp_grad.restype = I
     L.tbg_mlp_train.argtypes = [P, P, P, U64, I, C.c_float, U64]
     L.tbg_mlp_train.restype = I
+    L.tbg_shard_split.argtypes = [P, U64, I, P, C.POINTER(U64), P]
+    L.tbg_shard_split.restype = I
+    L.tbg_shard_of.argtypes = [C.c_uint32, I]
+    L.tbg_shard_of.restype = C.c_uint32
     L.tbg_set_error_mode(ERRMODE_RETURN)  # Python callers get exceptions, not exit()
     _lib = L
     return L
@@ -321,6 +326,57 @@ def last_transfer_bytes():
     return int(h.value), int(d.value)
 
 
+# ------------------------------------------------------------------ several GPUs
+def shard_of(keys, nshards: int) -> np.ndarray:
+    """Shard of each key for a join split over nshards ranks (tbg_shard_of):
+    the top bits of the multiplicative hash key * 0x9E3779B1 (mod 2^32),
+    range-reduced to [0, nshards) by a multiply-shift."""
+    h = (np.asarray(keys, dtype=np.uint64) * np.uint64(0x9E3779B1)) & np.uint64(0xFFFFFFFF)
+    return ((h * np.uint64(nshards)) >> np.uint64(32)).astype(np.int64)
+
+
+def shard_split(d_in: int, n: int, nshards: int, d_out: int, stream: int = 0) -> list:
+    """Groups n device rows by shard into d_out (tbg_shard_split); returns
+    the nshards + 1 row offsets of the groups."""
+    offs = (C.c_uint64 * (nshards + 1))()
+    _check(lib().tbg_shard_split(d_in or None, n, nshards, d_out or None, offs, stream or None))
+    return [int(x) for x in offs]
+
+
+def distributed_join_count(dist, R, S, split, join, new_rows):
+    """Count of one equi-join whose relations are spread over the ranks of the
+    process group `dist` (NCCL on GPUs, gloo in CPU tests); every rank calls
+    it with its own rows of R and of S (1-D int64 tensors, one row each).
+
+    Every rank splits its rows by shard (``split(rows, nshards) -> (grouped
+    rows, offsets)``), the pieces move to their shards' ranks with an
+    all-to-all (counts first, then rows), each rank joins what it received
+    (``join(R_recv, S_recv) -> count``) and the counts are summed.  Keys never
+    meet across shards, so the sum is the join's count, which every rank
+    returns.  ``new_rows(n)`` allocates a receive buffer of n rows.  With one
+    rank the rows are joined as they are.  This replaces the reference's
+    per-thread chunking of one join (Joins/radix_join.c:1285-1306) by a split
+    across GPUs by key."""
+    import torch
+    world = dist.get_world_size() if dist is not None and dist.is_initialized() else 1
+    if world == 1:
+        return int(join(R, S))
+    received = []
+    for rows in (R, S):
+        grouped, offs = split(rows, world)
+        send = [offs[d + 1] - offs[d] for d in range(world)]
+        sc = torch.tensor(send, dtype=torch.int64, device=rows.device)
+        rc = torch.empty_like(sc)
+        dist.all_to_all_single(rc, sc)
+        recv = [int(x) for x in rc.tolist()]
+        out = new_rows(sum(recv))
+        dist.all_to_all_single(out, grouped, output_split_sizes=recv, input_split_sizes=send)
+        received.append(out)
+    c = torch.tensor([int(join(received[0], received[1]))], dtype=torch.int64, device=R.device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return int(c.item())
+
+
 # ------------------------------------------------------------------ model
 def mlp_init(seed: int) -> np.ndarray:
     L = lib()
@@ -351,9 +407,10 @@ def mlp_train(params, x, y, steps, lr=0.01, seed=1):
     return p
 
 
-def mlp_feature(keys) -> np.ndarray:
-    """Model input of keys: log2(key + 1) / 16 - 1 (what LRN feeds the MLP)."""
-    return (np.log2(np.asarray(keys, dtype=np.float64) + 1.0) / 16.0 - 1.0).astype(np.float32)
+def mlp_feature(ranks) -> np.ndarray:
+    """Model input of sample ranks: log2(rank + 1) / 16 - 1 (what LRN feeds
+    the MLP; rank 1 is the key the sample saw most often)."""
+    return (np.log2(np.asarray(ranks, dtype=np.float64) + 1.0) / 16.0 - 1.0).astype(np.float32)
 
 
 # ------------------------------------------------------------------ batches

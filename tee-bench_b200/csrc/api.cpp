@@ -107,7 +107,10 @@ Workspace *workspace_for(cudaStream_t st) {
     Workspace *w = new Workspace();
     w->device = dev;
     cudaDeviceGetAttribute(&w->nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaMallocHost(&w->host_ctrl, sizeof(Ctrl)) != cudaSuccess) {
+    if (cudaMallocHost(&w->host_ctrl, sizeof(Ctrl)) != cudaSuccess ||
+        cudaMallocHost(&w->host_small, Workspace::HOST_SMALL_BYTES) != cudaSuccess) {
+        cudaGetLastError();
+        if (w->host_ctrl) cudaFreeHost(w->host_ctrl);
         delete w;
         return nullptr;
     }
@@ -128,6 +131,13 @@ uint32_t Workspace::next_epoch(cudaStream_t st) {
     }
     return epoch;
 }
+
+// Pass 2 processes units of at least this many rows (consecutive chunks of
+// one pass-1 partition).
+#ifndef TBG_PASS2_UNIT_ROWS
+#define TBG_PASS2_UNIT_ROWS 65536
+#endif
+static constexpr uint64_t PASS2_UNIT_ROWS = TBG_PASS2_UNIT_ROWS;
 
 static int ceil_log2(uint64_t x) {
     int k = 0;
@@ -291,7 +301,7 @@ int part_pass(int rel, int which, const RadixGeom &g, const Row *d, Workspace &w
     a.chunk_len = nullptr;
     a.G = g.G[rel];
     const uint64_t per_unit = std::max<uint64_t>(n / ((uint64_t)a.G * g.F1), 1);
-    a.group = (int)std::min<uint64_t>((uint64_t)a.G, std::max<uint64_t>(1, 65536 / per_unit));
+    a.group = (int)std::min<uint64_t>((uint64_t)a.G, std::max<uint64_t>(1, PASS2_UNIT_ROWS / per_unit));
     a.b1 = g.b1;
     a.b2 = g.b2;
     a.rf = g.rf;
@@ -501,6 +511,8 @@ int finish_join(const tbg_config &cfg, Workspace &w, cudaStream_t st, const Join
         stats->predicted_imbalance = run.predicted_imbalance;
         stats->train_steps = run.train_steps;
         stats->train_loss = run.train_loss;
+        stats->heavy_rows_predicted = run.heavy_pred;
+        stats->heavy_rows_sampled = run.heavy_sampled;
         stats->kernel_launches = (uint32_t)run.launches;
         if (run.timed) {
             float t;

@@ -1,17 +1,21 @@
 // Host pipeline of LRN, the learned skew-aware join, and the C-ABI entry
 // points of its model.
 //
-//   1. sample 1% of S's keys (seeded) and sort the sample (LSD radix sort);
-//   2. list the keys the sample repeats with their sample estimates, and
-//      train the MLP on them (log-key feature -> log2(rows) / 32) on the GPU;
-//   3. score the candidates with the model (predicted S rows) and keep the
-//      largest (up to HEAVY_MAX) as heavy keys;
-//   4. fall back to plain radix (RHO) when the keys the model selected hold,
-//      by the sample's measure, less than 5% of S: the bypass would not pay
-//      for its set-up;
-//   5. otherwise build the heavy table, count (and, materialising, collect)
-//      R's heavy rows, radix partition R and the non-heavy rows of S (the S
-//      histogram joins heavy rows on the spot) and join the partitions.
+//   1. sample 1% of S's keys (seeded blocks of 64 rows) and count them: a
+//      shared-memory aggregation per CTA, then a global hash table;
+//   2. the sample's frequency curve: count-of-counts bins, one training point
+//      per bin (rank feature -> log2(count) / 32), and the MLP trained on
+//      them on the GPU;
+//   3. the decision kernel predicts the S rows of ranks 1 .. HEAVY_MAX from
+//      the trained curve: the heavy keys are the sampled keys at the ranks
+//      predicted to hold at least tau_min rows, and LRN bypasses when the
+//      model predicts those keys to hold at least 5% of S (below that, the
+//      bypass would not pay for its set-up and plain radix runs);
+//   4. with the bypass: build the heavy table, count (and, materialising,
+//      collect) R's heavy rows, radix partition R and the non-heavy rows of S
+//      (the S histogram joins heavy rows on the spot) and join the partitions.
+// Steps 1-3 run on a second stream while R is partitioned, and the host reads
+// the decision back once.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -27,15 +31,6 @@ namespace tbg {
 
 static constexpr double kMinHeavyFraction = 0.05;
 static constexpr unsigned kCandCap = 1u << 20;
-
-struct LearnCounters {
-    unsigned ncand;
-    unsigned inserted;
-    float loss_sum;
-    unsigned pad;
-    unsigned bins[64];
-    unsigned long long mass[64];
-};
 
 int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                      tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run) {
@@ -59,11 +54,15 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
             return cuda_error(e, "stream");
     }
     cudaStream_t s2 = w.side;
-    double rate = cfg.sample_rate > 0 ? cfg.sample_rate : 0.01;
-    uint64_t m = (uint64_t)((double)nS * rate);
-    m = std::max<uint64_t>(m, 65536);
-    m = std::min<uint64_t>(m, nS);
-    const uint64_t tiles = (m + SCATTER_TILE - 1) / SCATTER_TILE + 1;
+    // the sample: nb whole blocks of SAMPLE_BLOCK rows, one per stride of S
+    const double rate = cfg.sample_rate > 0 ? cfg.sample_rate : 0.01;
+    const uint64_t nfull = nS / SAMPLE_BLOCK;
+    uint64_t nb = (uint64_t)((double)nS * rate / SAMPLE_BLOCK);
+    nb = std::min<uint64_t>(std::max<uint64_t>(nb, 65536 / SAMPLE_BLOCK), nfull);
+    const uint64_t stride = nfull / nb;
+    const uint64_t m = nb * SAMPLE_BLOCK;
+    uint32_t tslots = 1u << 16;
+    while (tslots < m + m / 2 && tslots < (1u << 24)) tslots <<= 1;
     const int capR = join_capacity(nR);
     const RadixGeom g = radix_geometry(cfg, nR, nS, capR, w);
     run->B = g.B;
@@ -76,25 +75,32 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         e = (buf).ensure(bytes);                                  \
         if (e != cudaSuccess) return cuda_error(e, "cudaMalloc"); \
     } while (0)
-    ENSURE(w.aux[0], m * 8);                     // sample, sort ping
-    ENSURE(w.aux[1], m * 8);                     // sort pong
-    ENSURE(w.aux[4], 8192);                      // digit histograms of the sample, then candidate counts
-    ENSURE(w.aux[5], 4 * 256 * 8);
-    ENSURE(w.aux[2], (size_t)16384 * 8);         // training set x, y
-    ENSURE(w.aux[3], (size_t)MLP_PARAMS_PAD * 4 * 2 + sizeof(LearnCounters));
+    ENSURE(w.aux[0], m * 4);                                         // sample keys
+    ENSURE(w.aux[1], (size_t)tslots * 8);                            // count table: keys, counts
+    ENSURE(w.aux[2], (size_t)CC_BINS * (4 + 8 + 4 + 4));            // bins, training points
+    ENSURE(w.aux[3], (size_t)MLP_PARAMS_PAD * 4 + sizeof(LrnDecision));
     ENSURE(w.aux[6], (size_t)kCandCap * sizeof(HeavyCand));
-    ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 4 + (1 << FILTER_LOG2) / 8);  // keys, cnt, start, cur, filter
-    ENSURE(w.status, tiles * SCATTER_FMAX * 8);
+    ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 4 + (1 << FILTER_LOG2) / 8 + 16);  // keys, cnt, start, cur, filter
 #undef ENSURE
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
-    float *xs = w.aux[2].as<float>(), *ys = xs + 16384;
-    float *params = w.aux[3].as<float>();
-    float *grad = params + MLP_PARAMS_PAD;
-    LearnCounters *lc = reinterpret_cast<LearnCounters *>(grad + MLP_PARAMS_PAD);
+    LearnBufs lb;
+    lb.keys = w.aux[0].as<uint32_t>();
+    lb.tkeys = w.aux[1].as<uint32_t>();
+    lb.tcnt = lb.tkeys + tslots;
+    lb.tmask = tslots - 1;
+    lb.bin_rows = w.aux[2].as<unsigned long long>();
+    lb.bin_keys = reinterpret_cast<unsigned *>(lb.bin_rows + CC_BINS);
+    lb.xs = reinterpret_cast<float *>(lb.bin_keys + CC_BINS);
+    lb.ys = lb.xs + CC_BINS;
+    lb.params = w.aux[3].as<float>();
+    lb.dec = reinterpret_cast<LrnDecision *>(lb.params + MLP_PARAMS_PAD);
+    lb.cand = w.aux[6].as<HeavyCand>();
+    lb.cand_cap = kCandCap;
+    lb.err = &ctrl->error;
     uint32_t *hkeys = w.aux[7].as<uint32_t>();
     unsigned *hcnt = hkeys + HEAVY_CAP, *hstart = hcnt + HEAVY_CAP, *hcur = hstart + HEAVY_CAP;
     uint32_t *hfilter = hcur + HEAVY_CAP;
-    HeavyCand *cand = w.aux[6].as<HeavyCand>();
+    unsigned *hinserted = hfilter + (1 << FILTER_LOG2) / 32;
 
     // main stream: R's partitioning needs nothing from the model
     if (timing) cudaEventRecord(w.ev[0], st);
@@ -106,80 +112,46 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
 
     // side stream: learn the heavy keys meanwhile
     if ((e = cudaStreamWaitEvent(s2, w.fork, 0)) != cudaSuccess) return cuda_error(e, "event");
-    if ((e = cudaMemsetAsync(lc, 0, sizeof(LearnCounters), s2)) != cudaSuccess) return cuda_error(e, "memset");
-    // 1. sample and sort
-    if ((e = launch_sample(dS, nS, w.aux[0].as<Row>(), m, cfg.seed, s2)) != cudaSuccess) return cuda_error(e, "sample");
-    if ((e = launch_digit_hist(w.aux[0].as<Row>(), m, w.aux[4].as<uint32_t>(), w.aux[5].as<uint64_t>(), w.nsm, s2)) !=
-        cudaSuccess)
-        return cuda_error(e, "sample digits");
-    uint32_t hh[1024];
-    if ((e = cudaMemcpyAsync(hh, w.aux[4].p, sizeof hh, cudaMemcpyDeviceToHost, s2)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(s2)) != cudaSuccess)
-        return cuda_error(e, "sample digits");
-    const Row *sorted = nullptr;
-    int npass = 0;
-    // ping-pong aux[1] -> aux[0] -> ...: the first pass never writes its input
-    if ((rc = lsd_sort(w.aux[0].as<Row>(), m, w.aux[1], w.aux[0], hh, w.aux[5].as<uint64_t>(), 8, w, s2, &sorted,
-                       &npass)))
-        return rc;
-    // 2. candidates (distinct sampled keys) and the frequency model
-    if ((e = launch_candidates(sorted, m, (double)nS, cand, &lc->ncand, kCandCap, w.aux[4].as<unsigned>(), s2)) !=
-        cudaSuccess)
-        return cuda_error(e, "candidates");
-    unsigned ncand_raw = 0;
-    if ((e = cudaMemcpyAsync(&ncand_raw, &lc->ncand, 4, cudaMemcpyDeviceToHost, s2)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(s2)) != cudaSuccess)
-        return cuda_error(e, "candidates");
-    const unsigned ncand = std::min(ncand_raw, kCandCap);
-    const uint32_t T = std::min<uint32_t>(ncand, 16384);
-    if ((e = launch_mlp_init(params, cfg.seed, s2)) != cudaSuccess) return cuda_error(e, "mlp init");
-    const int steps = cfg.model == TBG_MODEL_MLP && T ? std::min(std::max(cfg.train_steps, 1), 500) : 0;
-    if (T) {
-        if ((e = launch_freq_points(cand, ncand, xs, ys, T, s2)) != cudaSuccess) return cuda_error(e, "points");
-        if (steps && (e = launch_mlp_train(xs, ys, T, params, steps, 0.03f, cfg.seed, s2)) != cudaSuccess)
-            return cuda_error(e, "mlp train");
-        if ((e = launch_mlp_grad(params, xs, ys, T, grad, &lc->loss_sum, s2)) != cudaSuccess)
-            return cuda_error(e, "mlp loss");
-    }
-    // 3. score: the model (or, for the ablation, the sample) proposes; keys the
-    // sample saw once are not scored (they cannot reach the threshold)
-    const double tau_min = std::max(64.0, (double)nS / (double)(1 << 20));
+    if ((e = cudaMemsetAsync(lb.tkeys, 0xFF, (size_t)tslots * 4, s2)) != cudaSuccess ||
+        (e = cudaMemsetAsync(lb.tcnt, 0, (size_t)tslots * 4, s2)) != cudaSuccess ||
+        (e = cudaMemsetAsync(lb.bin_rows, 0, (size_t)CC_BINS * 12, s2)) != cudaSuccess ||
+        (e = cudaMemsetAsync(lb.dec, 0, sizeof(LrnDecision), s2)) != cudaSuccess ||
+        (e = cudaMemsetAsync(hkeys, 0xFF, HEAVY_CAP * 4, s2)) != cudaSuccess ||
+        (e = cudaMemsetAsync(hcnt, 0, HEAVY_CAP * 4 * 3 + (1 << FILTER_LOG2) / 8 + 16, s2)) != cudaSuccess)
+        return cuda_error(e, "memset");
+    const int steps = cfg.model == TBG_MODEL_MLP ? std::min(std::max(cfg.train_steps, 1), 500) : 0;
     const int use_model = cfg.model == TBG_MODEL_SAMPLE ? 0 : 1;
-    const double single = (double)nS / (double)m;
-    if ((e = launch_heavy_score(cand, ncand, params, use_model, tau_min, 1.5 * single, lc->bins, lc->mass, s2)) !=
-        cudaSuccess)
-        return cuda_error(e, "heavy score");
-    LearnCounters h;
-    if ((e = cudaMemcpyAsync(&h, lc, sizeof h, cudaMemcpyDeviceToHost, s2)) != cudaSuccess ||
+    // a key must be predicted to hold at least tau_min S rows to be heavy
+    const double tau_min = std::max(64.0, (double)nS / (double)(1 << 20));
+    if ((e = launch_sample_blocks(dS, nS, lb.keys, nb, stride, cfg.seed, s2)) != cudaSuccess ||
+        (e = launch_count_keys(lb, m, s2)) != cudaSuccess || (e = launch_count_stats(lb, s2)) != cudaSuccess ||
+        (e = launch_rank_points(lb, s2)) != cudaSuccess || (e = launch_mlp_init(lb.params, cfg.seed, s2)) != cudaSuccess ||
+        (steps && (e = launch_mlp_train(lb.xs, lb.ys, &lb.dec->npoints, 0, lb.params, steps, 0.03f, cfg.seed, s2)) !=
+                      cudaSuccess) ||
+        (e = launch_decide(lb, use_model, (double)nS, (double)m, tau_min, kMinHeavyFraction, s2)) != cudaSuccess)
+        return cuda_error(e, "learning stage");
+    LrnDecision *hd = static_cast<LrnDecision *>(w.host_small);
+    if ((e = cudaMemcpyAsync(hd, lb.dec, sizeof(LrnDecision), cudaMemcpyDeviceToHost, s2)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s2)) != cudaSuccess)
-        return cuda_error(e, "heavy score");
+        return cuda_error(e, "learning stage");
+    const LrnDecision dec = *hd;
     run->train_steps = steps;
-    run->train_loss = T ? h.loss_sum / (float)T : 0.f;
-    // 4. largest bins first while the table has room; the sample measures them
-    unsigned taken = 0;
-    double heavy_mass = 0;
-    int lowest = 64;
-    for (int b = 63; b >= 0; b--) {
-        if (!h.bins[b]) continue;
-        if (taken + h.bins[b] > (unsigned)HEAVY_MAX) break;
-        taken += h.bins[b];
-        heavy_mass += (double)h.mass[b];
-        lowest = b;
-    }
-    run->predicted_imbalance = lowest < 64 ? std::ldexp(1.0, lowest) / ((double)nS / (double)g.P) : 0.0;
-    const bool bypass = taken > 0 && heavy_mass >= kMinHeavyFraction * (double)nS;
+    run->train_loss = dec.loss;
+    run->predicted_imbalance = dec.next_rows / ((double)nS / (double)g.P);
+    run->heavy_pred = dec.pred_mass;
+    run->heavy_sampled = dec.sample_mass;
+    const bool bypass = dec.bypass != 0;
     if (dbg)
-        fprintf(stderr, "[lrn] m=%llu T=%u ncand=%u taken=%u lowest=%d heavy_mass=%.0f loss=%.3e bypass=%d\n",
-                (unsigned long long)m, T, ncand, taken, lowest, heavy_mass, (double)run->train_loss, (int)bypass);
+        fprintf(stderr,
+                "[lrn] m=%llu slots=%u points=%u cand=%u k*=%u count_min=%u heavy=%u pred_mass=%.0f "
+                "sample_mass=%.0f loss=%.3e bypass=%d\n",
+                (unsigned long long)m, tslots, dec.npoints, dec.ncand, dec.k_star, dec.count_min, dec.heavy_sample,
+                dec.pred_mass, dec.sample_mass, (double)dec.loss, (int)bypass);
     if (timing) cudaEventRecord(w.ev[5], s2);
     SBypass bp;
     memset(&bp, 0, sizeof bp);
     if (bypass) {
-        const float tau = (float)std::ldexp(1.0, lowest);
-        if ((e = cudaMemsetAsync(hkeys, 0xFF, HEAVY_CAP * 4, s2)) != cudaSuccess) return cuda_error(e, "memset");
-        if ((e = cudaMemsetAsync(hcnt, 0, HEAVY_CAP * 4 * 3 + (1 << FILTER_LOG2) / 8, s2)) != cudaSuccess)
-            return cuda_error(e, "memset");
-        if ((e = launch_heavy_build(cand, ncand, tau, hkeys, hfilter, &lc->inserted, s2)) != cudaSuccess)
+        if ((e = launch_heavy_build(lb, hkeys, hfilter, hinserted, s2)) != cudaSuccess)
             return cuda_error(e, "heavy build");
         uint32_t *rpay = nullptr;
         if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, s2)) !=
@@ -192,7 +164,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
             if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, hstart, hcur, rpay, 1, w.nsm, s2)) != cudaSuccess)
                 return cuda_error(e, "heavy R");
         }
-        if ((e = cudaMemcpyAsync(&ctrl->heavy_keys, &lc->inserted, 4, cudaMemcpyDeviceToDevice, s2)) != cudaSuccess)
+        if ((e = cudaMemcpyAsync(&ctrl->heavy_keys, hinserted, 4, cudaMemcpyDeviceToDevice, s2)) != cudaSuccess)
             return cuda_error(e, "copy");
         bp.filter = hfilter;
         bp.keys = hkeys;
@@ -275,12 +247,12 @@ int tbg_mlp_train(float *params, const float *x, const float *y, uint64_t n, int
     e = cudaMemcpy(dp, params, MLP_PARAMS * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dx, x, n * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dy, y, n * 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = launch_mlp_train(dx, dy, (uint32_t)n, dp, steps, lr, seed, 0);
+    if (e == cudaSuccess) e = launch_mlp_train(dx, dy, nullptr, (uint32_t)n, dp, steps, lr, seed, 0);
     if (e == cudaSuccess) e = cudaMemcpy(params, dp, MLP_PARAMS * 4, cudaMemcpyDeviceToHost);
     cudaFree(d);
     return e == cudaSuccess ? TBG_OK : cuda_error(e, "mlp train");
 }
 
-float tbg_mlp_feature(uint32_t key) { return key_feature((double)key); }
+float tbg_mlp_feature(uint32_t rank) { return rank_feature((double)rank); }
 
 }  // extern "C"

@@ -1,19 +1,23 @@
 // LRN: learned skew-aware partitioning for sm_100a.
 //
-// A small FP32 MLP (1 -> 32 -> 32 -> 1, tanh) models the frequency of S's
-// keys: log2(rows of S with key k) / 32 as a function of log2(k + 1) / 16 - 1,
-// trained per join on the keys a seeded 1% sample of S repeats, by the kernels
-// in this file (forward, backward, Adam; the trainer is one 8-CTA thread-block
-// cluster that all-reduces gradients through distributed shared memory).
-// The model predicts how many S rows each candidate key has; keys predicted
-// above a threshold are flagged heavy.  Heavy keys never enter the radix
+// A small FP32 MLP (1 -> 32 -> 32 -> 1, tanh) models the frequency curve of
+// S's keys: log2(sample count) / 32 of the key of sample rank r as a function
+// of log2(r + 1) / 16 - 1 (rank 1 = the most frequent key of a seeded 1%
+// sample of S).  It is trained per join on that sample's curve by the
+// kernels in this file (forward, backward, Adam; the trainer is one 8-CTA
+// thread-block cluster that all-reduces gradients through distributed shared
+// memory).  The input is a rank the sample measures, never the key's value,
+// so the curve is the same whether hot keys are small integers or scattered
+// over the key range.  From the trained curve the decision kernel predicts
+// the S rows of ranks 1 .. HEAVY_MAX: the ranks predicted above a threshold
+// are the heavy keys (taken by sample count), and LRN bypasses only when the
+// model predicts they hold enough of S.  Heavy keys never enter the radix
 // partitions: their (R, S) pairs are joined in the histogram read itself,
 // split across every CTA that streams S, against a shared-memory table of
 // their R rows.  The remaining rows are radix partitioned and joined as in
 // RHO.  The model only chooses which keys take the heavy path; every row's
 // destination is decided by an exact key comparison, so results are exact
-// whatever the model predicts.  When the model predicts too little heavy
-// mass, the host falls back to plain radix partitioning.
+// whatever the model predicts.
 #include <cooperative_groups.h>
 
 #include "tbg_device.cuh"
@@ -170,10 +174,14 @@ __global__ void __launch_bounds__(MLP_BATCH_CTA) k_mlp_grad(const float *__restr
 // shared memory, applies Adam, and writes the new values into every CTA's
 // parameter copy; a second barrier ends the step.
 __global__ void __cluster_dims__(MLP_CLUSTER, 1, 1) __launch_bounds__(MLP_BATCH_CTA)
-    k_mlp_train(const float *__restrict__ xs, const float *__restrict__ ys, uint32_t n, float *params,
-                int steps, float lr0, uint64_t seed) {
+    k_mlp_train(const float *__restrict__ xs, const float *__restrict__ ys, const unsigned *n_dev, uint32_t n_host,
+                float *params, int steps, float lr0, uint64_t seed) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
+    // the point count: from device memory when the caller's kernels made the
+    // points (the same value for every CTA), else the host's
+    const uint32_t n = n_dev ? *n_dev : n_host;
+    if (n == 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
     float *p = reinterpret_cast<float *>(smem);
     float *gpart = p + MLP_PARAMS_PAD;
@@ -254,194 +262,385 @@ cudaError_t launch_mlp_grad(const float *params, const float *xs, const float *y
     return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_train(const float *xs, const float *ys, uint32_t n, float *params, int steps, float lr,
-                             uint64_t seed, cudaStream_t st) {
-    if (n == 0 || steps <= 0) return cudaSuccess;
+cudaError_t launch_mlp_train(const float *xs, const float *ys, const unsigned *n_dev, uint32_t n, float *params,
+                             int steps, float lr, uint64_t seed, cudaStream_t st) {
+    if ((!n_dev && n == 0) || steps <= 0) return cudaSuccess;
     const size_t smem = mlp_train_smem();
     cudaError_t e = smem_limit((const void *)k_mlp_train, smem);
     if (e != cudaSuccess) return e;
-    k_mlp_train<<<MLP_CLUSTER, MLP_BATCH_CTA, smem, st>>>(xs, ys, n, params, steps, lr, seed);
+    k_mlp_train<<<MLP_CLUSTER, MLP_BATCH_CTA, smem, st>>>(xs, ys, n_dev, n, params, steps, lr, seed);
     count_launch();
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// sample and training set
+// learning stage: sample, key counts, rank curve, decision
 // ---------------------------------------------------------------------------
-__global__ void k_sample(const Row *__restrict__ in, uint64_t n, Row *__restrict__ out, uint64_t m, uint64_t seed) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t j = mix64(seed ^ mix64(i + 0x51ED)) % n;
-        out[i] = Row{in[j].key, 0u};
+// The sample: nblocks blocks of SAMPLE_BLOCK consecutive S rows, block j taken
+// from the stride-sized stretch j of S at a seeded offset (a stratified 1%
+// sample read with coalesced loads).  One warp per block; every block lies
+// inside S (stride * nblocks <= nS / SAMPLE_BLOCK).
+__global__ void k_sample_blocks(const Row *__restrict__ S, uint32_t *__restrict__ keys, uint64_t nblocks,
+                                uint64_t stride, uint64_t seed) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nblocks; j += nw) {
+        const uint64_t sb = j * stride + (stride > 1 ? mix64(seed ^ mix64(j + 0x51ED)) % stride : 0);
+        const Row *src = S + sb * SAMPLE_BLOCK;
+        const uint2 a = ldg_stream(reinterpret_cast<const uint2 *>(src) + lane);
+        const uint2 b = ldg_stream(reinterpret_cast<const uint2 *>(src) + lane + 32);
+        keys[j * SAMPLE_BLOCK + lane] = a.x;
+        keys[j * SAMPLE_BLOCK + lane + 32] = b.x;
     }
 }
 
-cudaError_t launch_sample(const Row *in, uint64_t n, Row *out, uint64_t m, uint64_t seed, cudaStream_t st) {
-    k_sample<<<(unsigned)umin64((m + 255) / 256, 148 * 8), 256, 0, st>>>(in, n, out, m, seed);
+cudaError_t launch_sample_blocks(const Row *S, uint64_t nS, uint32_t *keys, uint64_t nblocks, uint64_t stride,
+                                 uint64_t seed, cudaStream_t st) {
+    (void)nS;
+    if (!nblocks) return cudaSuccess;
+    const unsigned g = (unsigned)umin64((nblocks * 32 + 255) / 256, 148 * 16);
+    k_sample_blocks<<<g, 256, 0, st>>>(S, keys, nblocks, stride, seed);
     count_launch();
     return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// heavy keys: candidates from the sorted sample, scored by the model
-// ---------------------------------------------------------------------------
-// Candidates: each distinct key of the sorted sample, with the sample's
-// estimate of its S rows (nS * run / m).
-// Candidates: the distinct keys of the sorted sample with their sample
-// estimate of S rows, written in key order (so the training points, and the
-// trained model, do not depend on scheduling).  CTA c owns a contiguous range
-// of the sample; k_cand_count counts the run starts in each range, then every
-// CTA places its run starts after those of the ranges before it.
-constexpr int CAND_THREADS = 256;
+__device__ __forceinline__ uint32_t count_hash(uint32_t k) { return (k * 0x9E3779B1u) ^ (k >> 15); }
 
-__device__ __forceinline__ bool run_start(const Row *sorted, uint64_t i) {
-    const uint32_t k = sorted[i].key;
-    return k != 0xFFFFFFFFu && (i == 0 || sorted[i - 1].key != k);
-}
-
-__global__ void __launch_bounds__(CAND_THREADS) k_cand_count(const Row *__restrict__ sorted, uint64_t m,
-                                                            uint64_t chunk, unsigned *cnt) {
-    __shared__ uint64_t scratch[CAND_THREADS / 32 + 1];
-    const uint64_t lo = (uint64_t)blockIdx.x * chunk, hi = umin64(m, lo + chunk);
-    uint64_t c = 0;
-    for (uint64_t i = lo + threadIdx.x; i < hi; i += CAND_THREADS) c += run_start(sorted, i);
-    uint64_t tot;
-    block_excl_scan<CAND_THREADS>(c, &tot, scratch);
-    if (threadIdx.x == 0) cnt[blockIdx.x] = (unsigned)tot;
-}
-
-__global__ void __launch_bounds__(CAND_THREADS) k_candidates(const Row *__restrict__ sorted, uint64_t m,
-                                                            uint64_t chunk, const unsigned *__restrict__ cnt,
-                                                            double nS, HeavyCand *cand, unsigned *ncand,
-                                                            unsigned cand_cap) {
-    __shared__ uint64_t scratch[CAND_THREADS / 32 + 1];
-    const uint64_t lo = (uint64_t)blockIdx.x * chunk, hi = umin64(m, lo + chunk);
-    uint64_t before = 0;  // run starts in the ranges before this one
-    for (unsigned c = threadIdx.x; c < blockIdx.x; c += CAND_THREADS) before += cnt[c];
-    uint64_t base;
-    block_excl_scan<CAND_THREADS>(before, &base, scratch);
-    for (uint64_t t = lo; t < hi; t += CAND_THREADS) {  // block-uniform trip count
-        const uint64_t i = t + threadIdx.x;
-        const bool start = i < hi && run_start(sorted, i);
-        uint64_t tile;
-        const uint64_t pos = base + block_excl_scan<CAND_THREADS>(start ? 1 : 0, &tile, scratch);
-        if (start) {
-            const uint32_t k = sorted[i].key;
-            uint64_t a = i + 1, b = m;  // run end: first index with a larger key
-            while (a < b) {
-                const uint64_t mid = (a + b) >> 1;
-                if (sorted[mid].key == k) a = mid + 1;
-                else b = mid;
-            }
-            if (pos < cand_cap) cand[pos] = HeavyCand{k, (float)(nS * (double)(a - i) / (double)m)};
+// Adds c to key k's count in the global open-addressing table (tmask + 1
+// slots).  A full table drops the key: a key that is not counted is never
+// heavy, which only costs speed.
+__device__ __forceinline__ void table_add(uint32_t *tk, uint32_t *tc, uint32_t tmask, uint32_t k, uint32_t c) {
+    uint32_t h = count_hash(k) & tmask;
+    for (uint32_t probe = 0; probe <= tmask && probe < 4096; probe++) {
+        const uint32_t old = atomicCAS(&tk[h], EMPTY_KEY, k);
+        if (old == EMPTY_KEY || old == k) {
+            atomicAdd(&tc[h], c);
+            return;
         }
-        base += tile;
+        h = (h + 1) & tmask;
     }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *ncand = (unsigned)base;
 }
 
-cudaError_t launch_candidates(const Row *sorted, uint64_t m, double nS, HeavyCand *cand, unsigned *ncand,
-                              unsigned cand_cap, unsigned *scratch_cnt, cudaStream_t st) {
-    if (!m) return cudaMemsetAsync(ncand, 0, sizeof(unsigned), st);
-    const unsigned g = (unsigned)umin64((m + 4095) / 4096, 148 * 8);
-    const uint64_t chunk = (m + g - 1) / g;
-    k_cand_count<<<g, CAND_THREADS, 0, st>>>(sorted, m, chunk, scratch_cnt);
-    k_candidates<<<g, CAND_THREADS, 0, st>>>(sorted, m, chunk, scratch_cnt, nS, cand, ncand, cand_cap);
-    count_launch(2);
-    return cudaGetLastError();
-}
-
-// Training points of the frequency model: T candidates evenly spread over
-// the list; x = key feature, y = log2(sample estimate) / 32.
-__global__ void k_freq_points(const HeavyCand *__restrict__ cand, unsigned ncand, float *xs, float *ys, uint32_t T) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
-    const HeavyCand c = cand[(uint64_t)t * ncand / T];
-    xs[t] = key_feature((double)c.key);
-    ys[t] = log2f(fmaxf(c.count, 1.f)) / 32.f;
-}
-
-cudaError_t launch_freq_points(const HeavyCand *cand, unsigned ncand, float *xs, float *ys, uint32_t T,
-                               cudaStream_t st) {
-    k_freq_points<<<(T + 255) / 256, 256, 0, st>>>(cand, ncand, xs, ys, T);
-    count_launch();
-    return cudaGetLastError();
-}
-
-// Scores every candidate: predicted S rows 2^(32 * M(x)) from the model, or
-// the sample estimate (quantile ablation).  Scores at or above tau_min are
-// binned by floor(log2(score)): bins[] counts them, mass[] sums the sample's
-// estimate of their rows (the model proposes, the sample measures); the score
-// replaces cand[].count (0 below tau_min).
-__global__ void __launch_bounds__(256) k_heavy_score(HeavyCand *cand, unsigned ncand, const float *__restrict__ params,
-                                                     int use_model, double tau_min, double min_sample,
-                                                     unsigned *bins, unsigned long long *mass) {
-    __shared__ float p[MLP_PARAMS];
-    for (int q = threadIdx.x; q < MLP_PARAMS; q += 256) p[q] = params[q];
+// Counts the sample's keys: CTA c aggregates keys [c * CNT_CHUNK, ...) in a
+// shared table (equal keys of a warp first combined with __match_any_sync,
+// so a hot key costs one shared atomic per warp), then adds each distinct
+// key once to the global table.  Key EMPTY_KEY is never counted.
+__global__ void __launch_bounds__(CNT_THREADS) k_count_keys(const uint32_t *__restrict__ keys, uint64_t m,
+                                                           uint32_t *tk, uint32_t *tc, uint32_t tmask) {
+    constexpr int SLOTS = 2 * CNT_CHUNK;
+    __shared__ uint32_t lk[SLOTS];
+    __shared__ uint32_t lc[SLOTS];
+    for (int i = threadIdx.x; i < SLOTS; i += CNT_THREADS) {
+        lk[i] = EMPTY_KEY;
+        lc[i] = 0;
+    }
     __syncthreads();
-    for (unsigned i = blockIdx.x * 256 + threadIdx.x; i < ncand; i += gridDim.x * 256) {
-        HeavyCand c = cand[i];
-        double score = c.count;
-        if (c.count < min_sample) score = 0.0;  // seen once in the sample
-        else if (use_model) score = exp2(32.0 * (double)mlp_eval(p, key_feature((double)c.key)));
-        if (!(score >= tau_min)) score = 0.0;  // also rejects NaN
-        score = fmin(score, 4.0e18);
-        cand[i].count = (float)score;
-        if (score > 0.0) {
-            const int bin = min(63, max(0, (int)floor(log2(score))));
-            atomicAdd(&bins[bin], 1u);
-            atomicAdd(&mass[bin], (unsigned long long)c.count);
+    const uint64_t lo = (uint64_t)blockIdx.x * CNT_CHUNK;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int u = 0; u < CNT_CHUNK / CNT_THREADS; u++) {
+        const uint64_t i = lo + (uint64_t)u * CNT_THREADS + threadIdx.x;
+        const uint32_t k = i < m ? keys[i] : EMPTY_KEY;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        if (k != EMPTY_KEY && lane == __ffs(peers) - 1) {
+            uint32_t h = count_hash(k) & (SLOTS - 1);
+            for (int probe = 0; probe < SLOTS; probe++) {  // at most CNT_CHUNK keys in 2x the slots
+                const uint32_t old = atomicCAS(&lk[h], EMPTY_KEY, k);
+                if (old == EMPTY_KEY || old == k) {
+                    atomicAdd(&lc[h], (uint32_t)__popc(peers));
+                    break;
+                }
+                h = (h + 1) & (SLOTS - 1);
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < SLOTS; i += CNT_THREADS)
+        if (lk[i] != EMPTY_KEY) table_add(tk, tc, tmask, lk[i], lc[i]);
+}
+
+cudaError_t launch_count_keys(const LearnBufs &b, uint64_t m, cudaStream_t st) {
+    if (!m) return cudaSuccess;
+    k_count_keys<<<(unsigned)((m + CNT_CHUNK - 1) / CNT_CHUNK), CNT_THREADS, 0, st>>>(b.keys, m, b.tkeys, b.tcnt,
+                                                                                      b.tmask);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Bin of a sample count: exact below CC_EXACT, then CC_OCT bins per octave.
+__host__ __device__ __forceinline__ int cc_bin(uint32_t c) {
+    if (c < (uint32_t)CC_EXACT) return (int)c;
+#ifdef __CUDA_ARCH__
+    const int e = 31 - __clz(c);
+#else
+    const int e = 31 - __builtin_clz(c);
+#endif
+    return CC_EXACT + (e - 11) * CC_OCT + (int)((c >> (e - 4)) & (CC_OCT - 1));
+}
+// Smallest count in bin b.
+__host__ __device__ __forceinline__ uint32_t cc_bin_min(int b) {
+    if (b < CC_EXACT) return (uint32_t)b;
+    const int e = 11 + (b - CC_EXACT) / CC_OCT, f = (b - CC_EXACT) % CC_OCT;
+    return (1u << e) | ((uint32_t)f << (e - 4));
+}
+
+// Count-of-counts over the table (keys per bin, sample rows per bin) and the
+// candidate list: the keys the sample saw at least CAND_MIN_COUNT times.
+__global__ void __launch_bounds__(256) k_count_stats(const uint32_t *__restrict__ tk, const uint32_t *__restrict__ tc,
+                                                    uint32_t tmask, unsigned *bin_keys,
+                                                    unsigned long long *bin_rows, HeavyCand *cand,
+                                                    unsigned cand_cap, LrnDecision *dec) {
+    __shared__ unsigned sk[CC_BINS];
+    __shared__ unsigned long long sr[CC_BINS];
+    for (int i = threadIdx.x; i < CC_BINS; i += 256) {
+        sk[i] = 0;
+        sr[i] = 0;
+    }
+    __syncthreads();
+    const uint64_t slots = (uint64_t)tmask + 1;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t base = (uint64_t)blockIdx.x * 256; base < slots; base += (uint64_t)gridDim.x * 256) {
+        const uint64_t i = base + threadIdx.x;  // warp-uniform trip count (slots is a multiple of 256)
+        const uint32_t k = tk[i], c = tc[i];
+        const bool used = k != EMPTY_KEY && c > 0;
+        if (used) {
+            const int b = cc_bin(c);
+            atomicAdd(&sk[b], 1u);
+            atomicAdd(&sr[b], (unsigned long long)c);
+        }
+        const bool is_cand = used && c >= (uint32_t)CAND_MIN_COUNT;
+        const unsigned bal = __ballot_sync(0xffffffffu, is_cand);
+        unsigned wb = 0;
+        if (lane == 0 && bal) wb = atomicAdd(&dec->ncand, (unsigned)__popc(bal));
+        wb = __shfl_sync(0xffffffffu, wb, 0);
+        const unsigned pos = wb + __popc(bal & lanemask_lt());
+        if (is_cand && pos < cand_cap) cand[pos] = HeavyCand{k, c};
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < CC_BINS; i += 256) {
+        if (sk[i]) {
+            atomicAdd(&bin_keys[i], sk[i]);
+            atomicAdd(&bin_rows[i], sr[i]);
         }
     }
 }
 
-cudaError_t launch_heavy_score(HeavyCand *cand, unsigned ncand, const float *params, int use_model, double tau_min,
-                               double min_sample, unsigned *bins, unsigned long long *mass, cudaStream_t st) {
-    if (!ncand) return cudaSuccess;
-    k_heavy_score<<<(ncand + 255) / 256, 256, 0, st>>>(cand, ncand, params, use_model, tau_min, min_sample, bins, mass);
+cudaError_t launch_count_stats(const LearnBufs &b, cudaStream_t st) {
+    const uint64_t slots = (uint64_t)b.tmask + 1;
+    const unsigned g = (unsigned)umin64(slots / 256, 148 * 4);
+    k_count_stats<<<g, 256, 0, st>>>(b.tkeys, b.tcnt, b.tmask, b.bin_keys, b.bin_rows, b.cand, b.cand_cap, b.dec);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Training points of the frequency model, one per non-empty count bin in
+// decreasing count order: x = rank_feature(mid rank of the bin's keys),
+// y = log2(mean sample count of the bin) / 32.  One block; writes the point
+// count to dec->npoints.
+__global__ void __launch_bounds__(1024) k_rank_points(const unsigned *__restrict__ bin_keys,
+                                                     const unsigned long long *__restrict__ bin_rows, float *xs,
+                                                     float *ys, LrnDecision *dec) {
+    constexpr int PER = (CC_BINS + 1023) / 1024;
+    __shared__ uint64_t scratch[1024 / 32 + 1];
+    // thread t owns reversed bins [t * PER, t * PER + PER): descending counts
+    const int t = threadIdx.x;
+    uint64_t keys_here = 0, pts_here = 0;
+    for (int j = 0; j < PER; j++) {
+        const int r = t * PER + j;
+        if (r < CC_BINS) {
+            const unsigned nk = bin_keys[CC_BINS - 1 - r];
+            keys_here += nk;
+            pts_here += nk ? 1 : 0;
+        }
+    }
+    uint64_t tot_keys, tot_pts;
+    uint64_t above = block_excl_scan<1024>(keys_here, &tot_keys, scratch);
+    uint64_t pt = block_excl_scan<1024>(pts_here, &tot_pts, scratch);
+    for (int j = 0; j < PER; j++) {
+        const int r = t * PER + j;
+        if (r >= CC_BINS) break;
+        const int b = CC_BINS - 1 - r;
+        const unsigned nk = bin_keys[b];
+        if (!nk) continue;
+        const double mid = (double)above + 0.5 * (double)(nk + 1);
+        xs[pt] = rank_feature(mid);
+        ys[pt] = (float)(log2((double)bin_rows[b] / (double)nk) / 32.0);
+        pt++;
+        above += nk;
+    }
+    if (t == 0) dec->npoints = (unsigned)tot_pts;
+}
+
+cudaError_t launch_rank_points(const LearnBufs &b, cudaStream_t st) {
+    k_rank_points<<<1, 1024, 0, st>>>(b.bin_keys, b.bin_rows, b.xs, b.ys, b.dec);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// The decision (one block).  pred(r), the predicted S rows of the key of
+// sample rank r, comes from the model (2^(32 M(rank_feature(r))) nS / m) or,
+// for the ablation, from the sample's own count at rank r.  k* = the ranks
+// 1 .. HEAVY_MAX whose predicted rows reach tau_min; the heavy keys are the
+// sampled keys whose count is at least that of rank k* (the lowest count bin
+// that keeps their number <= k*).  Bypass when the model predicts those keys
+// to hold at least min_frac of S.  Also the model's loss on the points.
+constexpr int DECIDE_THREADS = 512;
+
+__global__ void __launch_bounds__(DECIDE_THREADS) k_decide(const float *__restrict__ params, int use_model,
+                                                          const unsigned *__restrict__ bin_keys,
+                                                          const unsigned long long *__restrict__ bin_rows,
+                                                          const float *__restrict__ xs, const float *__restrict__ ys,
+                                                          double nS, double m, double tau_min, double min_frac,
+                                                          LrnDecision *dec) {
+    __shared__ float p[MLP_PARAMS];
+    __shared__ uint32_t cnt_at[HEAVY_MAX + 2];  // sample count of rank r (r = 1 .. HEAVY_MAX + 1)
+    __shared__ float lpred[HEAVY_MAX + 2];      // log2 of the predicted S rows of rank r
+    __shared__ double red[DECIDE_THREADS / 32];
+    __shared__ unsigned s_kstar;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    for (int q = t; q < MLP_PARAMS; q += DECIDE_THREADS) p[q] = params[q];
+    for (int r = t; r <= HEAVY_MAX + 1; r += DECIDE_THREADS) cnt_at[r] = 0;
+    if (t == 0) s_kstar = 0;
+    __syncthreads();
+    // ranks 1 .. HEAVY_MAX + 1 sit in the highest bins: thread 0 walks them
+    if (t == 0) {
+        unsigned r = 1;
+        for (int b = CC_BINS - 1; b >= 1 && r <= (unsigned)HEAVY_MAX + 1; b--) {
+            const unsigned nk = bin_keys[b];
+            if (!nk) continue;
+            const uint32_t c = (uint32_t)(bin_rows[b] / nk);
+            for (unsigned j = 0; j < nk && r <= (unsigned)HEAVY_MAX + 1; j++) cnt_at[r++] = c;
+        }
+    }
+    __syncthreads();
+    const double lscale = log2(nS / m);
+    for (int r = 1 + t; r <= HEAVY_MAX + 1; r += DECIDE_THREADS)
+        lpred[r] = use_model ? (float)(32.0 * (double)mlp_eval(p, rank_feature((double)r)) + lscale)
+                             : (cnt_at[r] ? (float)(log2((double)cnt_at[r]) + lscale) : -INFINITY);
+    __syncthreads();
+    // k*: the largest rank <= HEAVY_MAX predicted at or above tau_min among the
+    // ranks the sample saw at least CAND_MIN_COUNT times
+    const float ltau = (float)log2(tau_min);
+    unsigned last_ok = 0;
+    for (int r = 1 + t; r <= HEAVY_MAX; r += DECIDE_THREADS)
+        if (lpred[r] >= ltau && cnt_at[r] >= (uint32_t)CAND_MIN_COUNT) last_ok = max(last_ok, (unsigned)r);
+    for (int o = 16; o > 0; o >>= 1) last_ok = max(last_ok, __shfl_xor_sync(0xffffffffu, last_ok, o));
+    if (lane == 0 && last_ok) atomicMax(&s_kstar, last_ok);
+    __syncthreads();
+    const unsigned kstar = s_kstar;
+    double mass = 0.0;
+    for (int r = 1 + t; r <= (int)kstar; r += DECIDE_THREADS) mass += exp2((double)lpred[r]);
+    // the model's mean squared error on the training points
+    const unsigned np = dec->npoints;
+    double loss = 0.0;
+    for (unsigned i = t; i < np; i += DECIDE_THREADS) {
+        const double d = (double)mlp_eval(p, xs[i]) - (double)ys[i];
+        loss += d * d;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mass += __shfl_xor_sync(0xffffffffu, mass, o);
+        loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    }
+    if (lane == 0) red[w] = mass;
+    __syncthreads();
+    double pred_mass = 0.0;
+    for (int i = 0; i < DECIDE_THREADS / 32; i++) pred_mass += red[i];
+    __syncthreads();
+    if (lane == 0) red[w] = loss;
+    __syncthreads();
+    if (t == 0) {
+        double lsum = 0;
+        for (int i = 0; i < DECIDE_THREADS / 32; i++) lsum += red[i];
+        // count threshold: the lowest bin whose keys, with all above it, number <= k*
+        unsigned above = 0, count_min = 0xFFFFFFFFu, heavy = 0;
+        unsigned long long rows = 0;
+        for (int b = CC_BINS - 1; b >= CAND_MIN_COUNT && kstar; b--) {
+            const unsigned nk = bin_keys[b];
+            if (!nk) continue;
+            if (above + nk > kstar) break;
+            above += nk;
+            rows += bin_rows[b];
+            count_min = cc_bin_min(b);
+            heavy = above;
+        }
+        LrnDecision d = *dec;
+        d.k_star = kstar;
+        d.count_min = count_min;
+        d.heavy_sample = heavy;
+        d.pred_mass = pred_mass;
+        d.sample_mass = (double)rows * (nS / m);
+        d.next_rows = kstar < (unsigned)HEAVY_MAX ? exp2((double)lpred[kstar + 1]) : 0.0;
+        d.loss = np ? (float)(lsum / np) : 0.f;
+        d.bypass = heavy > 0 && pred_mass >= min_frac * nS ? 1u : 0u;
+        *dec = d;
+    }
+}
+
+cudaError_t launch_decide(const LearnBufs &b, int use_model, double nS, double m, double tau_min, double min_frac,
+                          cudaStream_t st) {
+    k_decide<<<1, DECIDE_THREADS, 0, st>>>(b.params, use_model, b.bin_keys, b.bin_rows, b.xs, b.ys, nS, m, tau_min, min_frac,
+                                 b.dec);
     count_launch();
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// heavy table: open addressing on the key, HEAVY_CAP slots, key EMPTY_KEY
-// marks a free slot; val = R rows with the key, start = first of them in the
-// heavy R payload list (materialisation).
+// heavy table: HEAVY_BUCKETS buckets of 4 key slots; key EMPTY_KEY marks a
+// free slot (so EMPTY_KEY itself is never heavy).  A key goes to the first
+// free slot of its bucket, or of the next buckets when that one is full;
+// slots fill in order and are never freed, so a lookup stops at the first
+// bucket with a free slot (at <= 50% load almost always the first).  Slot s
+// = 4 * bucket + i indexes cnt (R rows with the key) and start (first of them
+// in the heavy R payload list, materialisation).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t heavy_hash(uint32_t k) { return (k * 0x9E3779B1u) >> (32 - HEAVY_LOG2); }
+__device__ __forceinline__ uint32_t heavy_bucket(uint32_t k) { return (k * 0x9E3779B1u) >> (32 - HEAVY_LOG2 + 2); }
 __device__ __forceinline__ uint32_t filter_bit(uint32_t k) { return (k * 0x85EBCA6Bu) >> (32 - FILTER_LOG2); }
 
 __device__ __forceinline__ int heavy_find(const uint32_t *keys, uint32_t k) {
-    uint32_t h = heavy_hash(k);
-    for (int probe = 0; probe < HEAVY_CAP; probe++) {
-        const uint32_t x = keys[h];
-        if (x == k) return (int)h;
-        if (x == EMPTY_KEY) return -1;
-        h = (h + 1) & (HEAVY_CAP - 1);
+    if (k == EMPTY_KEY) return -1;
+    uint32_t b = heavy_bucket(k);
+    for (int probe = 0; probe < HEAVY_BUCKETS; probe++) {
+        const uint4 q = reinterpret_cast<const uint4 *>(keys)[b];
+        const int i = q.x == k ? 0 : q.y == k ? 1 : q.z == k ? 2 : q.w == k ? 3 : -1;
+        if (i >= 0) return (int)(4 * b) + i;
+        if (q.w == EMPTY_KEY) return -1;  // slots fill in order: a free last slot ends the search
+        b = (b + 1) & (HEAVY_BUCKETS - 1);
     }
     return -1;
 }
 
-__global__ void k_heavy_build(const HeavyCand *__restrict__ cand, unsigned ncand, float tau, uint32_t *keys,
-                              uint32_t *filter, unsigned *inserted) {
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
-        if (!(cand[i].count >= tau)) continue;
-        if (atomicAdd(inserted, 1u) >= HEAVY_MAX) continue;
-        const uint32_t k = cand[i].key;
-        const uint32_t fb = filter_bit(k);
-        atomicOr(&filter[fb >> 5], 1u << (fb & 31));
-        uint32_t h = heavy_hash(k);
-        for (int probe = 0; probe < HEAVY_CAP; probe++) {
-            const uint32_t old = atomicCAS(&keys[h], EMPTY_KEY, k);
-            if (old == EMPTY_KEY || old == k) break;
-            h = (h + 1) & (HEAVY_CAP - 1);
+__device__ __forceinline__ void heavy_insert(uint32_t *keys, uint32_t k) {
+    uint32_t b = heavy_bucket(k);
+    for (int probe = 0; probe < HEAVY_BUCKETS; probe++) {
+        for (int i = 0; i < 4; i++) {
+            const uint32_t old = atomicCAS(&keys[4 * b + i], EMPTY_KEY, k);
+            if (old == EMPTY_KEY || old == k) return;
         }
+        b = (b + 1) & (HEAVY_BUCKETS - 1);
     }
 }
 
-cudaError_t launch_heavy_build(const HeavyCand *cand, unsigned ncand, float tau, uint32_t *keys, uint32_t *filter,
-                               unsigned *inserted, cudaStream_t st) {
-    if (!ncand) return cudaSuccess;
-    k_heavy_build<<<(ncand + 255) / 256, 256, 0, st>>>(cand, ncand, tau, keys, filter, inserted);
+// Inserts the candidates whose sample count reaches the decision's
+// count_min (at most HEAVY_MAX of them; the decision keeps their number at
+// or below k* <= HEAVY_MAX) and sets their filter bits.
+__global__ void k_heavy_build(const HeavyCand *__restrict__ cand, unsigned cand_cap, const LrnDecision *dec,
+                              uint32_t *keys, uint32_t *filter, unsigned *inserted) {
+    const unsigned n = min(dec->ncand, cand_cap);
+    const unsigned cmin = dec->count_min;
+    if (!dec->bypass) return;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const HeavyCand c = cand[i];
+        if (c.count < cmin || c.key == EMPTY_KEY) continue;
+        if (atomicAdd(inserted, 1u) >= (unsigned)HEAVY_MAX) continue;
+        const uint32_t fb = filter_bit(c.key);
+        atomicOr(&filter[fb >> 5], 1u << (fb & 31));
+        heavy_insert(keys, c.key);
+    }
+}
+
+cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, uint32_t *filter, unsigned *inserted,
+                               cudaStream_t st) {
+    k_heavy_build<<<148 * 2, 256, 0, st>>>(b.cand, b.cand_cap, b.dec, keys, filter, inserted);
     count_launch();
     return cudaGetLastError();
 }
@@ -536,13 +735,44 @@ cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const
 // rows out), every other row is counted in its radix bin and appended to
 // the chunk's region of the compacted S (warp-aggregated, coalesced).
 // ---------------------------------------------------------------------------
+// Heavy check of one row against the filter and the table in shared memory:
+// the row's slot, or -1.
+__device__ __forceinline__ int heavy_slot(const uint32_t *filt, const uint32_t *hkeys, uint32_t k) {
+    const uint32_t fb = filter_bit(k);
+    if (!((filt[fb >> 5] >> (fb & 31)) & 1u)) return -1;
+    return heavy_find(hkeys, k);
+}
+
+// One row outside the vector body (the chunk's first row when it starts 8
+// bytes past a 16-byte boundary, or its last row): thread 0 only.
+template <bool MAT>
+__device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *filt, const uint32_t *hkeys,
+                                const unsigned *hcnt, uint32_t *hist, unsigned *s_keep, uint2 *dst, Row x,
+                                unsigned long long &matches, unsigned long long &heavy_rows) {
+    const int s = heavy_slot(filt, hkeys, x.key);
+    if (s < 0) {
+        atomicAdd(&hist[radix_f(a.rf, x.key)], 1u);
+        dst[atomicAdd(s_keep, 1u)] = make_uint2(x.key, x.payload);
+        return;
+    }
+    const unsigned c = hcnt[s];
+    matches += c;
+    heavy_rows++;
+    if (MAT && c) {
+        uint64_t op = atomicAdd(a.rows_ctr, (unsigned long long)c);
+        const unsigned st0 = a.hstart[s];
+        for (unsigned q = 0; q < c; q++, op++)
+            if (op < a.cap) a.rows[op] = tbg_row_out{x.key, a.rpay[st0 + q], x.payload};
+    }
+}
+
 template <bool MAT>
 __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
-    uint32_t *filt = hist + a.nbins;              // 2^FILTER_LOG2 bits
-    uint32_t *hkeys = filt + (1 << FILTER_LOG2) / 32;
+    uint32_t *hkeys = reinterpret_cast<uint32_t *>(smem);  // 16-byte aligned buckets
     unsigned *hcnt = hkeys + HEAVY_CAP;
+    uint32_t *filt = hcnt + HEAVY_CAP;                     // 2^FILTER_LOG2 bits
+    uint32_t *hist = filt + (1 << FILTER_LOG2) / 32;
     __shared__ unsigned s_keep;
     __shared__ uint64_t scan_scratch[1024 / 32 + 1];
     const int tid = threadIdx.x, lane = tid & 31;
@@ -556,44 +786,45 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     __syncthreads();
     const uint64_t lo = (uint64_t)blockIdx.x * a.chunk;
     const uint64_t hi = umin64(a.n, lo + a.chunk);
-    const uint64_t len = hi > lo ? hi - lo : 0;
+    const uint32_t len = hi > lo ? (uint32_t)(hi - lo) : 0u;  // a chunk holds < 2^32 rows
     const Row *src = a.in + lo;
     uint2 *dst = reinterpret_cast<uint2 *>(a.out + lo);
-    const bool vec = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+    const uint32_t head = (len && (reinterpret_cast<uintptr_t>(src) & 15)) ? 1u : 0u;
+    const uint32_t npairs = (len - head) / 2;
+    const bool tail = ((len - head) & 1) != 0;
+    const uint4 *v = reinterpret_cast<const uint4 *>(src + head);
     unsigned long long matches = 0, heavy_rows = 0;
-    // rounds of 8 rows per thread: row pairs p = base/2 + u * 1024 + tid
-    for (uint64_t base = 0; base < len; base += 8 * 1024) {
-        uint32_t k[8], v[8];
-        int slot[8];
-        unsigned keep = 0, emit = 0, nheavy = 0;
+    // rounds of 4 row pairs per thread: pair p = base + u * 1024 + tid
+    for (uint32_t base = 0; base < npairs; base += 4 * 1024) {
+        uint32_t k[8], pv[8];
+        unsigned valid = 0;
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const uint64_t r = base + 2 * ((uint64_t)u * 1024 + tid);
-            if (vec && r + 1 < len) {
-                const uint4 x = ldg_stream(reinterpret_cast<const uint4 *>(src + r));
-                k[2 * u] = x.x; v[2 * u] = x.y; k[2 * u + 1] = x.z; v[2 * u + 1] = x.w;
-            } else {
-                k[2 * u] = k[2 * u + 1] = 0; v[2 * u] = v[2 * u + 1] = 0;
-                if (r < len) { const uint2 x = ldg_stream(reinterpret_cast<const uint2 *>(src + r)); k[2 * u] = x.x; v[2 * u] = x.y; }
-                if (r + 1 < len) { const uint2 x = ldg_stream(reinterpret_cast<const uint2 *>(src + r + 1)); k[2 * u + 1] = x.x; v[2 * u + 1] = x.y; }
-            }
-            const uint32_t valid = (r < len ? 1u : 0u) | (r + 1 < len ? 2u : 0u);
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int j = 2 * u + h;
-                slot[j] = -1;
-                const uint32_t fb = filter_bit(k[j]);
-                if ((valid >> h & 1) && (filt[fb >> 5] >> (fb & 31) & 1)) slot[j] = heavy_find(hkeys, k[j]);
-                if (slot[j] >= 0) {
-                    emit += hcnt[slot[j]];
-                    nheavy++;
-                } else if (valid >> h & 1) {
-                    keep |= 1u << j;
-                }
+            const uint32_t p = base + u * 1024 + tid;
+            k[2 * u] = k[2 * u + 1] = EMPTY_KEY;
+            pv[2 * u] = pv[2 * u + 1] = 0;
+            if (p < npairs) {
+                const uint4 x = ldg_stream(v + p);
+                k[2 * u] = x.x;
+                pv[2 * u] = x.y;
+                k[2 * u + 1] = x.z;
+                pv[2 * u + 1] = x.w;
+                valid |= 3u << (2 * u);
             }
         }
-        matches += emit;
-        heavy_rows += nheavy;
+        int slot[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) slot[j] = (valid >> j & 1) ? heavy_slot(filt, hkeys, k[j]) : -1;
+        unsigned keep = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (slot[j] >= 0) {
+                matches += hcnt[slot[j]];
+                heavy_rows++;
+            } else if (valid >> j & 1) {
+                keep |= 1u << j;
+            }
+        }
         // coalesced compaction: one ballot per row slot, one shared atomic per warp
         unsigned m[8], wtot = 0;
 #pragma unroll
@@ -609,7 +840,7 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
         for (int j = 0; j < 8; j++) {
             if (keep >> j & 1) {
                 atomicAdd(&hist[radix_f(a.rf, k[j])], 1u);
-                dst[wb + __popc(m[j] & lt)] = make_uint2(k[j], v[j]);
+                dst[wb + __popc(m[j] & lt)] = make_uint2(k[j], pv[j]);
             }
             wb += __popc(m[j]);
         }
@@ -627,10 +858,15 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
                     const unsigned st0 = a.hstart[slot[j]];
                     uint64_t op = pos[j];
                     for (unsigned q = 0; q < c[j]; q++, op++)
-                        if (op < a.cap) a.rows[op] = tbg_row_out{k[j], a.rpay[st0 + q], v[j]};
+                        if (op < a.cap) a.rows[op] = tbg_row_out{k[j], a.rpay[st0 + q], pv[j]};
                 }
             }
         }
+    }
+    __syncthreads();  // every vector row is counted: the edge rows take the next output slots
+    if (tid == 0) {
+        if (head) bypass_edge_row<MAT>(a, filt, hkeys, hcnt, hist, &s_keep, dst, src[0], matches, heavy_rows);
+        if (tail) bypass_edge_row<MAT>(a, filt, hkeys, hcnt, hist, &s_keep, dst, src[len - 1], matches, heavy_rows);
     }
     __syncthreads();
     uint32_t *hdst = a.hist + (uint64_t)blockIdx.x * a.nbins;
@@ -644,8 +880,8 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
 }
 
 size_t bypass_smem(int nbins, bool mat) {
-    (void)mat;  // 2^15 bins + filter + keys + counts: 204,800 B at most
-    return (size_t)nbins * 4 + (1 << FILTER_LOG2) / 8 + (size_t)HEAVY_CAP * 4 * 2;
+    (void)mat;  // heavy keys + counts + filter + 2^15 bins: 204,800 B at most
+    return (size_t)HEAVY_CAP * 4 * 2 + (1 << FILTER_LOG2) / 8 + (size_t)nbins * 4;
 }
 
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st) {

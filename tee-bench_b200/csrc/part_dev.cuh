@@ -96,6 +96,18 @@ struct DigitOp {
     __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return (key >> shift) & mask; }
 };
 
+// Destination shard of a key for a join split over n shards (n <= 256): the
+// top bits of a multiplicative hash, range-reduced by a multiply-shift, so
+// every shard gets an even share of the keys whatever their order or skew,
+// and the low key bits that the shards' own radix passes use stay evenly
+// spread inside each shard.
+struct ShardOp {
+    uint32_t n;
+    __host__ __device__ __forceinline__ uint32_t operator()(uint32_t key) const {
+        return (uint32_t)(((uint64_t)(key * 0x9E3779B1u) * n) >> 32);
+    }
+};
+
 // Where tile rows [t, t + cnt) sit in a shared buffer: the bulk copy moves
 // the 16-byte aligned rows [a_lo, a_hi); row r is at buffer index r + off so
 // the copy's destination is 16-byte aligned too; edge rows outside the copy
@@ -137,8 +149,8 @@ __device__ __forceinline__ void issue_tile(const Row *in, const TileGeo &g, Row 
 // q & 1.
 
 // Waits for tile q and ranks its rows on cnt[q & 1].
-template <int THREADS, bool FULL>
-__device__ __forceinline__ void tile_load_rank(const Row *__restrict__ in, const TileGeo &g, uint32_t q, DigitOp dop,
+template <int THREADS, bool FULL, class Dig>
+__device__ __forceinline__ void tile_load_rank(const Row *__restrict__ in, const TileGeo &g, uint32_t q, Dig dop,
                                                PartSmem<THREADS> &sm, uint64_t *mbar, uint2 (&v)[PART_ITEMS],
                                                uint32_t (&rank)[PART_ITEMS], unsigned *err) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -206,8 +218,8 @@ __device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS> &
 }
 
 // Stages tile q's rows digit-sorted into its own buffer.
-template <int THREADS, bool FULL>
-__device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, DigitOp dop, PartSmem<THREADS> &sm,
+template <int THREADS, bool FULL, class Dig>
+__device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, Dig dop, PartSmem<THREADS> &sm,
                                            const uint2 (&v)[PART_ITEMS], const uint32_t (&rank)[PART_ITEMS]) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
@@ -223,9 +235,9 @@ __device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, DigitOp
 }
 
 // Writes staged tile q (cnt rows) to out, by threads [t0, THREADS).
-template <int THREADS>
+template <int THREADS, class Dig>
 __device__ __forceinline__ void tile_write(uint32_t q, uint32_t cnt, uint2 *__restrict__ out, uint32_t out_n,
-                                           DigitOp dop, PartSmem<THREADS> &sm, int t0, unsigned *err) {
+                                           Dig dop, PartSmem<THREADS> &sm, int t0, unsigned *err) {
     if ((int)threadIdx.x < t0) return;
     const Row *buf = sm.buf[q % PART_NBUF];
     const uint32_t *dl = sm.delta[q & 1];
@@ -247,9 +259,9 @@ __device__ __forceinline__ TileGeo range_tile(const Row *in, uint64_t lo, uint64
 // the caller initialises sm.cursor[0..F) and synchronises.  Three barriers
 // per tile; `kseq` is the CTA's running tile count (see above), and the
 // barriers mbar[0..PART_NBUF) are initialised once by the caller.
-template <int THREADS>
+template <int THREADS, class Dig>
 __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
-                           uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm, uint64_t *mbar,
+                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS> &sm, uint64_t *mbar,
                            uint32_t &kseq, unsigned *err) {
     constexpr uint32_t T = THREADS * PART_ITEMS;
     uint2 *o = reinterpret_cast<uint2 *>(out);
@@ -268,35 +280,35 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
         const TileGeo g = range_tile(in, lo, hi, k, T);
         uint2 v[PART_ITEMS];
         uint32_t rank[PART_ITEMS];
-        if (g.cnt == T) tile_load_rank<THREADS, true>(in, g, q, dop, sm, mbar, v, rank, err);
-        else tile_load_rank<THREADS, false>(in, g, q, dop, sm, mbar, v, rank, err);
+        if (g.cnt == T) tile_load_rank<THREADS, true, Dig>(in, g, q, dop, sm, mbar, v, rank, err);
+        else tile_load_rank<THREADS, false, Dig>(in, g, q, dop, sm, mbar, v, rank, err);
         __syncthreads();
         if (threadIdx.x < 32) tile_scan<THREADS>(q, F, sm);
-        else if (k > 0) tile_write<THREADS>(q - 1, prev_cnt, o, out_n, dop, sm, 32, err);
+        else if (k > 0) tile_write<THREADS, Dig>(q - 1, prev_cnt, o, out_n, dop, sm, 32, err);
         __syncthreads();
         // tile q - 1's buffer is free: copy tile k + 2 into it
         if (threadIdx.x == 0 && k + 2 < ntiles)
             issue_tile(in, range_tile(in, lo, hi, k + 2, T), sm.buf[(q + 2) % PART_NBUF], &mbar[(q + 2) % PART_NBUF]);
-        if (g.cnt == T) tile_stage<THREADS, true>(g, q, dop, sm, v, rank);
-        else tile_stage<THREADS, false>(g, q, dop, sm, v, rank);
+        if (g.cnt == T) tile_stage<THREADS, true, Dig>(g, q, dop, sm, v, rank);
+        else tile_stage<THREADS, false, Dig>(g, q, dop, sm, v, rank);
         __syncthreads();
         prev_cnt = g.cnt;
     }
-    tile_write<THREADS>(kseq + ntiles - 1, prev_cnt, o, out_n, dop, sm, 0, err);
+    tile_write<THREADS, Dig>(kseq + ntiles - 1, prev_cnt, o, out_n, dop, sm, 0, err);
     __syncthreads();  // every buffer is free again
     kseq += ntiles;
 }
 
 // One range per CTA: initialises the barriers held in `sm`.
-template <int THREADS>
+template <int THREADS, class Dig>
 __device__ void part_range(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
-                           uint32_t out_n, DigitOp dop, int F, PartSmem<THREADS> &sm, unsigned *err) {
+                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS> &sm, unsigned *err) {
     if (threadIdx.x == 0) {
         for (int i = 0; i < PART_NBUF; i++) mbar_init(&sm.mbar[i], 1);
         fence_mbar_init();
     }
     uint32_t kseq = 0;
-    part_tiles<THREADS>(in, lo, hi, out, out_n, dop, F, sm, sm.mbar, kseq, err);
+    part_tiles<THREADS, Dig>(in, lo, hi, out, out_n, dop, F, sm, sm.mbar, kseq, err);
 }
 
 }  // namespace tbg

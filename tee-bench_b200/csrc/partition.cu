@@ -25,6 +25,16 @@
 
 namespace tbg {
 
+// Threads per CTA of the two passes (tiles of THREADS * PART_ITEMS rows).
+#ifndef TBG_PASS1_THREADS
+#define TBG_PASS1_THREADS 512
+#endif
+#ifndef TBG_PASS2_THREADS
+#define TBG_PASS2_THREADS 512
+#endif
+constexpr int PASS1_THREADS = TBG_PASS1_THREADS;
+constexpr int PASS2_THREADS = TBG_PASS2_THREADS;
+
 // ---------------------------------------------------------------------------
 // K1 per-chunk histogram over the final partition index f
 // ---------------------------------------------------------------------------
@@ -248,9 +258,10 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
 // ---------------------------------------------------------------------------
 // K4 pass 1: CTA c scatters chunk c by d1.  With one pass, d1 is f itself.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_part_pass1(PartArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto &sm = *reinterpret_cast<PartSmem<PART_THREADS> *>(smem_raw);
+    auto &sm = *reinterpret_cast<PartSmem<THREADS> *>(smem_raw);
     const int c = blockIdx.x, tid = threadIdx.x;
     const int P = 1 << (a.b1 + a.b2);
     const int F = 1 << a.b1;
@@ -259,14 +270,14 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
     // cursors: sum the chunk's prefix over each pass-1 digit's final partitions
     // (delta[0] holds the chunk's row count per pass-1 digit until the scatter)
     uint32_t *rows1 = sm.delta[0];
-    for (int i = tid; i < F; i += PART_THREADS) {
+    for (int i = tid; i < F; i += THREADS) {
         sm.cursor[i] = 0;
         rows1[i] = 0;
     }
     __syncthreads();
     {
         // each thread sums a contiguous run of f (one pass-1 digit per flush)
-        const int per = P >= PART_THREADS ? P / PART_THREADS : 1;
+        const int per = P >= THREADS ? P / THREADS : 1;
         const int f0 = tid * per;
         uint32_t acc_c = 0, acc_t = 0;
         int cur_s = -1;
@@ -289,7 +300,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
         }
     }
     __syncthreads();
-    for (int s = tid; s < F; s += PART_THREADS) {
+    for (int s = tid; s < F; s += THREADS) {
         const uint32_t cur = (uint32_t)a.base[(uint64_t)s << a.b2] + sm.cursor[s];
         sm.cursor[s] = cur;
         if (a.off1) {
@@ -301,15 +312,16 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass1(PartArgs a) {
     const uint64_t lo = (uint64_t)c * a.chunk;
     const uint64_t hi = a.chunk_len ? lo + a.chunk_len[c] : umin64(a.n, lo + a.chunk);
     DigitOp dop{0u, (uint32_t)F - 1};
-    part_range<PART_THREADS>(a.in, lo, hi, a.out, (uint32_t)a.n, dop, F, sm, a.err);
+    part_range<THREADS>(a.in, lo, hi, a.out, (uint32_t)a.n, dop, F, sm, a.err);
 }
 
 // ---------------------------------------------------------------------------
 // K5 pass 2: unit (c, s), s-major, scatters by d2 within pass-1 partition s.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass2(PartArgs a) {
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_part_pass2(PartArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto &sm = *reinterpret_cast<PartSmem<PART_THREADS> *>(smem_raw);
+    auto &sm = *reinterpret_cast<PartSmem<THREADS> *>(smem_raw);
     const int F1 = 1 << a.b1, F2 = 1 << a.b2;
     const int P = F1 * F2;
     const int ngroups = (a.G + a.group - 1) / a.group;
@@ -321,13 +333,13 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_part_pass2(PartArgs a) {
     const uint64_t lo = a.off1[(uint64_t)c0 * F1 + s];
     const uint64_t hi = (uint64_t)a.off1[(uint64_t)c1 * F1 + s] + a.cnt1[(uint64_t)c1 * F1 + s];
     if (lo >= hi) return;
-    for (int d = threadIdx.x; d < F2; d += PART_THREADS) {
+    for (int d = threadIdx.x; d < F2; d += THREADS) {
         const uint64_t f = ((uint64_t)s << a.b2) | d;
         sm.cursor[d] = (uint32_t)a.base[f] + a.pre[(uint64_t)c0 * P + f];
     }
     __syncthreads();
     DigitOp dop{(uint32_t)a.b1, (uint32_t)F2 - 1};
-    part_range<PART_THREADS>(a.in, lo, hi, a.out, (uint32_t)a.n, dop, F2, sm, a.err);
+    part_range<THREADS>(a.in, lo, hi, a.out, (uint32_t)a.n, dop, F2, sm, a.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -376,20 +388,22 @@ cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st) {
 }
 
 cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st) {
-    const size_t smem = sizeof(PartSmem<PART_THREADS>);
-    cudaError_t e = smem_limit((const void *)k_part_pass1, smem);
+    constexpr int T = PASS1_THREADS;
+    const size_t smem = sizeof(PartSmem<T>);
+    cudaError_t e = smem_limit((const void *)k_part_pass1<T>, smem);
     if (e != cudaSuccess) return e;
-    k_part_pass1<<<a.G, PART_THREADS, smem, st>>>(a);
+    k_part_pass1<T><<<a.G, T, smem, st>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st) {
-    const size_t smem = sizeof(PartSmem<PART_THREADS>);
-    cudaError_t e = smem_limit((const void *)k_part_pass2, smem);
+    constexpr int T = PASS2_THREADS;
+    const size_t smem = sizeof(PartSmem<T>);
+    cudaError_t e = smem_limit((const void *)k_part_pass2<T>, smem);
     if (e != cudaSuccess) return e;
     const uint64_t units = (uint64_t)((a.G + a.group - 1) / a.group) << a.b1;
-    k_part_pass2<<<(unsigned)units, PART_THREADS, smem, st>>>(a);
+    k_part_pass2<T><<<(unsigned)units, T, smem, st>>>(a);
     count_launch();
     return cudaGetLastError();
 }

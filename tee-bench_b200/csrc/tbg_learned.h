@@ -20,9 +20,10 @@ constexpr int MLP_SLICE = 152;        // parameters updated by each CTA
 static_assert(MLP_PARAMS <= MLP_PARAMS_PAD, "parameter stride");
 static_assert(MLP_SLICE * MLP_CLUSTER >= MLP_PARAMS, "every parameter belongs to a slice");
 
-// Heavy-key table (open addressing on the key).
+// Heavy-key table: HEAVY_CAP slots in buckets of 4 (one 16-byte load).
 constexpr int HEAVY_LOG2 = 13;
 constexpr int HEAVY_CAP = 1 << HEAVY_LOG2;
+constexpr int HEAVY_BUCKETS = HEAVY_CAP / 4;
 constexpr int HEAVY_MAX = HEAVY_CAP / 2;  // at most half full
 constexpr uint32_t EMPTY_KEY = 0xFFFFFFFFu;
 constexpr int FILTER_LOG2 = 16;  // bit filter in front of the heavy table (8 KB)
@@ -32,12 +33,43 @@ constexpr int FILTER_LOG2 = 16;  // bit filter in front of the heavy table (8 KB
 #else
 #define TBG_HD
 #endif
-// Model input feature of a key: log2(key + 1) / 16 - 1 maps 0 .. 2^32 onto [-1, 1].
-TBG_HD inline float key_feature(double key) { return (float)(log2(key + 1.0) / 16.0 - 1.0); }
+// Model input: a key's frequency rank r in the sample (1 = most frequent),
+// log2(r + 1) / 16 - 1, which maps ranks 0 .. 2^32 onto [-1, 1].  The rank
+// comes from the sample's counts, never from the key's value, so the model
+// sees the same curve whether hot keys are small integers or scattered over
+// the key range.
+TBG_HD inline float rank_feature(double rank) { return (float)(log2(rank + 1.0) / 16.0 - 1.0); }
+
+// Sample of S: blocks of SAMPLE_BLOCK consecutive rows (coalesced reads).
+constexpr int SAMPLE_BLOCK = 64;
+// Per-CTA shared-memory aggregation of the sample's keys before the global
+// count table: CNT_CHUNK keys per CTA into 2 * CNT_CHUNK slots.
+constexpr int CNT_THREADS = 1024;
+constexpr int CNT_CHUNK = 2048;
+// Count-of-counts bins: exact below CC_EXACT, then CC_OCT bins per octave.
+constexpr int CC_EXACT = 2048;
+constexpr int CC_OCT = 16;
+constexpr int CC_BINS = CC_EXACT + CC_OCT * 21;
+constexpr int CAND_MIN_COUNT = 2;  // sampled keys seen once are never heavy candidates
 
 struct HeavyCand {
     uint32_t key;
-    float count;  // predicted rows of S with this key
+    uint32_t count;  // occurrences in the sample
+};
+
+// What the learning stage decided (device memory, read back once).
+struct LrnDecision {
+    unsigned bypass;          // 1: heavy keys skip partitioning
+    unsigned count_min;       // heavy keys: sample count >= count_min
+    unsigned k_star;          // ranks whose predicted S rows reach the threshold
+    unsigned heavy_sample;    // sampled keys at or above count_min
+    unsigned npoints;         // training points (non-empty count bins)
+    unsigned ncand;           // candidates listed (sample count >= CAND_MIN_COUNT)
+    double pred_mass;         // predicted S rows of ranks 1 .. k_star
+    double sample_mass;       // the sample's estimate of the heavy keys' S rows
+    double next_rows;         // predicted S rows of rank k_star + 1 (largest key left)
+    float loss;               // mean squared error of the model on the points
+    unsigned pad;
 };
 
 struct BypassArgs {
@@ -65,17 +97,31 @@ struct BypassArgs {
 cudaError_t launch_mlp_init(float *params, uint64_t seed, cudaStream_t st);
 cudaError_t launch_mlp_grad(const float *params, const float *xs, const float *ys, uint32_t n, float *grad,
                             float *loss_sum, cudaStream_t st);
-cudaError_t launch_mlp_train(const float *xs, const float *ys, uint32_t n, float *params, int steps, float lr,
-                             uint64_t seed, cudaStream_t st);
-cudaError_t launch_sample(const Row *in, uint64_t n, Row *out, uint64_t m, uint64_t seed, cudaStream_t st);
-cudaError_t launch_candidates(const Row *sorted, uint64_t m, double nS, HeavyCand *cand, unsigned *ncand,
-                              unsigned cand_cap, unsigned *scratch_cnt, cudaStream_t st);
-cudaError_t launch_freq_points(const HeavyCand *cand, unsigned ncand, float *xs, float *ys, uint32_t T,
+cudaError_t launch_mlp_train(const float *xs, const float *ys, const unsigned *n_dev, uint32_t n, float *params,
+                             int steps, float lr, uint64_t seed, cudaStream_t st);
+// Learning stage of LRN (all on the device, learned.cu).
+struct LearnBufs {
+    uint32_t *keys;             // sample keys [m]
+    uint32_t *tkeys, *tcnt;     // global count table [slots]
+    uint32_t tmask;             // slots - 1
+    unsigned *bin_keys;         // [CC_BINS]
+    unsigned long long *bin_rows;  // [CC_BINS]
+    HeavyCand *cand;            // [cand_cap]
+    unsigned cand_cap;
+    float *xs, *ys;             // training points [CC_BINS]
+    float *params;              // MLP parameters
+    LrnDecision *dec;
+    unsigned *err;
+};
+cudaError_t launch_sample_blocks(const Row *S, uint64_t nS, uint32_t *keys, uint64_t nblocks, uint64_t stride,
+                                 uint64_t seed, cudaStream_t st);
+cudaError_t launch_count_keys(const LearnBufs &b, uint64_t m, cudaStream_t st);
+cudaError_t launch_count_stats(const LearnBufs &b, cudaStream_t st);
+cudaError_t launch_rank_points(const LearnBufs &b, cudaStream_t st);
+cudaError_t launch_decide(const LearnBufs &b, int use_model, double nS, double m, double tau_min, double min_frac,
+                          cudaStream_t st);
+cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, uint32_t *filter, unsigned *inserted,
                                cudaStream_t st);
-cudaError_t launch_heavy_score(HeavyCand *cand, unsigned ncand, const float *params, int use_model, double tau_min,
-                               double min_sample, unsigned *bins, unsigned long long *mass, cudaStream_t st);
-cudaError_t launch_heavy_build(const HeavyCand *cand, unsigned ncand, float tau, uint32_t *keys, uint32_t *filter,
-                               unsigned *inserted, cudaStream_t st);
 cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const uint32_t *filter, unsigned *cnt,
                            unsigned *start, unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st);
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st);

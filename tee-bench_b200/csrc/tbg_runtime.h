@@ -32,8 +32,11 @@ struct Workspace {
     DevBuf sorthist;            // PSM sort: per-chunk digit histograms and totals
     DevBuf chain_rows, chain_rel;  // chained join: first join's rows and the relation made of them
     DevBuf aux[8];              // algorithm-specific scratch (sort, learned model)
+    DevBuf shard;               // shard split: per-chunk histograms and totals
     uint32_t epoch = 0;         // last look-back epoch used on `status`
     Ctrl *host_ctrl = nullptr;  // pinned mirror of the control block
+    static constexpr size_t HOST_SMALL_BYTES = 4096;
+    void *host_small = nullptr;  // pinned HOST_SMALL_BYTES: mid-call read-backs (LRN's decision, shard totals)
     cudaEvent_t ev[8];
     cudaStream_t side = nullptr;       // second stream (learned path), created on first use
     cudaEvent_t fork = nullptr, joined = nullptr;
@@ -50,6 +53,7 @@ struct JoinRun {
     int train_steps = 0;
     float train_loss = 0;
     float ms_learn = 0;
+    double heavy_pred = 0, heavy_sampled = 0;
     uint64_t launches = 0;
 };
 

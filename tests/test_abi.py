@@ -140,3 +140,17 @@ print('not reached')
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
     assert r.returncode == 1, r.stderr
     assert "[ERROR]" in r.stderr and "not reached" not in r.stdout
+
+
+def test_shard_of_matches_the_host_rule(tbg):
+    """tbg_shard_of (a host function of the library) and the package's numpy
+    shard_of give every key the same shard."""
+    import numpy as np
+    L = tbg.lib()
+    keys = np.random.default_rng(3).integers(0, 2 ** 32, 2000, dtype=np.uint64).astype(np.uint32)
+    keys[:3] = [0, 1, 0xFFFFFFFF]
+    for n in (1, 2, 3, 7, 8, 256):
+        want = tbg.shard_of(keys, n)
+        got = [L.tbg_shard_of(int(k), n) for k in keys]
+        assert list(want) == got
+        assert want.min() >= 0 and want.max() < n

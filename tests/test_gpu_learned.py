@@ -133,40 +133,49 @@ def test_lrn_dropin(tbg, oracle, cuda):
     assert c == ref and len(rows) == ref
 
 
-def _ablation(tbg, cuda, nR, nS, z):
+def _ablation(tbg, cuda, nR, nS, z, scatter=0):
     tR, pR = dev_relation(cuda, nR)
     tS, pS = dev_relation(cuda, nS)
     tbg.gen_pk(pR, nR, 1)
-    tbg.gen_zipf(pS, nS, nR, z, 0, 2)
+    tbg.gen_zipf(pS, nS, nR, z, scatter, 2)
     cuda.cuda.synchronize()
     out = {}
     for name, algo, model in [("radix", "RHO", 0), ("trained", "LRN", tbg.MODEL_MLP),
                               ("untrained", "LRN", tbg.MODEL_UNTRAINED), ("sample", "LRN", tbg.MODEL_SAMPLE)]:
         cfg = tbg.config(algo, model=model)
         _, m, st = tbg.join_device(cfg, pR, nR, pS, nS)
-        out[name] = (m, st.heavy_rows_S / nS, st.used_fallback, st.train_loss)
+        out[name] = {"count": m, "share": st.heavy_rows_S / nS, "fallback": st.used_fallback,
+                     "loss": st.train_loss, "pred": st.heavy_rows_predicted, "sampled": st.heavy_rows_sampled}
     return out
 
 
-def test_trained_network_gain_over_method_without_it(tbg, cuda):
-    """Same pipeline, same data (Zipf over R's keys, hot keys at small ranks as
-    the reference generator makes them).  At z = 1.0 the trained frequency
-    model routes the heaviest keys (a large share of S) around partitioning,
-    the untrained network picks candidates at random and routes far less.  At
-    z = 0.5 no key is heavy: the trained model predicts that and falls back to
-    radix, the untrained one commits to a bypass that cannot pay.  Results are
-    identical in every case."""
+@pytest.mark.parametrize("scatter", [0, 1], ids=["rank_is_key", "scattered"])
+def test_trained_network_against_sample_counts_and_untrained(tbg, cuda, scatter):
+    """Same pipeline, same data, Zipf over R's keys with the hot keys at small
+    ranks or scattered.  The heavy keys are always the sample's most frequent
+    ones; the model predicts how many S rows the top ranks hold, which sets
+    how many keys bypass and whether the bypass runs at all.
+
+    * Trained, the network's prediction of the heavy keys' rows is within 25%
+      of the sample's own estimate at z = 1.0 and its decisions equal the
+      raw-count method's: it matches the method without the network, it does
+      not beat it (both pick the same keys).
+    * Untrained (its initialisation), the prediction is off by orders of
+      magnitude, and at z = 0.5, where no key is heavy enough to pay, it
+      commits to a bypass that the trained model and the sample both reject.
+    * Counts are identical in every case."""
     nR, nS = 1 << 22, 1 << 25
-    o = _ablation(tbg, cuda, nR, nS, 1.0)
-    counts = {k: v[0] for k, v in o.items()}
-    assert len(set(counts.values())) == 1 and counts["radix"] == nS
-    assert o["trained"][2] == 0 and o["trained"][1] > 0.30, o
-    assert o["untrained"][1] < o["trained"][1] - 0.10, o
-    assert o["trained"][1] > 0.8 * o["sample"][1], o
-    o = _ablation(tbg, cuda, nR, nS, 0.5)
-    assert len({v[0] for v in o.values()}) == 1
-    assert o["trained"][2] == 1, o          # predicted no heavy mass: radix
-    assert o["sample"][2] == 1, o
+    o = _ablation(tbg, cuda, nR, nS, 1.0, scatter)
+    assert len({v["count"] for v in o.values()}) == 1 and o["radix"]["count"] == nS
+    t, smp, u = o["trained"], o["sample"], o["untrained"]
+    assert t["fallback"] == 0 and smp["fallback"] == 0, o
+    assert t["share"] > 0.30 and abs(t["share"] - smp["share"]) < 0.02, o
+    assert abs(t["pred"] - t["sampled"]) < 0.25 * t["sampled"], o
+    assert u["pred"] > 4 * nS or u["pred"] < 0.25 * u["sampled"], o
+    o = _ablation(tbg, cuda, nR, nS, 0.5, scatter)
+    assert len({v["count"] for v in o.values()}) == 1
+    assert o["trained"]["fallback"] == 1 and o["sample"]["fallback"] == 1, o
+    assert o["untrained"]["fallback"] == 0, o
 
 
 def test_full_size_skewed_config(tbg, cuda):
@@ -181,3 +190,31 @@ def test_full_size_skewed_config(tbg, cuda):
     _, m0, st0 = tbg.join_device(tbg.config("RHO"), pR, nR, pS, nS)
     assert m0 == m1 == nS
     assert st1.used_fallback == 0 and st1.heavy_rows_S > nS // 3
+
+
+C3_CASES = [(0.0, 0), (0.5, 0), (1.5, 0), (0.5, 1), (1.0, 1), (1.5, 1)]
+
+
+@pytest.mark.parametrize("z,scatter", C3_CASES, ids=[f"z{z}-{'scattered' if s else 'rank_is_key'}"
+                                                    for z, s in C3_CASES])
+def test_full_size_c3_configs(tbg, cuda, z, scatter):
+    """|R| = 2^26, |S| = 2^29 Zipf over R's keys at every exponent of the
+    skewed configuration, with the hot keys at small ranks (rank = key, as
+    the reference's generator leaves them) or scattered over the key range
+    by a seeded permutation.  LRN, RHO with the skew split and plain RHO all
+    count |S|; what LRN chose is printed."""
+    nR, nS = 1 << 26, 1 << 29
+    tR, pR = dev_relation(cuda, nR)
+    tS, pS = dev_relation(cuda, nS)
+    tbg.gen_pk(pR, nR, 11111)
+    tbg.gen_zipf(pS, nS, nR, z, scatter, 22222)
+    cuda.cuda.synchronize()
+    _, m1, st1 = tbg.join_device(tbg.config("LRN"), pR, nR, pS, nS)
+    _, m0, _ = tbg.join_device(tbg.config("RHO"), pR, nR, pS, nS)
+    _, m2, st2 = tbg.join_device(tbg.config("RHO", skew_split=0), pR, nR, pS, nS)
+    assert m0 == m1 == m2 == nS
+    print(f"\n[c3] z={z} scattered={scatter} lrn: fallback={st1.used_fallback} heavy_keys={st1.heavy_keys} "
+          f"heavy_share={st1.heavy_rows_S / nS:.3f} loss={st1.train_loss:.3e} max_part_S={st1.max_part_S} "
+          f"plain max_part_S={st2.max_part_S} mean={nS / st2.partitions:.0f}")
+    if z == 0.0:
+        assert st1.used_fallback == 1 and st1.heavy_rows_S == 0

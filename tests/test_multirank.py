@@ -64,6 +64,7 @@ def test_single_process_needs_no_group():
 
 def _sharded_rank(rank, world, port, q):
     import datetime
+    import importlib
     import sys
 
     import numpy as np
@@ -74,49 +75,66 @@ def _sharded_rank(rank, world, port, q):
     sys.path.insert(0, os.path.join(root, "oracle"))
     import bench
     import oracle as O
+    tbg = importlib.import_module("tee-bench_b200")
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         nR, nS = 5000, 40001
-        rng = np.random.default_rng(5)  # every rank draws the same S; each keeps its shard
-        R_rows = np.zeros(nR, dtype=O.ROW)
-        R_rows["key"] = rng.permutation(nR) + 1
+        rng = np.random.default_rng(5)  # every rank draws the same relations; each keeps its rows
+        R_all = np.zeros(nR, dtype=O.ROW)
+        R_all["key"] = rng.permutation(nR) + 1
+        R_all["key"][:40] = 7  # duplicate R keys
+        R_all["payload"] = np.arange(nR)
         S_all = np.zeros(nS, dtype=O.ROW)
-        S_all["key"] = rng.integers(1, 2 * nR, nS)
-        lo, hi = bench.shard_rows(nS, world, rank)
-        R = torch.zeros(nR, dtype=torch.int64)
-        if rank == 0:  # R exists on rank 0 only until the broadcast
-            R.copy_(torch.from_numpy(R_rows.view(np.int64).copy()))
+        S_all["key"] = rng.zipf(1.3, nS) % (2 * nR) + 1  # skew and misses
+        S_all["payload"] = np.arange(nS)
+        rlo, rhi = bench.shard_rows(nR, world, rank)
+        slo, shi = bench.shard_rows(nS, world, rank)
 
-        def join_count(Rt, S):
-            return O.rho(Rt.numpy().view(O.ROW), S)
+        def as_tensor(rows):
+            return torch.from_numpy(np.ascontiguousarray(rows).view(np.int64).copy())
 
-        m = bench.sharded_count(dist, R, S_all[lo:hi], join_count)
-        q.put((rank, lo, hi, m, O.rho(R_rows, S_all)))
+        def split(t, nshards):  # the library's grouping, on the host
+            rows = t.numpy().view(O.ROW)
+            d = tbg.shard_of(rows["key"], nshards)
+            order = np.argsort(d, kind="stable")
+            offs = np.concatenate([[0], np.cumsum(np.bincount(d, minlength=nshards))]).tolist()
+            return as_tensor(rows[order]), offs
+
+        seen = []
+
+        def join(Rt, St):
+            Rr, Sr = Rt.numpy().view(O.ROW), St.numpy().view(O.ROW)
+            seen.append((set(tbg.shard_of(Rr["key"], world).tolist()), set(tbg.shard_of(Sr["key"], world).tolist())))
+            return O.rho(Rr, Sr)
+
+        m = tbg.distributed_join_count(dist, as_tensor(R_all[rlo:rhi]), as_tensor(S_all[slo:shi]), split, join,
+                                       lambda n: torch.empty(n, dtype=torch.int64))
+        q.put((rank, m, O.rho(R_all, S_all), seen))
     finally:
         dist.destroy_process_group()
 
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_sharded_join_matches_single_join(world):
-    """S split over the ranks, R broadcast from rank 0, counts all-reduced:
-    the total equals the oracle's count of the unsharded join."""
+    """R and S spread over the ranks, split by key hash, exchanged with an
+    all-to-all, joined per rank and the counts summed: every rank holds the
+    unsharded join's count (oracle), and each rank joined only its shard."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
     procs = [ctx.Process(target=_sharded_rank, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
-    out = sorted(q.get(timeout=120) for _ in range(world))
+    out = sorted((q.get(timeout=120) for _ in range(world)), key=lambda x: x[0])
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    bounds = [(lo, hi) for _, lo, hi, _, _ in out]
-    assert bounds[0][0] == 0 and bounds[-1][1] == 40001
-    assert all(bounds[i][1] == bounds[i + 1][0] for i in range(world - 1))
-    for _, _, _, m, want in out:
+    for rank, m, want, seen in out:
         assert m == want  # every rank holds the full join's count
+        (r_shards, s_shards), = seen
+        assert r_shards <= {rank} and s_shards <= {rank}  # a rank joins only its own shard's keys
 
 
 def test_shard_rows_cover_evenly():
