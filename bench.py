@@ -6,9 +6,13 @@
 
 One step = one full join (histogram, partitioning passes, build/probe) of a
 device-resident synthetic |R| = 2^27, |S| = 2^30 uniform foreign-key workload,
-count only (the headline configuration).  Prints ONE JSON line on rank 0.
+count only (the headline configuration).  On N > 1 GPUs (torchrun) the same
+join is spread over the ranks: each holds 1/N of R and S, splits its rows by
+key hash, an NCCL all-to-all exchanges the pieces, every rank joins its share
+and the counts are all-reduced (strong scaling).  Prints ONE JSON line on
+rank 0.
 
-* value      whole-job input M tuples/s = N * (|R| + |S|) * K / max-over-ranks
+* value      whole-job input M tuples/s = (|R| + |S|) * K / max-over-ranks
              device time (CUDA events on the join stream);
 * e2e        the same metric through the drop-in RHO(table_t*, table_t*, int)
              with pinned host buffers: H2D of R and S, the join and the result
@@ -16,11 +20,16 @@ count only (the headline configuration).  Prints ONE JSON line on rank 0.
 * roofline   the dominant kernel (the partitioning scatter) against the
              measured HBM copy bandwidth, from per-phase CUDA events recorded
              by the library on the join stream during the timed steps;
+* learned_vs_radix  LRN against RHO with and without its skew split on the
+             skewed configuration (2^26 / 2^29 Zipf z = 1), same process,
+             clocks sampled;
 * cpu_baseline  the reference's own RHO (oracle/_ref, built from the
-             reference sources) on this host, on a bounded sample.
+             reference sources) on this host's cores, on the workload's own
+             rows, at the physical and at the logical core count.
 
---impl reference times that reference RHO on the host cores (all threads) on
-the same workload definition (bounded sample per step); rank 0 only.
+--impl reference times that reference RHO on the host cores (all logical
+CPUs) on the same configuration, inputs from the reference's own generators;
+rank 0 only.
 """
 from __future__ import annotations
 
@@ -53,7 +62,8 @@ WORKLOADS = {
     "plain_c3_z15": ("RHO", 26, 29, "zipf", 1.5, {"skew_split": 0}),
     "lrn_c3_z15": ("LRN", 26, 29, "zipf", 1.5),
     "rho_c1": ("RHO", 21, 21, "fk", 100),
-    # one 2^27 / 2^30 join sharded over the ranks (S split, R broadcast from rank 0)
+    # the headline join spread over the ranks (key-hash split, all-to-all); the
+    # default workload takes this path whenever more than one GPU runs
     "rho_c2_sharded": ("RHO", 27, 30, "fk", 100, {"sharded": 1}),
     # 2^28 / 2^31 Zipf z = 1.0, materialised (2^31 output rows, 25.8 GB)
     "lrn_c5_mat": ("LRN", 28, 31, "zipf", 1.0, {"materialize": 1}),
@@ -123,20 +133,6 @@ def shard_rows(n, world, rank):
     base, rem = divmod(n, world)
     lo = rank * base + min(rank, rem)
     return lo, lo + base + (1 if rank < rem else 0)
-
-
-def sharded_count(dist, R, S_local, join_count, root=0):
-    """One equi-join of R with S split across the ranks: R (a tensor of rows,
-    valid on root) is broadcast from root, the exchange step; every rank joins
-    its shard of S; the counts are summed on every rank."""
-    import torch
-    multi = dist is not None and dist.is_initialized() and dist.get_world_size() > 1
-    if multi:
-        dist.broadcast(R, src=root)
-    t = torch.tensor([int(join_count(R, S_local))], dtype=torch.int64, device=R.device)
-    if multi:
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return int(t.item())
 
 
 def job_mtuples(world, rows_per_rank, steps, seconds):
@@ -449,7 +445,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload in BATCH_WORKLOADS:
         return batch_main(args, rank, world, local)
-    if wl_spec(args.workload)[5].get("sharded"):
+    if wl_spec(args.workload)[5].get("sharded") or (args.workload == "rho_c2" and world > 1):
+        # the headline join on several GPUs: one join spread over the ranks
         return sharded_main(args, rank, world, local)
     algo, lr, ls, kind, param, over = wl_spec(args.workload)
     lr = args.log2_r if args.log2_r is not None else lr
@@ -464,10 +461,13 @@ def main():
               " equi-join, bit-exact")
 
     base_config = {"workload": workload_name, "global_batch": world * (nR + nS), "nR": nR, "nS": nS}
+    # the headline is one join (spread over the ranks when N > 1); the other
+    # workloads run one independent join per rank
+    scaling = "strong" if args.workload == "rho_c2" else "weak"
     if args.impl == "reference":
         if rank != 0:
             return 0
-        return reference_main(args, metric, base_config, world, mat)
+        return reference_main(args, metric, base_config, world, mat, scaling=scaling)
 
     import torch
     import torch.distributed as dist
@@ -652,10 +652,11 @@ def main():
     line = {
         "metric": metric, "value": value, "unit": "Mtuples/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": pipe_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "scaling": scaling, "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": workload_name, "global_batch": world * rows, "nR": nR, "nS": nS,
                    "radix_bits": st.radix_bits, "passes": st.passes,
-                   "parallelism": f"{world} independent joins (R replicated, S per rank)",
+                   "parallelism": ("one join on one GPU (on N > 1 GPUs the same join is spread over the ranks)"
+                                   if scaling == "strong" else f"{world} independent joins (one per rank)"),
                    "l2": f"inputs {rows * 8 / 1e9:.1f} GB per step > 126 MB L2; no flush needed",
                    "generator": "on-GPU pk / fk / zipf (generator.cpp semantics)"},
         "gpu_launches": int(launches),
@@ -706,18 +707,23 @@ def cpu_baseline_line(host_rows, algo, mat):
 
 # ------------------------------------------------------------------ sharded
 def sharded_main(args, rank, world, local):
-    """One |R| = 2^27, |S| = 2^30 join over all ranks (strong scaling): S is
-    split evenly, R lives on rank 0 and is broadcast (NCCL) every step, each
-    rank joins its shard, the counts are all-reduced."""
+    """One |R| = 2^27, |S| = 2^30 uniform FK join spread over the ranks (strong
+    scaling): rank r holds rows shard_rows(n, world, r) of R and of S.  Each
+    step every rank splits its rows by shard (tbg_shard_split), an all-to-all
+    (NCCL over NVLink) moves every piece to its shard's rank, each rank joins
+    what it received (tbg_join_device) and the counts are all-reduced.  Every
+    rank partitions only its share of R and S.  With one rank it is the
+    single-GPU join."""
     algo, lr, ls, kind, param, _ = wl_spec(args.workload)
     lr = args.log2_r if args.log2_r is not None else lr
     ls = args.log2_s if args.log2_s is not None else ls
     nR, nS = 1 << lr, 1 << ls
-    lo, hi = shard_rows(nS, world, rank)
-    nSl = hi - lo
-    workload_name = (f"{algo} |R|=2^{lr} |S|=2^{ls} uniform FK, count only, one join sharded over {world} GPU(s): "
-                     f"S split evenly, R broadcast from rank 0 each step, counts all-reduced")
-    metric = "input Mtuples/s (|R|+|S|)/t of one sharded count-only equi-join, bit-exact"
+    rlo, rhi = shard_rows(nR, world, rank)
+    slo, shi = shard_rows(nS, world, rank)
+    workload_name = (f"{algo} |R|=2^{lr} |S|=2^{ls} uniform FK 100% selectivity, count only, one join spread over "
+                     f"the GPUs: each rank holds 1/N of R and S, splits its rows by key hash, all-to-all exchange, "
+                     f"local joins, counts all-reduced")
+    metric = "input Mtuples/s (|R|+|S|)/t, count-only equi-join, bit-exact"
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -730,21 +736,37 @@ def sharded_main(args, rank, world, local):
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300), device_id=dev)
-    # one stream (the current one) orders the broadcast, the join and the reduction
+    # one stream (the current one) orders the splits, the exchange and the joins
     sh = torch.cuda.current_stream().cuda_stream
-    tR = torch.zeros(nR, dtype=torch.int64, device=dev)
-    tS = torch.empty(max(nSl, 1), dtype=torch.int64, device=dev)
-    if rank == 0:
-        tbg.gen_pk(tR.data_ptr(), nR, 11111, sh)
-    tbg.gen_fk(tS.data_ptr(), nSl, nR, 22222 + rank, sh)
+    full = torch.empty(max(nR, nS), dtype=torch.int64, device=dev)  # every rank draws the same relations
+    tbg.gen_pk(full.data_ptr(), nR, 11111, sh)
+    tR = full[rlo:rhi].clone()
+    tbg.gen_fk(full.data_ptr(), nS, nR, 22222, sh)
+    tS = full[slo:shi].clone()
+    del full
     torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     cfg = tbg.config(algo)
+    moved = {"rows": 0}
 
-    def join_count(R, S):
-        return tbg.join_device(cfg, R.data_ptr(), nR, S.data_ptr(), nSl, stream=sh)[1]
+    def split(t, n):
+        out = torch.empty_like(t)
+        offs = tbg.shard_split(t.data_ptr(), t.numel(), n, out.data_ptr(), sh)
+        moved["rows"] += t.numel() - (offs[rank + 1] - offs[rank])
+        return out, offs
+
+    def join(Rt, St):
+        moved["joined"] = Rt.numel() + St.numel()
+        return tbg.join_device(cfg, Rt.data_ptr(), Rt.numel(), St.data_ptr(), St.numel(), stream=sh)[1]
+
+    def new_rows(n):
+        return torch.empty(max(n, 1), dtype=torch.int64, device=dev)[:n]
+
+    def step():
+        return tbg.distributed_join_count(dist, tR, tS, split, join, new_rows)
 
     for _ in range(args.warmup):
-        m = sharded_count(dist, tR, tS, join_count)
+        m = step()
     if m != nS:
         raise SystemExit(f"wrong match count {m} != {nS}")
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -753,23 +775,24 @@ def sharded_main(args, rank, world, local):
         dist.barrier()
     torch.cuda.synchronize()
     l0 = tbg.kernel_launches()
+    moved["rows"] = 0
     with ClockSampler(local) as clocks:
         ev0.record()
         for _ in range(args.steps):
-            m = sharded_count(dist, tR, tS, join_count)
+            m = step()
         ev1.record()
         torch.cuda.synchronize()
     launches = tbg.kernel_launches() - l0
-    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     K = args.steps
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     value = (nR + nS) * K / (ms / 1e3) / 1e6
+    sent_rows = moved["rows"] / K
     e2e = None
-    if args.e2e_steps > 0:  # every step: the shard (and R on rank 0) copied from pinned host memory
-        hS = torch.empty_like(tS, device="cpu", pin_memory=True)
+    if args.e2e_steps > 0:  # every step: this rank's rows copied from pinned host memory, the count read back
+        hR = torch.empty(tR.numel(), dtype=torch.int64, pin_memory=True)
+        hS = torch.empty(tS.numel(), dtype=torch.int64, pin_memory=True)
+        hR.copy_(tR)
         hS.copy_(tS)
-        hR = torch.empty_like(tR, device="cpu", pin_memory=True) if rank == 0 else None
-        if hR is not None:
-            hR.copy_(tR)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -777,38 +800,45 @@ def sharded_main(args, rank, world, local):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(args.e2e_steps):
+            tR.copy_(hR, non_blocking=True)
             tS.copy_(hS, non_blocking=True)
-            if hR is not None:
-                tR.copy_(hR, non_blocking=True)
-            m = sharded_count(dist, tR, tS, join_count)  # the count is read back to the host
+            m = step()  # the count is read back to the host
         e1.record()
         torch.cuda.synchronize()
         el = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, dev)
         e2e = {"value": (nR + nS) * args.e2e_steps / el / 1e6, "unit": "Mtuples/s",
-               "h2d_bytes_per_step": (nR + nS) * 8, "d2h_bytes_per_step": 8 * world,
-               "api": "tbg_join_device per shard, R broadcast over NCCL, count all-reduced; inputs copied from "
-                      "pinned host memory each step", "count": int(m)}
+               "h2d_bytes_per_step": (tR.numel() + tS.numel()) * 8, "d2h_bytes_per_step": 8,
+               "api": "distributed_join_count: tbg_shard_split + NCCL all-to-all + tbg_join_device per rank; "
+                      "each rank's rows copied from pinned host memory each step", "count": int(m)}
     peak, peak_kind = read_peaks()
-    alg = 48 * (nR + nSl)  # this rank's pipeline: histogram 8 + 2 passes x 16 + build/probe 8 B per row
+    local_rows = tR.numel() + tS.numel()
+    joined = moved.get("joined", local_rows)
+    # this rank's HBM bytes: split 8 (histogram) + 16 (scatter) per own row when
+    # world > 1, the join 48 per received row (histogram 8, 2 passes x 16, build/probe 8)
+    alg = (24 * local_rows if world > 1 else 0) + 48 * joined
     line = {
         "metric": metric, "value": value, "unit": "Mtuples/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": workload_name, "global_batch": nR + nS, "nR": nR, "nS": nS,
-                   "shard_rows_S": nSl, "exchange_bytes_per_step": nR * 8 * (world > 1),
-                   "parallelism": f"S sharded over {world} rank(s), R broadcast (NCCL), count all-reduce",
+                   "rows_per_rank": local_rows, "nvlink_rows_sent_per_rank": sent_rows,
+                   "parallelism": f"one join over {world} rank(s): key-hash split, all-to-all (NCCL), local RHO, "
+                                  f"count all-reduce",
                    "l2": "inputs larger than the 126 MB L2; no flush needed"},
         "gpu_launches": int(launches),
         "e2e": e2e,
-        "roofline": {"bound": "hbm", "kernel": "all kernels of one shard's RHO join (pipeline)",
+        "roofline": {"bound": "hbm", "kernel": "this rank's split and join kernels (pipeline)",
                      "achieved": alg / (ms / K / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (ms / K / 1e3) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_shard": alg},
+                     "algorithmic_bytes_per_rank": alg,
+                     "nvlink_bytes_per_rank": sent_rows * 8,
+                     "bytes_model": "split: histogram 8 + scatter 16 B per own row (world > 1); join: 48 B per "
+                                    "received row"},
         "clocks": clocks.summary(),
         "matches": int(m),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and reference_available():
-        host_rows = (host_copy_rows(tR, nR), host_copy_rows(tS, min(nSl, 1 << args.cpu_sample_log2)), nSl)
+        host_rows = (host_copy_rows(tR, nR), host_copy_rows(tS, min(tS.numel(), 1 << args.cpu_sample_log2)), nS)
         line["cpu_baseline"] = cpu_baseline_line(host_rows, "RHO", False)
     if rank == 0:
         print(json.dumps(line))
