@@ -428,6 +428,8 @@ def main():
     ap.add_argument("--workload", default="rho_c2", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-pageable-e2e", action="store_true",
+                    help="skip the drop-in's end-to-end run on pageable host memory")
     ap.add_argument("--no-learned-block", action="store_true",
                     help="skip the learned-vs-radix comparison the headline line carries")
     ap.add_argument("--cpu-sample-log2", type=int, default=30, help="S rows (log2) of the CPU baseline's sample")
@@ -593,6 +595,28 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "api": f"{algo}(table_t*, table_t*, int) drop-in, pinned host buffers",
                "count": int(cnt)}
+        if not args.no_pageable_e2e:
+            # the same call on ordinary (pageable) host memory, as the
+            # reference's driver allocates its tables (generator.cpp:22)
+            pR = np.empty(nR, dtype=np.int64)
+            pS = np.empty(nS, dtype=np.int64)
+            pR[:] = hR.numpy()
+            pS[:] = hS.numpy()
+            del hR, hS
+            tabR = tbg.Table(C.cast(pR.ctypes.data, C.POINTER(tbg.Row)), nR, 0, 0)
+            tabS = tbg.Table(C.cast(pS.ctypes.data, C.POINTER(tbg.Row)), nS, 0, 0)
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.e2e_steps):
+                res = fn(C.byref(tabR), C.byref(tabS), 1)
+                cntp = res.contents.totalresults
+                tbg.lib().tbg_result_free(res)
+            el = max_over_ranks(time.perf_counter() - t0, dist, dev)
+            e2e["pageable"] = {"value": job_mtuples(world, nR + nS, args.e2e_steps, el), "unit": "Mtuples/s",
+                               "api": f"{algo}(table_t*, table_t*, int) drop-in, pageable (malloc'd) host buffers",
+                               "count": int(cntp)}
+            del pR, pS
 
     peak, peak_kind = read_peaks()
     # algorithmic bytes: histogram reads 8 B/row; each partitioning pass
