@@ -138,6 +138,12 @@ uint32_t Workspace::next_epoch(cudaStream_t st) {
 #define TBG_PASS2_UNIT_ROWS 65536
 #endif
 static constexpr uint64_t PASS2_UNIT_ROWS = TBG_PASS2_UNIT_ROWS;
+// Pass-1 chunks (and histogram rows) per SM: a whole number of waves of the
+// resident partitioning CTAs.
+#ifndef TBG_PASS1_CHUNKS_PER_SM
+#define TBG_PASS1_CHUNKS_PER_SM 4
+#endif
+static constexpr uint64_t PASS1_CHUNKS_PER_SM = TBG_PASS1_CHUNKS_PER_SM;
 
 static int ceil_log2(uint64_t x) {
     int k = 0;
@@ -199,7 +205,7 @@ RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int ca
     g.item_cap = 2 * (nR / capR + (g.capS ? nS / g.capS : 0) + 2 * g.P) + 16;
     // four chunks per SM (two resident partitioning CTAs each), >= 32K rows each
     auto chunks = [&](uint64_t n) {
-        uint64_t c = std::min<uint64_t>((uint64_t)w.nsm * 4, (n + 32767) / 32768);
+        uint64_t c = std::min<uint64_t>((uint64_t)w.nsm * PASS1_CHUNKS_PER_SM, (n + 32767) / 32768);
         return (int)std::max<uint64_t>(c, 1);
     };
     g.G[0] = chunks(nR);

@@ -73,20 +73,20 @@ __device__ __forceinline__ uint32_t rank_warp(uint32_t *cnt, uint32_t d, bool va
 // ---------------------------------------------------------------------------
 // tile scatter shared by both passes
 // ---------------------------------------------------------------------------
-// Tiles in flight per CTA: tile q is loaded and ranked while tile q - 1 is
-// written out and tile q + 1 is being copied in.
+// Tile buffers per CTA (the default): tile q is loaded and ranked while tile
+// q - 1 is written out and tile q + 1 is being copied in.
 constexpr int PART_NBUF = 3;
 
-template <int THREADS>
+template <int THREADS, int NBUF = PART_NBUF>
 struct PartSmem {
     static constexpr int NW = THREADS / 32;
     static constexpr int T = THREADS * PART_ITEMS;
-    Row buf[PART_NBUF][T + 2];                  // input tiles (bulk copies), each then staged digit-sorted in place
+    Row buf[NBUF][T + 2];                       // input tiles (bulk copies), each then staged digit-sorted in place
     uint32_t cnt[2][SCATTER_FMAX];              // per-digit counts, then tile offsets, of the two newest tiles
     uint32_t delta[2][SCATTER_FMAX];            // output row - tile slot per digit, of the two newest tiles
     uint32_t cursor[SCATTER_FMAX];              // next output row of each digit
     uint64_t scan[NW + 1];
-    uint64_t mbar[PART_NBUF];
+    uint64_t mbar[NBUF];
 };
 
 // Digit of a pass: a bit field of the key (pass 1: bits [0, b1); pass 2:
@@ -144,20 +144,20 @@ __device__ __forceinline__ void issue_tile(const Row *in, const TileGeo &g, Row 
 // consecutive rows of each digit's run) during the next tile's prefix.
 //
 // Tile q (the CTA's running tile count, continued across ranges so a
-// persistent CTA never re-initialises its barriers) uses buffer q % 3 with
-// barrier mbar[q % 3] at phase parity (q / 3) & 1, and counters and deltas
+// persistent CTA never re-initialises its barriers) uses buffer q % NB with
+// barrier mbar[q % NB] at phase parity (q / NB) & 1, and counters and deltas
 // q & 1.
 
 // Waits for tile q and ranks its rows on cnt[q & 1].
-template <int THREADS, bool FULL, class Dig>
+template <int THREADS, bool FULL, class Dig, int NB>
 __device__ __forceinline__ void tile_load_rank(const Row *__restrict__ in, const TileGeo &g, uint32_t q, Dig dop,
-                                               PartSmem<THREADS> &sm, uint64_t *mbar, uint2 (&v)[PART_ITEMS],
+                                               PartSmem<THREADS, NB> &sm, uint64_t *mbar, uint2 (&v)[PART_ITEMS],
                                                uint32_t (&rank)[PART_ITEMS], unsigned *err) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
     const uint32_t cnt = g.cnt;
-    const int b = q % PART_NBUF;
-    if (!mbar_wait(&mbar[b], (q / PART_NBUF) & 1, SPIN_LIMIT * 16)) atomicCAS(err, 0u, (unsigned)TBG_ERR_TIMEOUT);
+    const int b = q % NB;
+    if (!mbar_wait(&mbar[b], (q / NB) & 1, SPIN_LIMIT * 16)) atomicCAS(err, 0u, (unsigned)TBG_ERR_TIMEOUT);
 #pragma unroll
     for (int i = 0; i < PART_ITEMS; i++) {
         const uint32_t r = wbase + i * 32 + lane;
@@ -183,8 +183,8 @@ __device__ __forceinline__ void tile_load_rank(const Row *__restrict__ in, const
 // cursors; clears the counters of tile q + 1.  Lane l owns digits l, l + 32,
 // ... and the tile lays digits out in that (lane, i) order: any order works
 // as long as each digit's rows stay contiguous.
-template <int THREADS>
-__device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS> &sm) {
+template <int THREADS, int NB>
+__device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS, NB> &sm) {
     const int lane = threadIdx.x & 31;
     constexpr int PER = SCATTER_FMAX / 32;
     uint32_t *c = sm.cnt[q & 1];
@@ -218,13 +218,13 @@ __device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS> &
 }
 
 // Stages tile q's rows digit-sorted into its own buffer.
-template <int THREADS, bool FULL, class Dig>
-__device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, Dig dop, PartSmem<THREADS> &sm,
+template <int THREADS, bool FULL, class Dig, int NB>
+__device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, Dig dop, PartSmem<THREADS, NB> &sm,
                                            const uint2 (&v)[PART_ITEMS], const uint32_t (&rank)[PART_ITEMS]) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t wbase = (uint32_t)w * 32 * PART_ITEMS;
     const uint32_t *c = sm.cnt[q & 1];
-    Row *buf = sm.buf[q % PART_NBUF];
+    Row *buf = sm.buf[q % NB];
 #pragma unroll
     for (int i = 0; i < PART_ITEMS; i++) {
         if (FULL || wbase + i * 32 + lane < g.cnt) {
@@ -235,11 +235,11 @@ __device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, Dig dop
 }
 
 // Writes staged tile q (cnt rows) to out, by threads [t0, THREADS).
-template <int THREADS, class Dig>
+template <int THREADS, class Dig, int NB>
 __device__ __forceinline__ void tile_write(uint32_t q, uint32_t cnt, uint2 *__restrict__ out, uint32_t out_n,
-                                           Dig dop, PartSmem<THREADS> &sm, int t0, unsigned *err) {
+                                           Dig dop, PartSmem<THREADS, NB> &sm, int t0, unsigned *err) {
     if ((int)threadIdx.x < t0) return;
-    const Row *buf = sm.buf[q % PART_NBUF];
+    const Row *buf = sm.buf[q % NB];
     const uint32_t *dl = sm.delta[q & 1];
 #pragma unroll 4
     for (uint32_t j = threadIdx.x - t0; j < cnt; j += THREADS - t0) {
@@ -257,11 +257,12 @@ __device__ __forceinline__ TileGeo range_tile(const Row *in, uint64_t lo, uint64
 
 // Scatters rows [lo, hi) of `in`, digit by digit, to out[sm.cursor[d]...];
 // the caller initialises sm.cursor[0..F) and synchronises.  Three barriers
-// per tile; `kseq` is the CTA's running tile count (see above), and the
-// barriers mbar[0..PART_NBUF) are initialised once by the caller.
-template <int THREADS, class Dig>
+// per tile; the bulk copies run NB - 1 tiles ahead.  `kseq` is the CTA's
+// running tile count (see above), and the barriers mbar[0..NB) are
+// initialised once by the caller.
+template <int THREADS, class Dig, int NB>
 __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
-                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS> &sm, uint64_t *mbar,
+                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS, NB> &sm, uint64_t *mbar,
                            uint32_t &kseq, unsigned *err) {
     constexpr uint32_t T = THREADS * PART_ITEMS;
     uint2 *o = reinterpret_cast<uint2 *>(out);
@@ -269,11 +270,9 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
     for (int i = threadIdx.x; i < F; i += THREADS) sm.cnt[kseq & 1][i] = 0;
     __syncthreads();
     if (ntiles == 0) return;
-    if (threadIdx.x == 0) {
-        issue_tile(in, range_tile(in, lo, hi, 0, T), sm.buf[kseq % PART_NBUF], &mbar[kseq % PART_NBUF]);
-        if (ntiles > 1)
-            issue_tile(in, range_tile(in, lo, hi, 1, T), sm.buf[(kseq + 1) % PART_NBUF], &mbar[(kseq + 1) % PART_NBUF]);
-    }
+    if (threadIdx.x == 0)
+        for (int i = 0; i < NB - 1 && i < ntiles; i++)
+            issue_tile(in, range_tile(in, lo, hi, i, T), sm.buf[(kseq + i) % NB], &mbar[(kseq + i) % NB]);
     uint32_t prev_cnt = 0;
     for (int k = 0; k < ntiles; k++) {
         const uint32_t q = kseq + k;
@@ -286,9 +285,10 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
         if (threadIdx.x < 32) tile_scan<THREADS>(q, F, sm);
         else if (k > 0) tile_write<THREADS, Dig>(q - 1, prev_cnt, o, out_n, dop, sm, 32, err);
         __syncthreads();
-        // tile q - 1's buffer is free: copy tile k + 2 into it
-        if (threadIdx.x == 0 && k + 2 < ntiles)
-            issue_tile(in, range_tile(in, lo, hi, k + 2, T), sm.buf[(q + 2) % PART_NBUF], &mbar[(q + 2) % PART_NBUF]);
+        // tile q - 1's buffer is free: copy tile k + NB - 1 into it
+        if (threadIdx.x == 0 && k + NB - 1 < ntiles)
+            issue_tile(in, range_tile(in, lo, hi, k + NB - 1, T), sm.buf[(q + NB - 1) % NB],
+                       &mbar[(q + NB - 1) % NB]);
         if (g.cnt == T) tile_stage<THREADS, true, Dig>(g, q, dop, sm, v, rank);
         else tile_stage<THREADS, false, Dig>(g, q, dop, sm, v, rank);
         __syncthreads();
@@ -300,11 +300,11 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
 }
 
 // One range per CTA: initialises the barriers held in `sm`.
-template <int THREADS, class Dig>
+template <int THREADS, class Dig, int NB>
 __device__ void part_range(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
-                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS> &sm, unsigned *err) {
+                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS, NB> &sm, unsigned *err) {
     if (threadIdx.x == 0) {
-        for (int i = 0; i < PART_NBUF; i++) mbar_init(&sm.mbar[i], 1);
+        for (int i = 0; i < NB; i++) mbar_init(&sm.mbar[i], 1);
         fence_mbar_init();
     }
     uint32_t kseq = 0;

@@ -34,6 +34,13 @@ namespace tbg {
 #endif
 constexpr int PASS1_THREADS = TBG_PASS1_THREADS;
 constexpr int PASS2_THREADS = TBG_PASS2_THREADS;
+// Tile buffers per CTA of the two passes (bulk copies run NBUF - 1 tiles ahead).
+#ifndef TBG_PASS_NBUF
+#define TBG_PASS_NBUF 3
+#endif
+constexpr int PASS_NBUF = TBG_PASS_NBUF;
+template <int THREADS>
+using PassSmem = PartSmem<THREADS, PASS_NBUF>;
 
 // ---------------------------------------------------------------------------
 // K1 per-chunk histogram over the final partition index f
@@ -261,7 +268,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_part_pass1(PartArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto &sm = *reinterpret_cast<PartSmem<THREADS> *>(smem_raw);
+    auto &sm = *reinterpret_cast<PassSmem<THREADS> *>(smem_raw);
     const int c = blockIdx.x, tid = threadIdx.x;
     const int P = 1 << (a.b1 + a.b2);
     const int F = 1 << a.b1;
@@ -321,7 +328,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_part_pass1(PartArgs
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_part_pass2(PartArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto &sm = *reinterpret_cast<PartSmem<THREADS> *>(smem_raw);
+    auto &sm = *reinterpret_cast<PassSmem<THREADS> *>(smem_raw);
     const int F1 = 1 << a.b1, F2 = 1 << a.b2;
     const int P = F1 * F2;
     const int ngroups = (a.G + a.group - 1) / a.group;
@@ -389,7 +396,7 @@ cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st) {
 
 cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st) {
     constexpr int T = PASS1_THREADS;
-    const size_t smem = sizeof(PartSmem<T>);
+    const size_t smem = sizeof(PassSmem<T>);
     cudaError_t e = smem_limit((const void *)k_part_pass1<T>, smem);
     if (e != cudaSuccess) return e;
     k_part_pass1<T><<<a.G, T, smem, st>>>(a);
@@ -399,7 +406,7 @@ cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st) {
 
 cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st) {
     constexpr int T = PASS2_THREADS;
-    const size_t smem = sizeof(PartSmem<T>);
+    const size_t smem = sizeof(PassSmem<T>);
     cudaError_t e = smem_limit((const void *)k_part_pass2<T>, smem);
     if (e != cudaSuccess) return e;
     const uint64_t units = (uint64_t)((a.G + a.group - 1) / a.group) << a.b1;
