@@ -656,8 +656,9 @@ def main():
         # whole join: LRN's learning and bypass run on two streams and PSM's
         # sort passes are not radix passes, so the pipeline is the unit
         if algo == "PSM":
-            alg = 8 * rows + 16 * 4 * rows + 8 * rows  # digit histogram, 4 LSD passes, merge
-            model = "PSM: digit histogram 8 + 4 LSD passes x 16 + merge read 8 B/row"
+            sp = st.passes or 4  # key-range read, per pass histogram read + scatter, merge read
+            alg = (8 + 24 * sp + 8) * rows
+            model = f"PSM: key range 8 + {sp} LSD passes x (histogram 8 + scatter 16) + merge read 8 B/row"
         else:
             heavy = int(st.heavy_rows_S) if algo == "LRN" else 0
             part_rows = rows - heavy

@@ -119,19 +119,6 @@ Workspace *workspace_for(cudaStream_t st) {
     return w;
 }
 
-uint32_t Workspace::next_epoch(cudaStream_t st) {
-    if (status.fresh) {
-        cudaMemsetAsync(status.p, 0, status.cap, st);
-        status.fresh = false;
-        epoch = 0;
-    }
-    if (++epoch > 255) {
-        cudaMemsetAsync(status.p, 0, status.cap, st);
-        epoch = 1;
-    }
-    return epoch;
-}
-
 // Pass 2 processes units of at least this many rows (consecutive chunks of
 // one pass-1 partition).
 #ifndef TBG_PASS2_UNIT_ROWS

@@ -3,8 +3,8 @@
 // RSM (Joins/radix_sortmerge_join.c:102-105) shares RHO's radix partitioning
 // and swaps the build/probe kernel for a per-partition sort + merge-path join.
 // PSM (Joins/psm/parallel_sortmerge_join.h:61-111) sorts both relations by key
-// (LSD radix sort, 8-bit digits, chunked stable passes; a pass whose digit is
-// the same for every row is skipped) and merges them.
+// (LSD radix sort over the bits of key - min that vary, 7- to 9-bit digits,
+// chunked stable passes) and merges them.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -58,17 +58,30 @@ int run_sortmerge_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const 
 }
 
 cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, const uint32_t *pre,
-                             const uint32_t *totals, uint32_t shift, int digit_bits, unsigned *err, cudaStream_t st);
+                             const uint32_t *totals, uint32_t shift, uint32_t sub, int digit_bits, unsigned *err,
+                             cudaStream_t st);
+
+// Passes of the LSD sort of keys in [kmin, kmax]: (shift, digit bits) over
+// the bits of key - kmin, the fewest passes of at most 9 bits with the bits
+// spread evenly (at least 7 per pass: at an equal pass count narrower digits
+// are cheaper to rank and give longer runs per digit).  Sorting by key - kmin
+// keeps the key order and needs only the bits of the range: 3 passes for
+// the keys 1..2^27 (27 bits of range), where the raw keys span 28 bits.
+std::vector<std::pair<uint32_t, int>> sort_plan(uint32_t kmin, uint32_t kmax) {
+    std::vector<std::pair<uint32_t, int>> plan;
+    if (kmax <= kmin) return plan;
+    const uint32_t span = kmax - kmin;
+    const int bits = 32 - __builtin_clz(span);
+    const int np = (bits + 8) / 9;
+    const int db = std::max(7, (bits + np - 1) / np);
+    for (int i = 0, lo = 0; i < np; i++, lo += db) plan.push_back({(uint32_t)lo, std::min(db, 32 - lo)});
+    return plan;
+}
 
 // LSD sort of n rows by key with chunked stable passes (per-chunk digit
 // histograms, column prefix, k_sort_pass): 24 B per row per pass and no
-// inter-CTA waits.  hhist holds the four 8-bit digit histograms of the input:
-// 8-bit digits that are the same for every row are skipped, and when the key
-// bits that vary fit fewer 9-bit digits than the remaining 8-bit passes, the
-// sort uses 9-bit digits instead (e.g. 3 passes for 27-bit keys, not 4); at
-// an equal pass count narrower digits win (4 passes of 7 bits for 28-bit
-// keys).
-int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, Workspace &w,
+// inter-CTA waits.  Digits are taken from key - kmin.
+int lsd_sort_chunked(const Row *in, uint64_t n, uint32_t kmin, uint32_t kmax, DevBuf &a, DevBuf &b, Workspace &w,
                      cudaStream_t st, const Row **out, int *passes) {
     const Row *src = in;
     Row *bufs[2] = {a.as<Row>(), b.as<Row>()};
@@ -84,85 +97,17 @@ int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint
         *out = src;
         return TBG_OK;
     }
-    // the passes: (shift, digit bits)
-    std::vector<std::pair<uint32_t, int>> plan;
-    int lo_bit = -1, hi_bit = -1;
-    for (int p = 0; p < 4; p++) {
-        bool trivial = false;
-        int top = 0;
-        for (int d = 0; d < 256; d++) {
-            if (hhist[p * 256 + d] == n) trivial = true;
-            if (hhist[p * 256 + d]) top = d;
-        }
-        if (trivial) continue;
-        plan.push_back({8u * p, 8});
-        if (lo_bit < 0) lo_bit = 8 * p;
-        hi_bit = 8 * p + (top ? 31 - __builtin_clz((unsigned)top) : 0);
-    }
-    if (lo_bit >= 0) {
-        // the fewest passes of at most 9 bits over the varying span, with the
-        // bits spread evenly (at least 7 per pass); taken when it saves a
-        // pass, or at equal passes when its digits are narrower (cheaper
-        // ranking, longer runs per digit)
-        const int bits = hi_bit - lo_bit + 1;
-        const int np = (bits + 8) / 9;
-        const int db = std::max(7, (bits + np - 1) / np);
-        if (np < (int)plan.size() || (np == (int)plan.size() && db < 8)) {
-            plan.clear();
-            for (int i = 0; i < np; i++) plan.push_back({(uint32_t)(lo_bit + db * i), db});
-        }
-    }
-    for (const auto &pp : plan) {
+    for (const auto &pp : sort_plan(kmin, kmax)) {
         const uint32_t shift = pp.first;
         const int db = pp.second;
         const uint32_t m2 = (1u << db) - 1;
-        if ((e = launch_hist_chunks(src, n, chunk, G, hist, db, RadixF{0u, shift, m2, 0u}, st)) != cudaSuccess ||
+        RadixF rf{0u, shift, m2, 0u};
+        rf.sub = kmin;
+        if ((e = launch_hist_chunks(src, n, chunk, G, hist, db, rf, st)) != cudaSuccess ||
             (e = launch_colscan(hist, G, 1 << db, totals, st)) != cudaSuccess ||
-            (e = launch_sort_pass(src, bufs[which], n, chunk, G, hist, totals, shift, db, err, st)) != cudaSuccess)
+            (e = launch_sort_pass(src, bufs[which], n, chunk, G, hist, totals, shift, kmin, db, err, st)) !=
+                cudaSuccess)
             return cuda_error(e, "sort pass");
-        src = bufs[which];
-        which ^= 1;
-        (*passes)++;
-    }
-    *out = src;
-    return TBG_OK;
-}
-
-// LSD sort of n rows by key with the one-sweep scatter (one launch per pass,
-// decoupled look-back): used for small inputs (LRN's sample), where launch
-// count matters more than bandwidth.  Returns the buffer holding the sorted
-// rows.
-int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist,
-                    const uint64_t *dbases, int slot0, Workspace &w, cudaStream_t st, const Row **out,
-                    int *passes) {
-    const Row *src = in;
-    Row *bufs[2] = {a.as<Row>(), b.as<Row>()};
-    int which = 0;
-    *passes = 0;
-    for (int p = 0; p < 4; p++) {
-        bool trivial = false;
-        for (int d = 0; d < 256; d++)
-            if (hhist[p * 256 + d] == n) trivial = true;
-        if (trivial || n <= 1) continue;
-        ScatterArgs s;
-        memset(&s, 0, sizeof s);
-        s.in = src;
-        s.out = bufs[which];
-        s.out_n = n;
-        s.seg_start = nullptr;
-        s.seg_tile = nullptr;
-        s.nseg = 0;
-        s.flat_n = n;
-        s.bases = dbases + p * 256;
-        s.status = w.status.as<uint64_t>();
-        s.tile_ctr = &w.ctrl.as<Ctrl>()->tiles[slot0 + p];
-        s.err = &w.ctrl.as<Ctrl>()->error;
-        s.epoch = w.next_epoch(st);
-        s.dshift = 8 * p;
-        s.dbits = 8;
-        s.rf = RadixF{0xFFFFFFFFu, 0, 0, 0};
-        cudaError_t e = launch_scatter(s, (n + SCATTER_TILE - 1) / SCATTER_TILE, st);
-        if (e != cudaSuccess) return cuda_error(e, "sort pass");
         src = bufs[which];
         which ^= 1;
         (*passes)++;
@@ -175,7 +120,6 @@ int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *d
                  tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run) {
     const bool timing = cfg.timing != 0;
     cudaError_t e;
-    const uint64_t tiles = (std::max(nR, nS) + SCATTER_TILE - 1) / SCATTER_TILE + 1;
 #define ENSURE(buf, bytes)                                        \
     do {                                                          \
         e = (buf).ensure(bytes);                                  \
@@ -186,31 +130,29 @@ int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *d
     ENSURE(w.aux[1], nR * 8);
     ENSURE(w.aux[2], nS * 8);
     ENSURE(w.aux[3], nS * 8);
-    ENSURE(w.aux[4], 2 * 4 * 256 * 4);
-    ENSURE(w.aux[5], 2 * 4 * 256 * 8);
+    ENSURE(w.aux[4], 64);
     ENSURE(w.aux[6], (merge_ctas(nR, nS) + 2) * 8);
-    ENSURE(w.status, tiles * SCATTER_FMAX * 8);
 #undef ENSURE
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
-    uint32_t *hist = w.aux[4].as<uint32_t>();
-    uint64_t *bases = w.aux[5].as<uint64_t>();
+    uint32_t *mm = w.aux[4].as<uint32_t>();  // min, max of R's keys, then of S's
     mark_ev(w, timing, 0, st);
     if ((e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st)) != cudaSuccess) return cuda_error(e, "memset");
-    if ((e = launch_digit_hist(dR, nR, hist, bases, w.nsm, st)) != cudaSuccess) return cuda_error(e, "digits R");
-    if ((e = launch_digit_hist(dS, nS, hist + 1024, bases + 1024, w.nsm, st)) != cudaSuccess)
-        return cuda_error(e, "digits S");
-    // which digit passes are needed decides the buffer chain: read the counts back
-    uint32_t hh[2048];
-    if ((e = cudaMemcpyAsync(hh, hist, sizeof hh, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-        return cuda_error(e, "digits");
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "digits");
+    if ((e = launch_key_range(dR, nR, mm, w.nsm, st)) != cudaSuccess ||
+        (e = launch_key_range(dS, nS, mm + 2, w.nsm, st)) != cudaSuccess)
+        return cuda_error(e, "key range");
+    // the key ranges decide the passes and so the buffer chain: read them back
+    uint32_t *hm = static_cast<uint32_t *>(w.host_small);
+    if ((e = cudaMemcpyAsync(hm, mm, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_error(e, "key range");
+    const uint32_t rmin = hm[0], rmax = hm[1], smin = hm[2], smax = hm[3];
     mark_ev(w, timing, 1, st);
     const Row *sR = nullptr, *sS = nullptr;
     int pr = 0, ps = 0;
-    int rc = lsd_sort_chunked(dR, nR, w.aux[0], w.aux[1], hh, w, st, &sR, &pr);
+    int rc = lsd_sort_chunked(dR, nR, rmin, rmax, w.aux[0], w.aux[1], w, st, &sR, &pr);
     if (rc) return rc;
     mark_ev(w, timing, 2, st);
-    rc = lsd_sort_chunked(dS, nS, w.aux[2], w.aux[3], hh + 1024, w, st, &sS, &ps);
+    rc = lsd_sort_chunked(dS, nS, smin, smax, w.aux[2], w.aux[3], w, st, &sS, &ps);
     if (rc) return rc;
     mark_ev(w, timing, 3, st);
     e = launch_merge_join(sR, nR, sS, nS, w.aux[6].as<uint64_t>(), &ctrl->matches, &ctrl->rows, d_rows,

@@ -593,47 +593,49 @@ cudaError_t launch_join_rsm(const JoinArgs &a, bool materialize, int grid, cudaS
 }
 
 // ---------------------------------------------------------------------------
-// PSM: digit histograms of all LSD passes in one read, then the merge join
-// of the globally sorted relations.
+// PSM: the key range of a relation in one read (the sort's passes cover the
+// bits of key - min that vary), then the merge join of the sorted relations.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_digit_hist(const Row *__restrict__ in, uint64_t n,
-                                                    uint32_t *__restrict__ hist /* [4][256] */) {
-    __shared__ uint32_t h[4][256];
-    for (int i = threadIdx.x; i < 4 * 256; i += 512) (&h[0][0])[i] = 0;
-    __syncthreads();
-    for (uint64_t i = (uint64_t)blockIdx.x * 512 + threadIdx.x; i < n; i += (uint64_t)gridDim.x * 512) {
-        const uint32_t k = in[i].key;
-        atomicAdd(&h[0][k & 255], 1u);
-        atomicAdd(&h[1][(k >> 8) & 255], 1u);
-        atomicAdd(&h[2][(k >> 16) & 255], 1u);
-        atomicAdd(&h[3][k >> 24], 1u);
+__global__ void __launch_bounds__(512) k_key_range(const Row *__restrict__ in, uint64_t n, uint32_t *minmax) {
+    uint32_t lo = 0xFFFFFFFFu, hi = 0;
+    const uint64_t np = n / 2;  // row pairs, read as 16-byte vectors when the start is aligned
+    const bool vec = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+    const uint64_t stride = (uint64_t)gridDim.x * 512;
+    if (vec) {
+        const uint4 *v = reinterpret_cast<const uint4 *>(in);
+        for (uint64_t i = (uint64_t)blockIdx.x * 512 + threadIdx.x; i < np; i += stride) {
+            const uint4 x = ldg_stream(v + i);
+            lo = min(lo, min(x.x, x.z));
+            hi = max(hi, max(x.x, x.z));
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) {
+            lo = min(lo, in[n - 1].key);
+            hi = max(hi, in[n - 1].key);
+        }
+    } else {
+        for (uint64_t i = (uint64_t)blockIdx.x * 512 + threadIdx.x; i < n; i += stride) {
+            const uint32_t k = in[i].key;
+            lo = min(lo, k);
+            hi = max(hi, k);
+        }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < 4 * 256; i += 512)
-        if ((&h[0][0])[i]) atomicAdd(&hist[i], (&h[0][0])[i]);
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&minmax[0], lo);
+        atomicMax(&minmax[1], hi);
+    }
 }
 
-// bases[p][d] = exclusive prefix of hist[p][.] (one block, 4 warps x 256 digits)
-__global__ void k_digit_bases(const uint32_t *__restrict__ hist, uint64_t *__restrict__ bases) {
-    const int p = threadIdx.x;  // 4 threads
-    if (p >= 4) return;
-    uint64_t run = 0;
-    for (int d = 0; d < 256; d++) {
-        bases[p * 256 + d] = run;
-        run += hist[p * 256 + d];
-    }
-}
-
-cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_t *bases, int nsm,
-                              cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(hist, 0, 4 * 256 * 4, st);
-    if (e != cudaSuccess) return e;
-    if (n) {
-        const uint64_t g = umin64((n + 511) / 512, (uint64_t)nsm * 4);
-        k_digit_hist<<<(unsigned)g, 512, 0, st>>>(in, n, hist);
-        count_launch();
-    }
-    k_digit_bases<<<1, 32, 0, st>>>(hist, bases);
+// minmax[0] = smallest key, minmax[1] = largest (0xFFFFFFFF, 0 for no rows).
+cudaError_t launch_key_range(const Row *in, uint64_t n, uint32_t *minmax, int nsm, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(minmax, 0xFF, 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(minmax + 1, 0, 4, st);
+    if (e != cudaSuccess || !n) return e;
+    const uint64_t g = umin64((n / 2 + 511) / 512 + 1, (uint64_t)nsm * 4);
+    k_key_range<<<(unsigned)g, 512, 0, st>>>(in, n, minmax);
     count_launch();
     return cudaGetLastError();
 }

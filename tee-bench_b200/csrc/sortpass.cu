@@ -1,5 +1,5 @@
 // One stable LSD radix-sort pass for the PSM sort (7-, 8- or 9-bit digit at
-// `shift`),
+// `shift` of key - sub, sub being the relation's smallest key),
 // built like the partitioning passes: CTA c owns chunk c of the input; its
 // digit cursors are base[d] + (rows of digit d in chunks before c), from the
 // per-chunk histograms (k_hist_chunks) and their column prefix (k_colscan),
@@ -44,7 +44,7 @@ __device__ __forceinline__ unsigned warp_peers_bits(uint32_t d) {
 template <int NB, int DB, bool FULL>
 __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const TileGeo &g, uint32_t k, bool has_next,
                                           const TileGeo &gnext, uint2 *__restrict__ out, uint32_t out_n,
-                                          uint32_t shift, SortSmem<NB> &sm, unsigned *err) {
+                                          uint32_t shift, uint32_t sub, SortSmem<NB> &sm, unsigned *err) {
     constexpr int NW = SortSmem<NB>::NW, C = NB * NW / SORT_THREADS, TPD = NW / C;  // TPD threads per digit
     static_assert(C >= 1 && NW % C == 0 && (TPD & (TPD - 1)) == 0 && TPD <= 32,
                   "a thread's counters belong to one digit; a digit's threads share a warp");
@@ -69,7 +69,7 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
                 v[i] = reinterpret_cast<const uint2 *>(in)[g.t + r];
             }
         }
-        const uint32_t d = valid ? (v[i].x >> shift) & (NB - 1) : NB;  // NB: the no-row sentinel
+        const uint32_t d = valid ? ((v[i].x - sub) >> shift) & (NB - 1) : NB;  // NB: the no-row sentinel
         // a full tile has no sentinel, so its digits need one ballot less
         const unsigned peers = FULL ? warp_peers_bits<DB>(d) : warp_peers_bits<DB + 1>(d);
         uint32_t base = 0;
@@ -109,7 +109,7 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
 #pragma unroll
     for (int i = 0; i < PART_ITEMS; i++) {
         if (FULL || wbase + i * 32 + lane < cnt) {
-            const uint32_t d = (v[i].x >> shift) & (NB - 1);
+            const uint32_t d = ((v[i].x - sub) >> shift) & (NB - 1);
             sm.buf[b][c[w * NB + d] + rank[i]] = Row{v[i].x, v[i].y};
         }
     }
@@ -119,7 +119,7 @@ __device__ __forceinline__ void sort_tile(const Row *__restrict__ in, const Tile
         const uint32_t j = kk * SORT_THREADS + tid;
         if (FULL || j < cnt) {
             const Row x = sm.buf[b][j];
-            const uint32_t pos = sm.delta[(x.key >> shift) & (NB - 1)] + j;
+            const uint32_t pos = sm.delta[((x.key - sub) >> shift) & (NB - 1)] + j;
             if (pos < out_n) out[pos] = make_uint2(x.key, x.payload);
             else atomicCAS(err, 0u, (unsigned)TBG_ERR_ARG);
         }
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 2) k_sort_pass(const Row *__rest
                                                                uint64_t n, uint64_t chunk,
                                                                const uint32_t *__restrict__ pre,
                                                                const uint32_t *__restrict__ totals, uint32_t shift,
-                                                               unsigned *err) {
+                                                               uint32_t sub, unsigned *err) {
     constexpr int NB = 1 << DB;
     static_assert(NB <= SORT_THREADS, "one digit total per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -162,34 +162,35 @@ __global__ void __launch_bounds__(SORT_THREADS, 2) k_sort_pass(const Row *__rest
         const uint64_t t1 = g.t + T;
         const bool more = k + 1 < ntiles;
         const TileGeo gn = more ? tile_geo(in, t1, (uint32_t)umin64(T, hi - t1)) : g;
-        if (g.cnt == T) sort_tile<NB, DB, true>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sm, err);
-        else sort_tile<NB, DB, false>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sm, err);
+        if (g.cnt == T) sort_tile<NB, DB, true>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sub, sm, err);
+        else sort_tile<NB, DB, false>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sub, sm, err);
         g = gn;
     }
 }
 
 // digit_bits: 7, 8 or 9
 cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk, int G, const uint32_t *pre,
-                             const uint32_t *totals, uint32_t shift, int digit_bits, unsigned *err, cudaStream_t st) {
+                             const uint32_t *totals, uint32_t shift, uint32_t sub, int digit_bits, unsigned *err,
+                             cudaStream_t st) {
     cudaError_t e;
     if (digit_bits == 7) {
         const size_t smem = sizeof(SortSmem<128>);
         if ((e = smem_limit((const void *)k_sort_pass<7>, smem)) !=
             cudaSuccess)
             return e;
-        k_sort_pass<7><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);
+        k_sort_pass<7><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, sub, err);
     } else if (digit_bits == 9) {
         const size_t smem = sizeof(SortSmem<512>);
         if ((e = smem_limit((const void *)k_sort_pass<9>, smem)) !=
             cudaSuccess)
             return e;
-        k_sort_pass<9><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);
+        k_sort_pass<9><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, sub, err);
     } else {
         const size_t smem = sizeof(SortSmem<256>);
         if ((e = smem_limit((const void *)k_sort_pass<8>, smem)) !=
             cudaSuccess)
             return e;
-        k_sort_pass<8><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, err);
+        k_sort_pass<8><<<G, SORT_THREADS, smem, st>>>(in, out, n, chunk, pre, totals, shift, sub, err);
     }
     count_launch();
     return cudaGetLastError();

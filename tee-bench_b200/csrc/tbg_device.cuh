@@ -18,6 +18,7 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 __host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
 __device__ __forceinline__ uint32_t radix_f(const RadixF &rf, uint32_t key) {
+    key -= rf.sub;
     return ((key & rf.m1) << rf.b2) | ((key >> rf.b1) & rf.m2);
 }
 

@@ -42,11 +42,8 @@ struct Ctrl {
     unsigned long long pad[4];
 };
 
-// Tile geometry of the stable partitioning scatter.
-constexpr int SCATTER_THREADS = 256;
-constexpr int SCATTER_ITEMS = 16;
-constexpr int SCATTER_TILE = SCATTER_THREADS * SCATTER_ITEMS;  // rows per tile
-constexpr int SCATTER_FMAX = 256;                              // digits per pass
+// Digits per pass of the tile scatter (part_dev.cuh).
+constexpr int SCATTER_FMAX = 256;
 
 // Rows per thread per tile of the chunked partitioning passes.
 constexpr int PART_THREADS = 512;
@@ -61,9 +58,11 @@ constexpr int JOIN_CAPR_SMALL = 4096;  // count-only tables when every R partiti
 constexpr unsigned int SPIN_LIMIT = 1u << 21;
 
 // Radix digit of the final partition index f for a key, pass-major:
-// f = ((key & m1) << b2) | ((key >> b1) & m2).  With one pass, b2 = m2 = 0.
+// f = ((k & m1) << b2) | ((k >> b1) & m2) with k = key - sub.  With one pass,
+// b2 = m2 = 0.
 struct RadixF {
     uint32_t m1, b1, m2, b2;
+    uint32_t sub = 0;  // digits are taken from key - sub (an order-preserving offset for sorts)
 };
 
 // Per-relation partition plan written by the planner kernel.
@@ -89,23 +88,6 @@ struct PartArgs {
     uint32_t *off1;           // [G][F1] start of unit (c, s) in the pass-1 output
     uint32_t *cnt1;           // [G][F1] rows of unit (c, s)
     unsigned *err;
-};
-
-struct ScatterArgs {
-    const Row *in;
-    Row *out;
-    uint64_t out_n;            // rows in `out` (bounds guard)
-    const uint64_t *seg_start; // null: one flat segment [0, flat_n)
-    const uint32_t *seg_tile;
-    uint32_t nseg;
-    uint64_t flat_n;
-    const uint64_t *bases;     // destination of digit d of segment s: bases[(s << dbits) | d]
-    uint64_t *status;          // decoupled look-back words, tiles x F
-    unsigned int *tile_ctr;
-    unsigned int *err;
-    uint32_t epoch;
-    uint32_t dshift, dbits;    // digit = (f(key) >> dshift) & ((1 << dbits) - 1)
-    RadixF rf;
 };
 
 struct JoinArgs {
@@ -140,7 +122,7 @@ struct PlanArgs {
     Ctrl *ctrl;
 };
 
-// ---- launchers (partition.cu, sweep.cu, join.cu, gen.cu) ----
+// ---- launchers (partition.cu, join.cu, gen.cu) ----
 cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G, uint32_t *hist,
                                int P_log2, RadixF rf, cudaStream_t st);
 cudaError_t launch_colscan(uint32_t *hist, int G, int P, uint32_t *totals, cudaStream_t st);
@@ -149,8 +131,6 @@ cudaError_t launch_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2
                               cudaStream_t st);
 cudaError_t launch_part_pass1(const PartArgs &a, cudaStream_t st);
 cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st);
-cudaError_t launch_scatter(const ScatterArgs &a, uint64_t max_tiles, cudaStream_t st);
-size_t scatter_smem_bytes();
 cudaError_t launch_join(const JoinArgs &a, bool materialize, int grid, cudaStream_t st);
 size_t join_smem_bytes(int capR);
 int join_ctas_per_sm(int capR);

@@ -26,21 +26,19 @@ struct Workspace {
     int device = 0;
     int nsm = 148;
     DevBuf ctrl, histR, histS, totR, totS, baseR, baseS, off1R, off1S, cnt1R, cnt1S;
-    DevBuf status, tmpR, tmpS, partR, partS, items, misc;
+    DevBuf tmpR, tmpS, partR, partS, items, misc;
     DevBuf inR, inS, rows;      // drop-in layer: device copies of host inputs and output rows
     DevBuf sc, kept;            // learned path: compacted S and kept rows per chunk
     DevBuf sorthist;            // PSM sort: per-chunk digit histograms and totals
     DevBuf chain_rows, chain_rel;  // chained join: first join's rows and the relation made of them
     DevBuf aux[8];              // algorithm-specific scratch (sort, learned model)
     DevBuf shard;               // shard split: per-chunk histograms and totals
-    uint32_t epoch = 0;         // last look-back epoch used on `status`
     Ctrl *host_ctrl = nullptr;  // pinned mirror of the control block
     static constexpr size_t HOST_SMALL_BYTES = 4096;
     void *host_small = nullptr;  // pinned HOST_SMALL_BYTES: mid-call read-backs (LRN's decision, shard totals)
     cudaEvent_t ev[8];
     cudaStream_t side = nullptr;       // second stream (learned path), created on first use
     cudaEvent_t fork = nullptr, joined = nullptr;
-    uint32_t next_epoch(cudaStream_t st);
 };
 
 // What one join call did (for stats).
@@ -100,12 +98,9 @@ int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row
                     int capR, Workspace &w, cudaStream_t st, JoinRun *run, int *join_grid_out);
 int radix_join_phase(const tbg_config &cfg, tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
                      JoinRun *run, int capR, int join_grid);
-int lsd_sort_chunked(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, Workspace &w,
+int lsd_sort_chunked(const Row *in, uint64_t n, uint32_t kmin, uint32_t kmax, DevBuf &a, DevBuf &b, Workspace &w,
                      cudaStream_t st, const Row **out, int *passes);
-int lsd_sort(const Row *in, uint64_t n, DevBuf &a, DevBuf &b, const uint32_t *hhist, const uint64_t *dbases,
-             int slot0, Workspace &w, cudaStream_t st, const Row **out, int *passes);
-cudaError_t launch_digit_hist(const Row *in, uint64_t n, uint32_t *hist, uint64_t *bases, int nsm,
-                              cudaStream_t st);
+cudaError_t launch_key_range(const Row *in, uint64_t n, uint32_t *minmax, int nsm, cudaStream_t st);
 int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                    tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run);
 int run_radix_join_sliced(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, const uint64_t *s_lo,

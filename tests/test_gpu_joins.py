@@ -233,25 +233,34 @@ def test_join_table_size_gate(tbg, oracle, cuda, algo, bits):
     assert (st.max_part_R > 4096) == (bits == 3)
 
 
-@pytest.mark.parametrize("span", [12, 20, 21, 27, 28, 32])
-def test_psm_digit_plans(tbg, oracle, cuda, span):
-    """PSM's LSD sort picks its digits from the key bits that vary: 8-bit
-    digits, 9-bit digits when they save a pass (27 bits: 3 passes), 7-bit
-    digits at an equal pass count (20, 21, 28 bits).  Every plan must give the
-    oracle's count and rows."""
+PSM_PLANS = [(12, 0), (20, 0), (21, 0), (27, 0), (28, 0), (32, 0), (27, 1), (20, 3_000_000_000)]
+
+
+@pytest.mark.parametrize("span,low", PSM_PLANS, ids=[f"span{s}-low{lo}" for s, lo in PSM_PLANS])
+def test_psm_digit_plans(tbg, oracle, cuda, span, low):
+    """PSM's LSD sort covers the bits of key - min that vary: 9-bit digits when
+    they save a pass (a 27-bit range: 3 passes), 7-bit digits at an equal pass
+    count (20, 21, 28 bits).  Keys 1..2^27 (low = 1) span 28 bits raw but 27
+    above their minimum, so they take 3 passes; a range high in the key space
+    takes the passes its width needs.  Every plan must give the oracle's count
+    and rows."""
     rng = np.random.default_rng(span)
-    hi = 1 << span
+    width = 1 << span
     R = np.zeros(150001, dtype=oracle.ROW)
     S = np.zeros(400003, dtype=oracle.ROW)
-    R["key"] = rng.integers(0, hi, len(R), dtype=np.uint64).astype(np.uint32)
-    R["key"][0] = hi - 1  # the span's top bit is set
+    R["key"] = (low + rng.integers(0, width, len(R), dtype=np.uint64)).astype(np.uint32)
+    R["key"][0] = low + width - 1  # the range's top key
+    R["key"][1] = low              # and its bottom one
     pick = R["key"][rng.integers(0, len(R), len(S))]
-    S["key"] = np.where(rng.random(len(S)) < 0.7, pick, rng.integers(0, hi, len(S), dtype=np.uint64).astype(np.uint32))
+    other = (low + rng.integers(0, width, len(S), dtype=np.uint64)).astype(np.uint32)
+    S["key"] = np.where(rng.random(len(S)) < 0.7, pick, other)
     oracle.fill_payloads(R, 0)
     oracle.fill_payloads(S, 1)
     ref, ref_rows = oracle.rho(R, S, materialize=True)
-    m, _, _ = run_join(tbg, cuda, "PSM", R, S)
+    m, _, st = run_join(tbg, cuda, "PSM", R, S)
     assert m == ref
+    bits = int(width - 1).bit_length()
+    assert st.passes == (bits + 8) // 9, (bits, st.passes)
     m, rows, _ = run_join(tbg, cuda, "PSM", R, S, materialize=True, cap=ref)
     assert m == ref
     assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
