@@ -631,20 +631,24 @@ def main():
         scat_ms = (phase["ms_pass1"] + phase["ms_pass2"]) / K
         scat_bytes = 16 * rows * passes
         achieved = scat_bytes / (scat_ms / 1e3) / 1e9 if scat_ms > 0 else None
-        traffic = None
+        traffic, traffic_source = None, None
         tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        geom = (f"B{st.radix_bits}_{st.radix_bits // 2}+{st.radix_bits - st.radix_bits // 2}" if passes == 2
+                else f"B{st.radix_bits}")
         if os.path.exists(tp):
             with open(tp) as f:
                 tt = json.load(f)
-            k = tt.get("k_part_pass")
-            if k:  # DRAM bytes per row moved, from one ncu capture; per launch like `achieved`
+            k = tt.get("k_part_pass", {}).get(geom)
+            if k:  # DRAM bytes per row moved at this radix geometry, from one ncu capture
                 traffic = k["dram_bytes_per_row"] * rows * passes
+                traffic_source = f"profiles/ncu_traffic.json [{geom}]: {k['source']}"
         total_bytes = (8 + 16 * passes + 8) * rows
         roofline = {"bound": "hbm",
                     "kernel": f"k_part_pass1 + k_part_pass2 ({passes} partitioning passes over R and S, "
                               f"{2 * passes} launches per join)",
                     "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None, "traffic": traffic,
+                    "traffic_source": traffic_source or f"no ncu capture at radix geometry {geom}",
                     "peak_source": peak_source,
                     "algorithmic_bytes_per_row_per_pass": 16,
                     "timing": "library CUDA events on the join stream around each pass, summed over "
