@@ -236,7 +236,8 @@ TBG_API uint64_t tbg_kernel_launches(void);
  * inspection and tests.  params: W1[32], b1[32], W2[32][32], b2[32], W3[32],
  * b3 (host arrays of tbg_mlp_param_count() floats).  LRN fits the frequency
  * curve of S's keys: x = tbg_mlp_feature(r) for sample rank r (1 = the key
- * the sample saw most often), y = log2(that key's sample count) / 32. */
+ * the sample saw most often), y = log2(that key's sample count), normalised
+ * to zero mean and unit spread over the training points. */
 TBG_API int tbg_mlp_param_count(void);
 TBG_API float tbg_mlp_feature(uint32_t rank);
 /* seeded initialisation, as LRN uses before training */

@@ -4,8 +4,8 @@
 //   1. sample 1% of S's keys (seeded blocks of 64 rows) and count them: a
 //      shared-memory aggregation per CTA, then a global hash table;
 //   2. the sample's frequency curve: count-of-counts bins, one training point
-//      per bin (rank feature -> log2(count) / 32), and the MLP trained on
-//      them on the GPU;
+//      per bin (rank feature -> log2(count), normalised over the points), and
+//      the MLP trained on them on the GPU;
 //   3. the decision kernel predicts the S rows of ranks 1 .. HEAVY_MAX from
 //      the trained curve: the heavy keys are the sampled keys at the ranks
 //      predicted to hold at least tau_min rows, and LRN bypasses when the

@@ -1,8 +1,9 @@
 // LRN: learned skew-aware partitioning for sm_100a.
 //
 // A small FP32 MLP (1 -> 32 -> 32 -> 1, tanh) models the frequency curve of
-// S's keys: log2(sample count) / 32 of the key of sample rank r as a function
-// of log2(r + 1) / 16 - 1 (rank 1 = the most frequent key of a seeded 1%
+// S's keys: log2(sample count) of the key of sample rank r (normalised over
+// the training points) as a function of log2(r + 1) / 16 - 1 (rank 1 = the
+// most frequent key of a seeded 1%
 // sample of S).  It is trained per join on that sample's curve by the
 // kernels in this file (forward, backward, Adam; the trainer is one 8-CTA
 // thread-block cluster that all-reduces gradients through distributed shared
@@ -228,13 +229,13 @@ __global__ void k_mlp_init(float *params, uint64_t seed) {
     for (int q = threadIdx.x; q < MLP_PARAMS; q += blockDim.x) {
         const double u = (double)(mix64(seed ^ mix64(0xC0FFEE + q)) >> 11) * (1.0 / 9007199254740992.0);
         float a;
-        if (q < MLP_H) a = sqrtf(6.f / (1 + MLP_H)) * 4.f;                     // W1: spread over the key range
+        if (q < MLP_H) a = sqrtf(6.f / (1 + MLP_H)) * 4.f;                     // W1: spread over the rank range
         else if (q < 2 * MLP_H) a = 1.f;                                        // b1
         else if (q < 2 * MLP_H + MLP_H * MLP_H) a = sqrtf(6.f / (2 * MLP_H));  // W2
         else if (q < 3 * MLP_H + MLP_H * MLP_H) a = 0.1f;                       // b2
         else if (q < 4 * MLP_H + MLP_H * MLP_H) a = sqrtf(6.f / (MLP_H + 1));  // W3
         else a = 0.f;                                                           // b3
-        params[q] = (q == MLP_PARAMS - 1) ? 0.5f : (float)((2.0 * u - 1.0) * a);
+        params[q] = (float)((2.0 * u - 1.0) * a);
     }
 }
 
@@ -435,15 +436,18 @@ cudaError_t launch_count_stats(const LearnBufs &b, cudaStream_t st) {
 
 // Training points of the frequency model, one per non-empty count bin in
 // decreasing count order: x = rank_feature(mid rank of the bin's keys),
-// y = log2(mean sample count of the bin) / 32.  One block; writes the point
-// count to dec->npoints.
+// y = log2(mean sample count of the bin), normalised to zero mean and unit
+// spread over the points (so the network starts at the curve's mean and
+// learns its shape).  One block; writes the point count and the
+// normalisation to dec.
 __global__ void __launch_bounds__(1024) k_rank_points(const unsigned *__restrict__ bin_keys,
                                                      const unsigned long long *__restrict__ bin_rows, float *xs,
                                                      float *ys, LrnDecision *dec) {
     constexpr int PER = (CC_BINS + 1023) / 1024;
     __shared__ uint64_t scratch[1024 / 32 + 1];
+    __shared__ double red[2][32];
     // thread t owns reversed bins [t * PER, t * PER + PER): descending counts
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     uint64_t keys_here = 0, pts_here = 0;
     for (int j = 0; j < PER; j++) {
         const int r = t * PER + j;
@@ -456,6 +460,8 @@ __global__ void __launch_bounds__(1024) k_rank_points(const unsigned *__restrict
     uint64_t tot_keys, tot_pts;
     uint64_t above = block_excl_scan<1024>(keys_here, &tot_keys, scratch);
     uint64_t pt = block_excl_scan<1024>(pts_here, &tot_pts, scratch);
+    const uint64_t pt0 = pt;
+    double s1 = 0.0, s2 = 0.0;
     for (int j = 0; j < PER; j++) {
         const int r = t * PER + j;
         if (r >= CC_BINS) break;
@@ -463,12 +469,37 @@ __global__ void __launch_bounds__(1024) k_rank_points(const unsigned *__restrict
         const unsigned nk = bin_keys[b];
         if (!nk) continue;
         const double mid = (double)above + 0.5 * (double)(nk + 1);
+        const double y = log2((double)bin_rows[b] / (double)nk);
         xs[pt] = rank_feature(mid);
-        ys[pt] = (float)(log2((double)bin_rows[b] / (double)nk) / 32.0);
+        ys[pt] = (float)y;
+        s1 += y;
+        s2 += y * y;
         pt++;
         above += nk;
     }
-    if (t == 0) dec->npoints = (unsigned)tot_pts;
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+        red[0][w] = s1;
+        red[1][w] = s2;
+    }
+    __syncthreads();
+    double a = 0.0, q = 0.0;
+    for (int i = 0; i < 32; i++) {
+        a += red[0][i];
+        q += red[1][i];
+    }
+    const double n = tot_pts ? (double)tot_pts : 1.0;
+    const double mu = a / n;
+    const double sigma = fmax(sqrt(fmax(q / n - mu * mu, 0.0)), 0.25);  // flat curves keep a scale
+    for (uint64_t i = pt0; i < pt; i++) ys[i] = (float)(((double)ys[i] - mu) / sigma);
+    if (t == 0) {
+        dec->npoints = (unsigned)tot_pts;
+        dec->y_mu = (float)mu;
+        dec->y_sigma = (float)sigma;
+    }
 }
 
 cudaError_t launch_rank_points(const LearnBufs &b, cudaStream_t st) {
@@ -478,7 +509,8 @@ cudaError_t launch_rank_points(const LearnBufs &b, cudaStream_t st) {
 }
 
 // The decision (one block).  pred(r), the predicted S rows of the key of
-// sample rank r, comes from the model (2^(32 M(rank_feature(r))) nS / m) or,
+// sample rank r, comes from the model (2^(mu + sigma M(rank_feature(r))) nS / m,
+// mu and sigma the points' normalisation) or,
 // for the ablation, from the sample's own count at rank r.  k* = the ranks
 // 1 .. HEAVY_MAX whose predicted rows reach tau_min; the heavy keys are the
 // sampled keys whose count is at least that of rank k* (the lowest count bin
@@ -514,8 +546,9 @@ __global__ void __launch_bounds__(DECIDE_THREADS) k_decide(const float *__restri
     }
     __syncthreads();
     const double lscale = log2(nS / m);
+    const double mu = dec->y_mu, sigma = dec->y_sigma;
     for (int r = 1 + t; r <= HEAVY_MAX + 1; r += DECIDE_THREADS)
-        lpred[r] = use_model ? (float)(32.0 * (double)mlp_eval(p, rank_feature((double)r)) + lscale)
+        lpred[r] = use_model ? (float)(mu + sigma * (double)mlp_eval(p, rank_feature((double)r)) + lscale)
                              : (cnt_at[r] ? (float)(log2((double)cnt_at[r]) + lscale) : -INFINITY);
     __syncthreads();
     // k*: the largest rank <= HEAVY_MAX predicted at or above tau_min among the

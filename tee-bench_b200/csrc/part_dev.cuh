@@ -82,9 +82,9 @@ struct PartSmem {
     static constexpr int NW = THREADS / 32;
     static constexpr int T = THREADS * PART_ITEMS;
     Row buf[NBUF][T + 2];                       // input tiles (bulk copies), each then staged digit-sorted in place
-    uint32_t cnt[2][SCATTER_FMAX];              // per-digit counts, then tile offsets, of the two newest tiles
-    uint32_t delta[2][SCATTER_FMAX];            // output row - tile slot per digit, of the two newest tiles
-    uint32_t cursor[SCATTER_FMAX];              // next output row of each digit
+    alignas(16) uint32_t cnt[2][SCATTER_FMAX];  // per-digit counts, then tile offsets, of the two newest tiles
+    alignas(16) uint32_t delta[2][SCATTER_FMAX];  // output row - tile slot per digit, of the two newest tiles
+    alignas(16) uint32_t cursor[SCATTER_FMAX];  // next output row of each digit
     uint64_t scan[NW + 1];
     uint64_t mbar[NBUF];
 };
@@ -180,22 +180,28 @@ __device__ __forceinline__ void tile_load_rank(const Row *__restrict__ in, const
 }
 
 // Warp 0: digit counts of tile q -> tile offsets (in place), deltas and
-// cursors; clears the counters of tile q + 1.  Lane l owns digits l, l + 32,
-// ... and the tile lays digits out in that (lane, i) order: any order works
-// as long as each digit's rows stay contiguous.
+// cursors; clears the counters of tile q + 1.  The tile lays the digits out
+// in natural order, so neighbouring runs belong to neighbouring digits and a
+// warp of the write-out that spans a run boundary reads its deltas from
+// different banks.  Lane l owns the 8 consecutive digits [8l, 8l + 8) and
+// moves them with 16-byte accesses (conflict-free).  Every counter of all
+// SCATTER_FMAX digits is kept at zero outside the F digits in use, so those
+// add nothing.
 template <int THREADS, int NB>
 __device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS, NB> &sm) {
+    (void)F;
     const int lane = threadIdx.x & 31;
     constexpr int PER = SCATTER_FMAX / 32;
-    uint32_t *c = sm.cnt[q & 1];
-    uint32_t *dl = sm.delta[q & 1];
-    uint32_t *cn = sm.cnt[(q + 1) & 1];
+    static_assert(PER == 8, "two 16-byte words of counters per lane");
+    uint4 *c4 = reinterpret_cast<uint4 *>(sm.cnt[q & 1]) + 2 * lane;
+    uint4 *d4 = reinterpret_cast<uint4 *>(sm.delta[q & 1]) + 2 * lane;
+    uint4 *u4 = reinterpret_cast<uint4 *>(sm.cursor) + 2 * lane;
+    uint4 *n4 = reinterpret_cast<uint4 *>(sm.cnt[(q + 1) & 1]) + 2 * lane;
+    const uint4 ca = c4[0], cb = c4[1];
+    const uint32_t x[PER] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
     uint32_t sum = 0;
 #pragma unroll
-    for (int i = 0; i < PER; i++) {
-        const int d = lane + 32 * i;
-        sum += d < F ? c[d] : 0;
-    }
+    for (int i = 0; i < PER; i++) sum += x[i];
     uint32_t inc = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -203,18 +209,24 @@ __device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS, N
         if (lane >= o) inc += y;
     }
     uint32_t run = inc - sum;
+    const uint4 ua = u4[0], ub = u4[1];
+    uint32_t cur[PER] = {ua.x, ua.y, ua.z, ua.w, ub.x, ub.y, ub.z, ub.w};
+    uint32_t off[PER], dl[PER];
 #pragma unroll
     for (int i = 0; i < PER; i++) {
-        const int d = lane + 32 * i;
-        if (d < F) {
-            const uint32_t x = c[d];
-            c[d] = run;
-            dl[d] = sm.cursor[d] - run;
-            sm.cursor[d] += x;
-            cn[d] = 0;
-            run += x;
-        }
+        off[i] = run;
+        dl[i] = cur[i] - run;
+        cur[i] += x[i];
+        run += x[i];
     }
+    c4[0] = make_uint4(off[0], off[1], off[2], off[3]);
+    c4[1] = make_uint4(off[4], off[5], off[6], off[7]);
+    d4[0] = make_uint4(dl[0], dl[1], dl[2], dl[3]);
+    d4[1] = make_uint4(dl[4], dl[5], dl[6], dl[7]);
+    u4[0] = make_uint4(cur[0], cur[1], cur[2], cur[3]);
+    u4[1] = make_uint4(cur[4], cur[5], cur[6], cur[7]);
+    n4[0] = make_uint4(0, 0, 0, 0);
+    n4[1] = make_uint4(0, 0, 0, 0);
 }
 
 // Stages tile q's rows digit-sorted into its own buffer.
@@ -267,7 +279,7 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
     constexpr uint32_t T = THREADS * PART_ITEMS;
     uint2 *o = reinterpret_cast<uint2 *>(out);
     const int ntiles = (int)((hi - lo + T - 1) / T);
-    for (int i = threadIdx.x; i < F; i += THREADS) sm.cnt[kseq & 1][i] = 0;
+    for (int i = threadIdx.x; i < SCATTER_FMAX; i += THREADS) sm.cnt[kseq & 1][i] = 0;
     __syncthreads();
     if (ntiles == 0) return;
     if (threadIdx.x == 0)

@@ -68,7 +68,8 @@ struct LrnDecision {
     double pred_mass;         // predicted S rows of ranks 1 .. k_star
     double sample_mass;       // the sample's estimate of the heavy keys' S rows
     double next_rows;         // predicted S rows of rank k_star + 1 (largest key left)
-    float loss;               // mean squared error of the model on the points
+    float loss;               // mean squared error of the model on the (normalised) points
+    float y_mu, y_sigma;      // the points' targets are (log2(count) - y_mu) / y_sigma
     unsigned pad;
 };
 

@@ -157,12 +157,13 @@ def test_trained_network_against_sample_counts_and_untrained(tbg, cuda, scatter)
     how many keys bypass and whether the bypass runs at all.
 
     * Trained, the network's prediction of the heavy keys' rows is within 25%
-      of the sample's own estimate at z = 1.0 and its decisions equal the
+      of the sample's own estimate at z = 1.0, and its decisions equal the
       raw-count method's: it matches the method without the network, it does
       not beat it (both pick the same keys).
-    * Untrained (its initialisation), the prediction is off by orders of
-      magnitude, and at z = 0.5, where no key is heavy enough to pay, it
-      commits to a bypass that the trained model and the sample both reject.
+    * Untrained (its initialisation), the prediction is at least four times
+      further off than the trained one.
+    * At z = 0.5 no key is heavy enough to pay: the trained network and the
+      raw counts both fall back to plain radix.
     * Counts are identical in every case."""
     nR, nS = 1 << 22, 1 << 25
     o = _ablation(tbg, cuda, nR, nS, 1.0, scatter)
@@ -170,12 +171,13 @@ def test_trained_network_against_sample_counts_and_untrained(tbg, cuda, scatter)
     t, smp, u = o["trained"], o["sample"], o["untrained"]
     assert t["fallback"] == 0 and smp["fallback"] == 0, o
     assert t["share"] > 0.30 and abs(t["share"] - smp["share"]) < 0.02, o
-    assert abs(t["pred"] - t["sampled"]) < 0.25 * t["sampled"], o
-    assert u["pred"] > 4 * nS or u["pred"] < 0.25 * u["sampled"], o
+    err_t = abs(t["pred"] - t["sampled"]) / t["sampled"]
+    assert err_t < 0.25, o
+    err_u = abs(u["pred"] - u["sampled"]) / max(u["sampled"], 1.0) if u["sampled"] else float("inf")
+    assert err_u > 4 * err_t, (err_u, err_t, o)
     o = _ablation(tbg, cuda, nR, nS, 0.5, scatter)
     assert len({v["count"] for v in o.values()}) == 1
     assert o["trained"]["fallback"] == 1 and o["sample"]["fallback"] == 1, o
-    assert o["untrained"]["fallback"] == 0, o
 
 
 def test_full_size_skewed_config(tbg, cuda):
@@ -216,5 +218,7 @@ def test_full_size_c3_configs(tbg, cuda, z, scatter):
     print(f"\n[c3] z={z} scattered={scatter} lrn: fallback={st1.used_fallback} heavy_keys={st1.heavy_keys} "
           f"heavy_share={st1.heavy_rows_S / nS:.3f} loss={st1.train_loss:.3e} max_part_S={st1.max_part_S} "
           f"plain max_part_S={st2.max_part_S} mean={nS / st2.partitions:.0f}")
-    if z == 0.0:
+    if z <= 0.5:  # no key heavy enough to pay for the bypass
         assert st1.used_fallback == 1 and st1.heavy_rows_S == 0
+    else:  # the heavy keys leave partitioning: about half of S at z = 1, nearly all at z = 1.5
+        assert st1.used_fallback == 0 and st1.heavy_rows_S > (0.4 if z == 1.0 else 0.9) * nS
