@@ -265,6 +265,7 @@ int part_histogram(int rel, const RadixGeom &g, const Row *d, const tbg_config &
         ba.filter = bypass->filter;
         ba.hkeys = bypass->keys;
         ba.hcnt = bypass->cnt;
+        ba.scnt = bypass->scnt;
         ba.hstart = bypass->start;
         ba.rpay = bypass->rpay;
         ba.matches = &ctrl->matches;

@@ -50,7 +50,8 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess ||
             (e = cudaStreamCreateWithPriority(&w.side, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&w.joined, cudaEventDisableTiming)) != cudaSuccess)
+            (e = cudaEventCreateWithFlags(&w.joined, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&w.table, cudaEventDisableTiming)) != cudaSuccess)
             return cuda_error(e, "stream");
     }
     cudaStream_t s2 = w.side;
@@ -80,7 +81,8 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     ENSURE(w.aux[2], (size_t)CC_BINS * (4 + 8 + 4 + 4));            // bins, training points
     ENSURE(w.aux[3], (size_t)MLP_PARAMS_PAD * 4 + sizeof(LrnDecision));
     ENSURE(w.aux[6], (size_t)kCandCap * sizeof(HeavyCand));
-    ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 4 + (1 << FILTER_LOG2) / 8 + 16);  // keys, cnt, start, cur, filter
+    // heavy table: keys, R counts, starts, cursors, filter, inserted count, S counts
+    ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 5 + (1 << FILTER_LOG2) / 8 + 16);
 #undef ENSURE
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
     LearnBufs lb;
@@ -101,6 +103,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     unsigned *hcnt = hkeys + HEAVY_CAP, *hstart = hcnt + HEAVY_CAP, *hcur = hstart + HEAVY_CAP;
     uint32_t *hfilter = hcur + HEAVY_CAP;
     unsigned *hinserted = hfilter + (1 << FILTER_LOG2) / 32;
+    unsigned *hscnt = hinserted + 4;  // S rows per heavy slot (counting joins)
 
     // main stream: R's partitioning needs nothing from the model
     if (timing) cudaEventRecord(w.ev[0], st);
@@ -117,7 +120,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         (e = cudaMemsetAsync(lb.bin_rows, 0, (size_t)CC_BINS * 12, s2)) != cudaSuccess ||
         (e = cudaMemsetAsync(lb.dec, 0, sizeof(LrnDecision), s2)) != cudaSuccess ||
         (e = cudaMemsetAsync(hkeys, 0xFF, HEAVY_CAP * 4, s2)) != cudaSuccess ||
-        (e = cudaMemsetAsync(hcnt, 0, HEAVY_CAP * 4 * 3 + (1 << FILTER_LOG2) / 8 + 16, s2)) != cudaSuccess)
+        (e = cudaMemsetAsync(hcnt, 0, HEAVY_CAP * 4 * 4 + (1 << FILTER_LOG2) / 8 + 16, s2)) != cudaSuccess)
         return cuda_error(e, "memset");
     const int steps = cfg.model == TBG_MODEL_MLP ? std::min(std::max(cfg.train_steps, 1), 500) : 0;
     const int use_model = cfg.model == TBG_MODEL_SAMPLE ? 0 : 1;
@@ -154,9 +157,22 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         if ((e = launch_heavy_build(lb, hkeys, hfilter, hinserted, s2)) != cudaSuccess)
             return cuda_error(e, "heavy build");
         uint32_t *rpay = nullptr;
-        if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, s2)) !=
-            cudaSuccess)
-            return cuda_error(e, "heavy R");
+        if (mat) {
+            // the S histogram emits heavy pairs on the spot: R's heavy rows
+            // (counts, then payload lists of at most |R| entries) come first
+            if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, s2)) !=
+                cudaSuccess)
+                return cuda_error(e, "heavy R");
+        } else {
+            // counting: the S histogram counts S rows per heavy key; R's heavy
+            // rows are counted on the main stream meanwhile (after R's passes)
+            if ((e = cudaEventRecord(w.table, s2)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(st, w.table, 0)) != cudaSuccess)
+                return cuda_error(e, "event");
+            if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, st)) !=
+                cudaSuccess)
+                return cuda_error(e, "heavy R");
+        }
         if (mat) {  // heavy R payload lists: at most |R| entries, so no count read-back
             if ((e = w.misc.ensure(std::max<uint64_t>(nR, 1) * 4 + 64)) != cudaSuccess)
                 return cuda_error(e, "cudaMalloc");
@@ -169,6 +185,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         bp.filter = hfilter;
         bp.keys = hkeys;
         bp.cnt = hcnt;
+        bp.scnt = hscnt;
         bp.start = hstart;
         bp.rpay = rpay;
         bp.rows = d_rows;
@@ -191,6 +208,8 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         cudaEventRecord(w.ev[3], st);
     }
     rc = radix_join_phase(cfg, d_rows, cap, w, st, run, capR, g.join_grid);
+    if (!rc && bypass && !mat && (e = launch_heavy_sum(hcnt, hscnt, &ctrl->matches, st)) != cudaSuccess)
+        return cuda_error(e, "heavy matches");
     if (timing) {
         float ms = 0;
         cudaEventSynchronize(w.ev[6]);

@@ -21,7 +21,7 @@
 // whatever the model predicts.
 #include <cooperative_groups.h>
 
-#include "tbg_device.cuh"
+#include "part_dev.cuh"
 #include "tbg_learned.h"
 
 namespace cg = cooperative_groups;
@@ -780,7 +780,7 @@ __device__ __forceinline__ int heavy_slot(const uint32_t *filt, const uint32_t *
 // bytes past a 16-byte boundary, or its last row): thread 0 only.
 template <bool MAT>
 __device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *filt, const uint32_t *hkeys,
-                                const unsigned *hcnt, uint32_t *hist, unsigned *s_keep, uint2 *dst, Row x,
+                                unsigned *hcnt, uint32_t *hist, unsigned *s_keep, uint2 *dst, Row x,
                                 unsigned long long &matches, unsigned long long &heavy_rows) {
     const int s = heavy_slot(filt, hkeys, x.key);
     if (s < 0) {
@@ -788,10 +788,14 @@ __device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *filt, const
         dst[atomicAdd(s_keep, 1u)] = make_uint2(x.key, x.payload);
         return;
     }
+    heavy_rows++;
+    if (!MAT) {  // counting: hcnt is this block's S rows per heavy slot
+        atomicAdd(&hcnt[s], 1u);
+        return;
+    }
     const unsigned c = hcnt[s];
     matches += c;
-    heavy_rows++;
-    if (MAT && c) {
+    if (c) {
         uint64_t op = atomicAdd(a.rows_ctr, (unsigned long long)c);
         const unsigned st0 = a.hstart[s];
         for (unsigned q = 0; q < c; q++, op++)
@@ -799,6 +803,11 @@ __device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *filt, const
     }
 }
 
+// Materialising, hcnt holds R's rows per heavy slot and every heavy S row
+// emits its pairs on the spot.  Counting, it counts this block's S rows per
+// heavy slot instead (added to a.scnt at the end): the join's heavy matches
+// are sum_slot S rows x R rows, formed after R's heavy rows are counted on
+// the other stream (k_heavy_sum), so that count is off this kernel's path.
 template <bool MAT>
 __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -813,7 +822,7 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     for (int i = tid; i < (1 << FILTER_LOG2) / 32; i += 1024) filt[i] = a.filter[i];
     for (int i = tid; i < HEAVY_CAP; i += 1024) {
         hkeys[i] = a.hkeys[i];
-        hcnt[i] = a.hcnt[i];
+        hcnt[i] = MAT ? a.hcnt[i] : 0u;
     }
     if (tid == 0) s_keep = 0;
     __syncthreads();
@@ -852,11 +861,16 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             if (slot[j] >= 0) {
-                matches += hcnt[slot[j]];
+                if (MAT) matches += hcnt[slot[j]];
                 heavy_rows++;
             } else if (valid >> j & 1) {
                 keep |= 1u << j;
             }
+        }
+        if (!MAT) {  // S rows per heavy slot; a warp's rows of one hot key add once
+            const bool dup = warp_has_dups((uint32_t)slot[0], slot[0] >= 0);
+#pragma unroll
+            for (int j = 0; j < 8; j++) hist_add_warp(hcnt, slot[j] >= 0 ? (uint32_t)slot[j] : 0u, slot[j] >= 0, dup);
         }
         // coalesced compaction: one ballot per row slot, one shared atomic per warp
         unsigned m[8], wtot = 0;
@@ -904,12 +918,31 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     __syncthreads();
     uint32_t *hdst = a.hist + (uint64_t)blockIdx.x * a.nbins;
     for (int i = tid; i < a.nbins; i += 1024) hdst[i] = hist[i];
+    if (!MAT)
+        for (int i = tid; i < HEAVY_CAP; i += 1024)
+            if (hcnt[i]) atomicAdd(&a.scnt[i], hcnt[i]);
     if (tid == 0) a.kept[blockIdx.x] = s_keep;
     const unsigned long long wm = warp_sum_u64(matches), wh = warp_sum_u64(heavy_rows);
     if (lane == 0) {
         if (wm) atomicAdd(a.matches, wm);
         if (wh) atomicAdd(a.heavy_rows, wh);
     }
+}
+
+// Heavy matches of a counting join: sum over slots of R rows x S rows.
+__global__ void __launch_bounds__(1024) k_heavy_sum(const unsigned *__restrict__ rcnt,
+                                                   const unsigned *__restrict__ scnt, unsigned long long *matches) {
+    unsigned long long m = 0;
+    for (int i = threadIdx.x; i < HEAVY_CAP; i += 1024) m += (unsigned long long)rcnt[i] * scnt[i];
+    m = warp_sum_u64(m);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(matches, m);
+}
+
+cudaError_t launch_heavy_sum(const unsigned *rcnt, const unsigned *scnt, unsigned long long *matches,
+                             cudaStream_t st) {
+    k_heavy_sum<<<1, 1024, 0, st>>>(rcnt, scnt, matches);
+    count_launch();
+    return cudaGetLastError();
 }
 
 size_t bypass_smem(int nbins, bool mat) {

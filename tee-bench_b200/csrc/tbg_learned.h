@@ -85,7 +85,8 @@ struct BypassArgs {
     uint32_t *kept;       // [G]
     const uint32_t *filter;
     const uint32_t *hkeys;
-    const unsigned *hcnt;
+    const unsigned *hcnt;       // materialising: R rows per heavy slot
+    unsigned *scnt;             // counting: S rows per heavy slot (added to)
     const unsigned *hstart;
     const uint32_t *rpay;
     unsigned long long *matches;
@@ -126,6 +127,7 @@ cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, uint32_t *fil
 cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const uint32_t *filter, unsigned *cnt,
                            unsigned *start, unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st);
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st);
+cudaError_t launch_heavy_sum(const unsigned *rcnt, const unsigned *scnt, unsigned long long *matches, cudaStream_t st);
 size_t bypass_smem(int nbins, bool mat);
 
 }  // namespace tbg

@@ -38,7 +38,7 @@ struct Workspace {
     void *host_small = nullptr;  // pinned HOST_SMALL_BYTES: mid-call read-backs (LRN's decision, shard totals)
     cudaEvent_t ev[8];
     cudaStream_t side = nullptr;       // second stream (learned path), created on first use
-    cudaEvent_t fork = nullptr, joined = nullptr;
+    cudaEvent_t fork = nullptr, joined = nullptr, table = nullptr;
 };
 
 // What one join call did (for stats).
@@ -72,6 +72,7 @@ struct SBypass {
     const uint32_t *filter;
     const uint32_t *keys;
     const unsigned *cnt;
+    unsigned *scnt;
     const unsigned *start;
     const uint32_t *rpay;
     tbg_row_out *rows;
