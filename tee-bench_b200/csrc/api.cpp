@@ -190,9 +190,13 @@ RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int ca
     // room for every R chunk of a partition to split its S side (k_plan
     // keeps oversized S sides whole if a skewed input still overflows this)
     g.item_cap = 2 * (nR / capR + (g.capS ? nS / g.capS : 0) + 2 * g.P) + 16;
-    // four chunks per SM (two resident partitioning CTAs each), >= 32K rows each
+    // four chunks per SM (two resident partitioning CTAs each).  A chunk's
+    // CTA reads its row of the per-chunk prefix (2^B counters) to set up its
+    // cursors, so a chunk holds at least max(4096, 2^B) rows: at 15 bits 32K
+    // rows, while small joins still get enough chunks to fill the GPU.
+    const uint64_t min_chunk = std::max<uint64_t>(4096, g.P);
     auto chunks = [&](uint64_t n) {
-        uint64_t c = std::min<uint64_t>((uint64_t)w.nsm * PASS1_CHUNKS_PER_SM, (n + 32767) / 32768);
+        uint64_t c = std::min<uint64_t>((uint64_t)w.nsm * PASS1_CHUNKS_PER_SM, (n + min_chunk - 1) / min_chunk);
         return (int)std::max<uint64_t>(c, 1);
     };
     g.G[0] = chunks(nR);
@@ -295,7 +299,11 @@ int part_pass(int rel, int which, const RadixGeom &g, const Row *d, Workspace &w
     a.chunk_len = nullptr;
     a.G = g.G[rel];
     const uint64_t per_unit = std::max<uint64_t>(n / ((uint64_t)a.G * g.F1), 1);
-    a.group = (int)std::min<uint64_t>((uint64_t)a.G, std::max<uint64_t>(1, PASS2_UNIT_ROWS / per_unit));
+    // pass-2 units of PASS2_UNIT_ROWS rows, smaller for small relations so
+    // that there are about two units per SM (at least 4096 rows each)
+    const uint64_t unit_rows =
+        std::min<uint64_t>(PASS2_UNIT_ROWS, std::max<uint64_t>(4096, n / ((uint64_t)w.nsm * 2)));
+    a.group = (int)std::min<uint64_t>((uint64_t)a.G, std::max<uint64_t>(1, unit_rows / per_unit));
     a.b1 = g.b1;
     a.b2 = g.b2;
     a.rf = g.rf;
