@@ -243,7 +243,7 @@ __device__ void scatter_chunk(const BatchArgs &a, uint32_t c, BPart &sm, uint64_
     const uint64_t n = rel ? J.nS : J.nR;
     const uint64_t lo = (uint64_t)idx * J.chunk;
     const uint64_t hi = umin64(n, lo + J.chunk);
-    part_tiles<BATCH_THREADS>(in, lo, hi, rel ? J.Sp : J.Rp, (uint32_t)n, DigitOp{0u, P - 1}, (int)P, sm, mbar,
+    part_tiles<BATCH_THREADS>(in, lo, hi, n, rel ? J.Sp : J.Rp, (uint32_t)n, DigitOp{0u, P - 1}, (int)P, sm, mbar,
                               kseq, a.err);
     cta_signal(&a.sync[ch.x].scat_done);
 }

@@ -78,7 +78,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     } while (0)
     ENSURE(w.aux[0], m * 4);                                         // sample keys
     ENSURE(w.aux[1], (size_t)tslots * 8);                            // count table: keys, counts
-    ENSURE(w.aux[2], (size_t)CC_BINS * (4 + 8 + 4 + 4));            // bins, training points
+    ENSURE(w.aux[2], (size_t)CC_BINS * (4 + 8 + 4 + 4 + 4));        // bins, training points, weights
     ENSURE(w.aux[3], (size_t)MLP_PARAMS_PAD * 4 + sizeof(LrnDecision));
     ENSURE(w.aux[6], (size_t)kCandCap * sizeof(HeavyCand));
     // heavy table: keys, R counts, starts, cursors, filter, inserted count, S counts
@@ -94,6 +94,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     lb.bin_keys = reinterpret_cast<unsigned *>(lb.bin_rows + CC_BINS);
     lb.xs = reinterpret_cast<float *>(lb.bin_keys + CC_BINS);
     lb.ys = lb.xs + CC_BINS;
+    lb.cw = lb.ys + CC_BINS;
     lb.params = w.aux[3].as<float>();
     lb.dec = reinterpret_cast<LrnDecision *>(lb.params + MLP_PARAMS_PAD);
     lb.cand = w.aux[6].as<HeavyCand>();
@@ -129,7 +130,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     if ((e = launch_sample_blocks(dS, nS, lb.keys, nb, stride, cfg.seed, s2)) != cudaSuccess ||
         (e = launch_count_keys(lb, m, s2)) != cudaSuccess || (e = launch_count_stats(lb, s2)) != cudaSuccess ||
         (e = launch_rank_points(lb, s2)) != cudaSuccess || (e = launch_mlp_init(lb.params, cfg.seed, s2)) != cudaSuccess ||
-        (steps && (e = launch_mlp_train(lb.xs, lb.ys, &lb.dec->npoints, 0, lb.params, steps, 0.03f, cfg.seed, s2)) !=
+        (steps && (e = launch_mlp_train(lb.xs, lb.ys, lb.cw, &lb.dec->npoints, 0, lb.params, steps, 0.03f, cfg.seed, s2)) !=
                       cudaSuccess) ||
         (e = launch_decide(lb, use_model, (double)nS, (double)m, tau_min, kMinHeavyFraction, s2)) != cudaSuccess)
         return cuda_error(e, "learning stage");
@@ -266,7 +267,7 @@ int tbg_mlp_train(float *params, const float *x, const float *y, uint64_t n, int
     e = cudaMemcpy(dp, params, MLP_PARAMS * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dx, x, n * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dy, y, n * 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = launch_mlp_train(dx, dy, nullptr, (uint32_t)n, dp, steps, lr, seed, 0);
+    if (e == cudaSuccess) e = launch_mlp_train(dx, dy, nullptr, nullptr, (uint32_t)n, dp, steps, lr, seed, 0);
     if (e == cudaSuccess) e = cudaMemcpy(params, dp, MLP_PARAMS * 4, cudaMemcpyDeviceToHost);
     cudaFree(d);
     return e == cudaSuccess ? TBG_OK : cuda_error(e, "mlp train");

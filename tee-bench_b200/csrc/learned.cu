@@ -169,14 +169,16 @@ __global__ void __launch_bounds__(MLP_BATCH_CTA) k_mlp_grad(const float *__restr
 }
 
 // Trainer: one cluster of MLP_CLUSTER CTAs, persistent over all steps.  Each
-// step every CTA draws MLP_BATCH_CTA seeded random training points, computes
-// their forward/backward and its partial parameter gradient; after a cluster
+// step every CTA draws MLP_BATCH_CTA seeded random training points (uniformly,
+// or in proportion to their weights), computes their forward/backward on its
+// first MLP_BATCH_CTA threads and its partial parameter gradient on all
+// MLP_TRAIN_THREADS; after a cluster
 // barrier CTA r sums the partials of its parameter slice from every CTA's
 // shared memory, applies Adam, and writes the new values into every CTA's
 // parameter copy; a second barrier ends the step.
-__global__ void __cluster_dims__(MLP_CLUSTER, 1, 1) __launch_bounds__(MLP_BATCH_CTA)
-    k_mlp_train(const float *__restrict__ xs, const float *__restrict__ ys, const unsigned *n_dev, uint32_t n_host,
-                float *params, int steps, float lr0, uint64_t seed) {
+__global__ void __cluster_dims__(MLP_CLUSTER, 1, 1) __launch_bounds__(MLP_TRAIN_THREADS)
+    k_mlp_train(const float *__restrict__ xs, const float *__restrict__ ys, const float *__restrict__ cw,
+                const unsigned *n_dev, uint32_t n_host, float *params, int steps, float lr0, uint64_t seed) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     // the point count: from device memory when the caller's kernels made the
@@ -190,25 +192,40 @@ __global__ void __cluster_dims__(MLP_CLUSTER, 1, 1) __launch_bounds__(MLP_BATCH_
     float *av = am + MLP_SLICE;
     BatchSmem &b = *reinterpret_cast<BatchSmem *>(av + MLP_SLICE);
     const int tid = threadIdx.x;
-    for (int q = tid; q < MLP_PARAMS; q += MLP_BATCH_CTA) p[q] = params[q];
-    for (int q = tid; q < MLP_SLICE; q += MLP_BATCH_CTA) am[q] = av[q] = 0.f;
+    for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) p[q] = params[q];
+    for (int q = tid; q < MLP_SLICE; q += MLP_TRAIN_THREADS) am[q] = av[q] = 0.f;
     cl.sync();
     const float b1c = 0.9f, b2c = 0.999f, eps = 1e-8f;
     const float scale = 1.f / (float)(MLP_BATCH_CTA * MLP_CLUSTER);
     const int q0 = rank * MLP_SLICE, q1 = min(MLP_PARAMS, q0 + MLP_SLICE);
+    const float wtot = cw ? cw[n - 1] : 0.f;
     float pow1 = 1.f, pow2 = 1.f;
     for (int step = 0; step < steps; step++) {
-        const uint64_t h = mix64(seed ^ mix64(((uint64_t)step << 20) | (uint64_t)(rank * MLP_BATCH_CTA + tid)));
-        const uint32_t i = (uint32_t)(h % n);
-        sample_fwd_bwd(p, xs[i], ys[i], scale, b, tid);
+        if (tid < MLP_BATCH_CTA) {  // one sample per thread of the first warps
+            const uint64_t h = mix64(seed ^ mix64(((uint64_t)step << 20) | (uint64_t)(rank * MLP_BATCH_CTA + tid)));
+            uint32_t i;
+            if (cw) {  // the first point whose cumulative weight exceeds u * total
+                const float u = (float)((h >> 40) * (1.0 / 16777216.0)) * wtot;
+                uint32_t lo = 0, hi = n - 1;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (cw[mid] > u) hi = mid;
+                    else lo = mid + 1;
+                }
+                i = lo;
+            } else {
+                i = (uint32_t)(h % n);
+            }
+            sample_fwd_bwd(p, xs[i], ys[i], scale, b, tid);
+        }
         __syncthreads();
-        for (int q = tid; q < MLP_PARAMS; q += MLP_BATCH_CTA) gpart[q] = param_grad(b, q, MLP_BATCH_CTA);
+        for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) gpart[q] = param_grad(b, q, MLP_BATCH_CTA);
         cl.sync();
         pow1 *= b1c;
         pow2 *= b2c;
         // cosine decay from lr0 to lr0 / 10
         const float lr = lr0 * (0.55f + 0.45f * cospif((float)step / (float)(steps > 1 ? steps - 1 : 1)));
-        for (int q = q0 + tid; q < q1; q += MLP_BATCH_CTA) {
+        for (int q = q0 + tid; q < q1; q += MLP_TRAIN_THREADS) {
             float g = 0.f;
             for (int r = 0; r < MLP_CLUSTER; r++) g += cl.map_shared_rank(gpart, r)[q];
             const int k = q - q0;
@@ -221,7 +238,7 @@ __global__ void __cluster_dims__(MLP_CLUSTER, 1, 1) __launch_bounds__(MLP_BATCH_
         cl.sync();
     }
     if (rank == 0)
-        for (int q = tid; q < MLP_PARAMS; q += MLP_BATCH_CTA) params[q] = p[q];
+        for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) params[q] = p[q];
 }
 
 // Seeded initialisation (uniform Glorot ranges) written to params.
@@ -263,13 +280,13 @@ cudaError_t launch_mlp_grad(const float *params, const float *xs, const float *y
     return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_train(const float *xs, const float *ys, const unsigned *n_dev, uint32_t n, float *params,
-                             int steps, float lr, uint64_t seed, cudaStream_t st) {
+cudaError_t launch_mlp_train(const float *xs, const float *ys, const float *cw, const unsigned *n_dev, uint32_t n,
+                             float *params, int steps, float lr, uint64_t seed, cudaStream_t st) {
     if ((!n_dev && n == 0) || steps <= 0) return cudaSuccess;
     const size_t smem = mlp_train_smem();
     cudaError_t e = smem_limit((const void *)k_mlp_train, smem);
     if (e != cudaSuccess) return e;
-    k_mlp_train<<<MLP_CLUSTER, MLP_BATCH_CTA, smem, st>>>(xs, ys, n_dev, n, params, steps, lr, seed);
+    k_mlp_train<<<MLP_CLUSTER, MLP_TRAIN_THREADS, smem, st>>>(xs, ys, cw, n_dev, n, params, steps, lr, seed);
     count_launch();
     return cudaGetLastError();
 }
@@ -387,21 +404,23 @@ __host__ __device__ __forceinline__ uint32_t cc_bin_min(int b) {
 
 // Count-of-counts over the table (keys per bin, sample rows per bin) and the
 // candidate list: the keys the sample saw at least CAND_MIN_COUNT times.
-__global__ void __launch_bounds__(256) k_count_stats(const uint32_t *__restrict__ tk, const uint32_t *__restrict__ tc,
+constexpr int STATS_THREADS = 1024;
+
+__global__ void __launch_bounds__(STATS_THREADS) k_count_stats(const uint32_t *__restrict__ tk, const uint32_t *__restrict__ tc,
                                                     uint32_t tmask, unsigned *bin_keys,
                                                     unsigned long long *bin_rows, HeavyCand *cand,
                                                     unsigned cand_cap, LrnDecision *dec) {
     __shared__ unsigned sk[CC_BINS];
     __shared__ unsigned long long sr[CC_BINS];
-    for (int i = threadIdx.x; i < CC_BINS; i += 256) {
+    for (int i = threadIdx.x; i < CC_BINS; i += STATS_THREADS) {
         sk[i] = 0;
         sr[i] = 0;
     }
     __syncthreads();
     const uint64_t slots = (uint64_t)tmask + 1;
     const int lane = threadIdx.x & 31;
-    for (uint64_t base = (uint64_t)blockIdx.x * 256; base < slots; base += (uint64_t)gridDim.x * 256) {
-        const uint64_t i = base + threadIdx.x;  // warp-uniform trip count (slots is a multiple of 256)
+    for (uint64_t base = (uint64_t)blockIdx.x * STATS_THREADS; base < slots; base += (uint64_t)gridDim.x * STATS_THREADS) {
+        const uint64_t i = base + threadIdx.x;  // warp-uniform trip count (slots is a multiple of STATS_THREADS)
         const uint32_t k = tk[i], c = tc[i];
         const bool used = k != EMPTY_KEY && c > 0;
         if (used) {
@@ -418,7 +437,7 @@ __global__ void __launch_bounds__(256) k_count_stats(const uint32_t *__restrict_
         if (is_cand && pos < cand_cap) cand[pos] = HeavyCand{k, c};
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < CC_BINS; i += 256) {
+    for (int i = threadIdx.x; i < CC_BINS; i += STATS_THREADS) {
         if (sk[i]) {
             atomicAdd(&bin_keys[i], sk[i]);
             atomicAdd(&bin_rows[i], sr[i]);
@@ -428,8 +447,8 @@ __global__ void __launch_bounds__(256) k_count_stats(const uint32_t *__restrict_
 
 cudaError_t launch_count_stats(const LearnBufs &b, cudaStream_t st) {
     const uint64_t slots = (uint64_t)b.tmask + 1;
-    const unsigned g = (unsigned)umin64(slots / 256, 148 * 4);
-    k_count_stats<<<g, 256, 0, st>>>(b.tkeys, b.tcnt, b.tmask, b.bin_keys, b.bin_rows, b.cand, b.cand_cap, b.dec);
+    const unsigned g = (unsigned)umin64(slots / STATS_THREADS, 148);
+    k_count_stats<<<g, STATS_THREADS, 0, st>>>(b.tkeys, b.tcnt, b.tmask, b.bin_keys, b.bin_rows, b.cand, b.cand_cap, b.dec);
     count_launch();
     return cudaGetLastError();
 }
@@ -442,7 +461,7 @@ cudaError_t launch_count_stats(const LearnBufs &b, cudaStream_t st) {
 // normalisation to dec.
 __global__ void __launch_bounds__(1024) k_rank_points(const unsigned *__restrict__ bin_keys,
                                                      const unsigned long long *__restrict__ bin_rows, float *xs,
-                                                     float *ys, LrnDecision *dec) {
+                                                     float *ys, float *cw, LrnDecision *dec) {
     constexpr int PER = (CC_BINS + 1023) / 1024;
     __shared__ uint64_t scratch[1024 / 32 + 1];
     __shared__ double red[2][32];
@@ -495,6 +514,37 @@ __global__ void __launch_bounds__(1024) k_rank_points(const unsigned *__restrict
     const double mu = a / n;
     const double sigma = fmax(sqrt(fmax(q / n - mu * mu, 0.0)), 0.25);  // flat curves keep a scale
     for (uint64_t i = pt0; i < pt; i++) ys[i] = (float)(((double)ys[i] - mu) / sigma);
+    // sampling weights: half uniform over the points, half in proportion to
+    // the sample rows their bin holds (the top ranks, which carry the heavy
+    // mass the decision predicts, are fitted more closely); cumulative in
+    // point order.  The sample's rows total m (tot_rows below).
+    __syncthreads();  // red is reused
+    double rows_here = 0.0;
+    for (int j = 0; j < PER; j++) {
+        const int r = t * PER + j;
+        if (r < CC_BINS) rows_here += (double)bin_rows[CC_BINS - 1 - r];
+    }
+    double rs = rows_here;
+    for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, o);
+    if (lane == 0) red[0][w] = rs;
+    __syncthreads();
+    double tot_rows = 0.0;
+    for (int i = 0; i < 32; i++) tot_rows += red[0][i];
+    tot_rows = fmax(tot_rows, 1.0);
+    const double wmy = 0.5 * (double)(pt - pt0) / n + 0.5 * rows_here / tot_rows;
+    uint64_t dummy;
+    // fixed point (2^-40) keeps the block scan in integers
+    double run = (double)block_excl_scan<1024>((uint64_t)(wmy * 1099511627776.0), &dummy, scratch) /
+                 1099511627776.0;
+    uint64_t i = pt0;
+    for (int j = 0; j < PER; j++) {
+        const int r = t * PER + j;
+        if (r >= CC_BINS) break;
+        const unsigned nk = bin_keys[CC_BINS - 1 - r];
+        if (!nk) continue;
+        run += 0.5 / n + 0.5 * (double)bin_rows[CC_BINS - 1 - r] / tot_rows;
+        cw[i++] = (float)run;
+    }
     if (t == 0) {
         dec->npoints = (unsigned)tot_pts;
         dec->y_mu = (float)mu;
@@ -503,7 +553,7 @@ __global__ void __launch_bounds__(1024) k_rank_points(const unsigned *__restrict
 }
 
 cudaError_t launch_rank_points(const LearnBufs &b, cudaStream_t st) {
-    k_rank_points<<<1, 1024, 0, st>>>(b.bin_keys, b.bin_rows, b.xs, b.ys, b.dec);
+    k_rank_points<<<1, 1024, 0, st>>>(b.bin_keys, b.bin_rows, b.xs, b.ys, b.cw, b.dec);
     count_launch();
     return cudaGetLastError();
 }
@@ -527,20 +577,28 @@ __global__ void __launch_bounds__(DECIDE_THREADS) k_decide(const float *__restri
     __shared__ float p[MLP_PARAMS];
     __shared__ uint32_t cnt_at[HEAVY_MAX + 2];  // sample count of rank r (r = 1 .. HEAVY_MAX + 1)
     __shared__ float lpred[HEAVY_MAX + 2];      // log2 of the predicted S rows of rank r
+    // the bins, staged (dynamic shared memory) for the single-thread walks below
+    extern __shared__ __align__(16) unsigned char dsm[];
+    unsigned long long *sr = reinterpret_cast<unsigned long long *>(dsm);
+    unsigned *sk = reinterpret_cast<unsigned *>(sr + CC_BINS);
     __shared__ double red[DECIDE_THREADS / 32];
     __shared__ unsigned s_kstar;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     for (int q = t; q < MLP_PARAMS; q += DECIDE_THREADS) p[q] = params[q];
     for (int r = t; r <= HEAVY_MAX + 1; r += DECIDE_THREADS) cnt_at[r] = 0;
+    for (int b = t; b < CC_BINS; b += DECIDE_THREADS) {
+        sk[b] = bin_keys[b];
+        sr[b] = bin_rows[b];
+    }
     if (t == 0) s_kstar = 0;
     __syncthreads();
     // ranks 1 .. HEAVY_MAX + 1 sit in the highest bins: thread 0 walks them
     if (t == 0) {
         unsigned r = 1;
         for (int b = CC_BINS - 1; b >= 1 && r <= (unsigned)HEAVY_MAX + 1; b--) {
-            const unsigned nk = bin_keys[b];
+            const unsigned nk = sk[b];
             if (!nk) continue;
-            const uint32_t c = (uint32_t)(bin_rows[b] / nk);
+            const uint32_t c = (uint32_t)(sr[b] / nk);
             for (unsigned j = 0; j < nk && r <= (unsigned)HEAVY_MAX + 1; j++) cnt_at[r++] = c;
         }
     }
@@ -588,11 +646,11 @@ __global__ void __launch_bounds__(DECIDE_THREADS) k_decide(const float *__restri
         unsigned above = 0, count_min = 0xFFFFFFFFu, heavy = 0;
         unsigned long long rows = 0;
         for (int b = CC_BINS - 1; b >= CAND_MIN_COUNT && kstar; b--) {
-            const unsigned nk = bin_keys[b];
+            const unsigned nk = sk[b];
             if (!nk) continue;
             if (above + nk > kstar) break;
             above += nk;
-            rows += bin_rows[b];
+            rows += sr[b];
             count_min = cc_bin_min(b);
             heavy = above;
         }
@@ -611,7 +669,10 @@ __global__ void __launch_bounds__(DECIDE_THREADS) k_decide(const float *__restri
 
 cudaError_t launch_decide(const LearnBufs &b, int use_model, double nS, double m, double tau_min, double min_frac,
                           cudaStream_t st) {
-    k_decide<<<1, DECIDE_THREADS, 0, st>>>(b.params, use_model, b.bin_keys, b.bin_rows, b.xs, b.ys, nS, m, tau_min, min_frac,
+    const size_t smem = (size_t)CC_BINS * 12;
+    cudaError_t e = smem_limit((const void *)k_decide, smem);
+    if (e != cudaSuccess) return e;
+    k_decide<<<1, DECIDE_THREADS, smem, st>>>(b.params, use_model, b.bin_keys, b.bin_rows, b.xs, b.ys, nS, m, tau_min, min_frac,
                                  b.dec);
     count_launch();
     return cudaGetLastError();

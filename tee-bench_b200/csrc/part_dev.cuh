@@ -108,32 +108,42 @@ struct ShardOp {
     }
 };
 
-// Where tile rows [t, t + cnt) sit in a shared buffer: the bulk copy moves
-// the 16-byte aligned rows [a_lo, a_hi); row r is at buffer index r + off so
-// the copy's destination is 16-byte aligned too; edge rows outside the copy
-// (at most one at each end) are read from global memory.
+// Where tile rows [t, t + cnt) of an n-row array sit in a shared buffer:
+// the bulk copy moves rows [t + c_lo, t + c_hi), a 16-byte aligned span;
+// row r (relative to t) is at buffer index r + off, so the copy's
+// destination is 16-byte aligned too.  When the tile starts or ends 8 bytes
+// past a 16-byte boundary, the copy takes the neighbouring row of the array
+// as well, so the whole tile arrives by the bulk copy; only at the array's
+// own ends, where no neighbour exists, is an edge row left out of the copy
+// (tile rows outside [a_lo, a_hi)) and read from global memory.
 struct TileGeo {
     uint64_t t;
     uint32_t cnt, a_lo, a_hi, off;
+    int32_t c_lo, c_hi;
 };
 
-__device__ __forceinline__ TileGeo tile_geo(const Row *in, uint64_t t, uint32_t cnt) {
+__device__ __forceinline__ TileGeo tile_geo(const Row *in, uint64_t t, uint32_t cnt, uint64_t n) {
     TileGeo g;
     g.t = t;
     g.cnt = cnt;
     const uintptr_t addr = reinterpret_cast<uintptr_t>(in + t);
-    g.a_lo = (addr & 15) ? 1u : 0u;
-    g.a_hi = ((addr + (uintptr_t)cnt * 8) & 15) ? cnt - 1 : cnt;
-    if (g.a_hi < g.a_lo) g.a_hi = g.a_lo;  // a single misaligned row: no copy
-    g.off = g.a_lo;
+    const bool lo_mis = (addr & 15) != 0;
+    const bool hi_mis = ((addr + (uintptr_t)cnt * 8) & 15) != 0;
+    g.c_lo = lo_mis ? (t >= 1 ? -1 : 1) : 0;
+    g.c_hi = hi_mis ? (t + cnt < n ? (int32_t)cnt + 1 : (int32_t)cnt - 1) : (int32_t)cnt;
+    if (g.c_hi < g.c_lo) g.c_hi = g.c_lo;  // a single row at an array end: no copy
+    g.off = lo_mis ? 1u : 0u;
+    g.a_lo = (uint32_t)max(g.c_lo, 0);
+    g.a_hi = (uint32_t)min(g.c_hi, (int32_t)cnt);
+    if (g.a_hi < g.a_lo) g.a_hi = g.a_lo;
     return g;
 }
 
 __device__ __forceinline__ void issue_tile(const Row *in, const TileGeo &g, Row *buf, uint64_t *bar) {
-    const uint32_t bytes = (g.a_hi - g.a_lo) * 8;
+    const uint32_t bytes = (uint32_t)(g.c_hi - g.c_lo) * 8;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
-    if (bytes) bulk_g2s(buf + g.a_lo + g.off, in + g.t + g.a_lo, bytes, bar);
+    if (bytes) bulk_g2s(buf + g.c_lo + (int32_t)g.off, in + (int64_t)g.t + g.c_lo, bytes, bar);
 }
 
 // A tile's rows are read from its landed buffer and ranked on one shared
@@ -262,20 +272,21 @@ __device__ __forceinline__ void tile_write(uint32_t q, uint32_t cnt, uint2 *__re
     }
 }
 
-__device__ __forceinline__ TileGeo range_tile(const Row *in, uint64_t lo, uint64_t hi, int k, uint32_t T) {
+__device__ __forceinline__ TileGeo range_tile(const Row *in, uint64_t lo, uint64_t hi, uint64_t n, int k,
+                                             uint32_t T) {
     const uint64_t t = lo + (uint64_t)k * T;
-    return tile_geo(in, t, (uint32_t)umin64(T, hi - t));
+    return tile_geo(in, t, (uint32_t)umin64(T, hi - t), n);
 }
 
-// Scatters rows [lo, hi) of `in`, digit by digit, to out[sm.cursor[d]...];
+// Scatters rows [lo, hi) of `in` (in_n rows), digit by digit, to out[sm.cursor[d]...];
 // the caller initialises sm.cursor[0..F) and synchronises.  Three barriers
 // per tile; the bulk copies run NB - 1 tiles ahead.  `kseq` is the CTA's
 // running tile count (see above), and the barriers mbar[0..NB) are
 // initialised once by the caller.
 template <int THREADS, class Dig, int NB>
-__device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
-                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS, NB> &sm, uint64_t *mbar,
-                           uint32_t &kseq, unsigned *err) {
+__device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi, uint64_t in_n,
+                           Row *__restrict__ out, uint32_t out_n, Dig dop, int F, PartSmem<THREADS, NB> &sm,
+                           uint64_t *mbar, uint32_t &kseq, unsigned *err) {
     constexpr uint32_t T = THREADS * PART_ITEMS;
     uint2 *o = reinterpret_cast<uint2 *>(out);
     const int ntiles = (int)((hi - lo + T - 1) / T);
@@ -284,11 +295,11 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
     if (ntiles == 0) return;
     if (threadIdx.x == 0)
         for (int i = 0; i < NB - 1 && i < ntiles; i++)
-            issue_tile(in, range_tile(in, lo, hi, i, T), sm.buf[(kseq + i) % NB], &mbar[(kseq + i) % NB]);
+            issue_tile(in, range_tile(in, lo, hi, in_n, i, T), sm.buf[(kseq + i) % NB], &mbar[(kseq + i) % NB]);
     uint32_t prev_cnt = 0;
     for (int k = 0; k < ntiles; k++) {
         const uint32_t q = kseq + k;
-        const TileGeo g = range_tile(in, lo, hi, k, T);
+        const TileGeo g = range_tile(in, lo, hi, in_n, k, T);
         uint2 v[PART_ITEMS];
         uint32_t rank[PART_ITEMS];
         if (g.cnt == T) tile_load_rank<THREADS, true, Dig>(in, g, q, dop, sm, mbar, v, rank, err);
@@ -299,7 +310,7 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
         __syncthreads();
         // tile q - 1's buffer is free: copy tile k + NB - 1 into it
         if (threadIdx.x == 0 && k + NB - 1 < ntiles)
-            issue_tile(in, range_tile(in, lo, hi, k + NB - 1, T), sm.buf[(q + NB - 1) % NB],
+            issue_tile(in, range_tile(in, lo, hi, in_n, k + NB - 1, T), sm.buf[(q + NB - 1) % NB],
                        &mbar[(q + NB - 1) % NB]);
         if (g.cnt == T) tile_stage<THREADS, true, Dig>(g, q, dop, sm, v, rank);
         else tile_stage<THREADS, false, Dig>(g, q, dop, sm, v, rank);
@@ -313,14 +324,15 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
 
 // One range per CTA: initialises the barriers held in `sm`.
 template <int THREADS, class Dig, int NB>
-__device__ void part_range(const Row *__restrict__ in, uint64_t lo, uint64_t hi, Row *__restrict__ out,
-                           uint32_t out_n, Dig dop, int F, PartSmem<THREADS, NB> &sm, unsigned *err) {
+__device__ void part_range(const Row *__restrict__ in, uint64_t lo, uint64_t hi, uint64_t in_n,
+                           Row *__restrict__ out, uint32_t out_n, Dig dop, int F, PartSmem<THREADS, NB> &sm,
+                           unsigned *err) {
     if (threadIdx.x == 0) {
         for (int i = 0; i < NB; i++) mbar_init(&sm.mbar[i], 1);
         fence_mbar_init();
     }
     uint32_t kseq = 0;
-    part_tiles<THREADS, Dig>(in, lo, hi, out, out_n, dop, F, sm, sm.mbar, kseq, err);
+    part_tiles<THREADS, Dig>(in, lo, hi, in_n, out, out_n, dop, F, sm, sm.mbar, kseq, err);
 }
 
 }  // namespace tbg

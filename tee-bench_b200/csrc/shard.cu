@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(SHARD_THREADS, 2) k_shard_scatter(const Row *_
     __syncthreads();
     const uint64_t lo = (uint64_t)c * chunk;
     const uint64_t hi = umin64(n, lo + chunk);
-    part_range<SHARD_THREADS>(in, lo, hi, out, (uint32_t)n, op, (int)op.n, sm, err);
+    part_range<SHARD_THREADS>(in, lo, hi, n, out, (uint32_t)n, op, (int)op.n, sm, err);
 }
 
 int shard_split(const Row *d_in, uint64_t n, int nshards, Row *d_out, uint64_t *offsets, cudaStream_t st) {

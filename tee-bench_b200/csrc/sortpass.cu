@@ -156,12 +156,12 @@ __global__ void __launch_bounds__(SORT_THREADS, 2) k_sort_pass(const Row *__rest
     if (lo >= hi) return;
     const int ntiles = (int)((hi - lo + T - 1) / T);
     uint2 *o = reinterpret_cast<uint2 *>(out);
-    TileGeo g = tile_geo(in, lo, (uint32_t)umin64(T, hi - lo));
+    TileGeo g = tile_geo(in, lo, (uint32_t)umin64(T, hi - lo), n);
     if (tid == 0) issue_tile(in, g, sm.buf[0], &sm.mbar[0]);
     for (int k = 0; k < ntiles; k++) {
         const uint64_t t1 = g.t + T;
         const bool more = k + 1 < ntiles;
-        const TileGeo gn = more ? tile_geo(in, t1, (uint32_t)umin64(T, hi - t1)) : g;
+        const TileGeo gn = more ? tile_geo(in, t1, (uint32_t)umin64(T, hi - t1), n) : g;
         if (g.cnt == T) sort_tile<NB, DB, true>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sub, sm, err);
         else sort_tile<NB, DB, false>(in, g, (uint32_t)k, more, gn, o, (uint32_t)n, shift, sub, sm, err);
         g = gn;

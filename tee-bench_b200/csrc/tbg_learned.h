@@ -16,6 +16,7 @@ constexpr int MLP_PARAMS = 2 * MLP_H + MLP_H * MLP_H + 2 * MLP_H + 1;
 constexpr int MLP_PARAMS_PAD = 1184;  // stride of parameter-sized arrays (>= MLP_PARAMS)
 constexpr int MLP_CLUSTER = 8;        // CTAs of the training cluster
 constexpr int MLP_BATCH_CTA = 128;    // samples per CTA per step
+constexpr int MLP_TRAIN_THREADS = 512;  // trainer threads per CTA (the gradient sums are spread over them)
 constexpr int MLP_SLICE = 152;        // parameters updated by each CTA
 static_assert(MLP_PARAMS <= MLP_PARAMS_PAD, "parameter stride");
 static_assert(MLP_SLICE * MLP_CLUSTER >= MLP_PARAMS, "every parameter belongs to a slice");
@@ -99,8 +100,10 @@ struct BypassArgs {
 cudaError_t launch_mlp_init(float *params, uint64_t seed, cudaStream_t st);
 cudaError_t launch_mlp_grad(const float *params, const float *xs, const float *ys, uint32_t n, float *grad,
                             float *loss_sum, cudaStream_t st);
-cudaError_t launch_mlp_train(const float *xs, const float *ys, const unsigned *n_dev, uint32_t n, float *params,
-                             int steps, float lr, uint64_t seed, cudaStream_t st);
+// cw (may be null): cumulative sampling weights of the points (cw[n - 1] =
+// their total); batches are then drawn in proportion to the weights.
+cudaError_t launch_mlp_train(const float *xs, const float *ys, const float *cw, const unsigned *n_dev, uint32_t n,
+                             float *params, int steps, float lr, uint64_t seed, cudaStream_t st);
 // Learning stage of LRN (all on the device, learned.cu).
 struct LearnBufs {
     uint32_t *keys;             // sample keys [m]
@@ -111,6 +114,7 @@ struct LearnBufs {
     HeavyCand *cand;            // [cand_cap]
     unsigned cand_cap;
     float *xs, *ys;             // training points [CC_BINS]
+    float *cw;                  // their cumulative sampling weights [CC_BINS]
     float *params;              // MLP parameters
     LrnDecision *dec;
     unsigned *err;
