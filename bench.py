@@ -665,11 +665,15 @@ def main():
             model = f"PSM: key range 8 + {sp} LSD passes x (histogram 8 + scatter 16) + merge read 8 B/row"
         else:
             heavy = int(st.heavy_rows_S) if algo == "LRN" else 0
+            bypass = algo == "LRN" and not st.used_fallback
             part_rows = rows - heavy
             alg = 8 * rows + (16 * passes + 8) * part_rows
             model = (f"histogram read 8 B/row of R and S; {passes} passes x 16 + build/probe 8 B/row of the "
                      f"rows that are partitioned ({part_rows}" + (f", {heavy} heavy S rows joined in the "
                                                                    f"histogram read" if heavy else "") + ")")
+            if bypass:  # the kept S rows written compacted, R read once more for its heavy rows
+                alg += 8 * (nS - heavy) + 8 * nR
+                model += "; compacted S 8 B per kept row; heavy R count 8 B per R row"
         if mat:
             alg += 12 * int(m)
             model += "; 12 B per output row"
