@@ -77,14 +77,30 @@ __device__ __forceinline__ uint32_t rank_warp(uint32_t *cnt, uint32_t d, bool va
 // q - 1 is written out and tile q + 1 is being copied in.
 constexpr int PART_NBUF = 3;
 
+// Write-out of a staged tile by bulk stores: every digit run is staged with
+// its shared-memory start in the same 16-byte phase as its global
+// destination (one spare slot per digit), and one thread per digit stores
+// the run's aligned body with one cp.async.bulk store, its edge rows (at most
+// one at each end) with plain stores.  The per-row shared loads and global
+// stores of the write-out leave the SM's load/store pipe.  An output that
+// is not 16-byte aligned takes plain stores for every row.
+#ifndef TBG_BULK_STORE
+#define TBG_BULK_STORE 0
+#endif
+constexpr bool PART_BULK = TBG_BULK_STORE != 0;
+constexpr int PART_PAD = PART_BULK ? SCATTER_FMAX : 0;  // spare slots per staged tile
+
 template <int THREADS, int NBUF = PART_NBUF>
 struct PartSmem {
     static constexpr int NW = THREADS / 32;
     static constexpr int T = THREADS * PART_ITEMS;
-    Row buf[NBUF][T + 2];                       // input tiles (bulk copies), each then staged digit-sorted in place
+    Row buf[NBUF][T + 2 + PART_PAD];            // input tiles (bulk copies), each then staged digit-sorted in place
     alignas(16) uint32_t cnt[2][SCATTER_FMAX];  // per-digit counts, then tile offsets, of the two newest tiles
     alignas(16) uint32_t delta[2][SCATTER_FMAX];  // output row - tile slot per digit, of the two newest tiles
     alignas(16) uint32_t cursor[SCATTER_FMAX];  // next output row of each digit
+    // bulk write-out: each digit's staged start and row count, of the two newest tiles
+    alignas(16) uint32_t rstart[PART_BULK ? 2 : 1][PART_BULK ? SCATTER_FMAX : 4];
+    alignas(16) uint32_t rcount[PART_BULK ? 2 : 1][PART_BULK ? SCATTER_FMAX : 4];
     uint64_t scan[NW + 1];
     uint64_t mbar[NBUF];
 };
@@ -224,10 +240,24 @@ __device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS, N
     uint32_t off[PER], dl[PER];
 #pragma unroll
     for (int i = 0; i < PER; i++) {
-        off[i] = run;
-        dl[i] = cur[i] - run;
+        if (PART_BULK) {
+            // one spare slot per digit: the run starts in its destination's 16-byte phase
+            off[i] = run + ((run ^ cur[i]) & 1u);
+            run += x[i] + 1;
+        } else {
+            off[i] = run;
+            run += x[i];
+        }
+        dl[i] = cur[i] - off[i];
         cur[i] += x[i];
-        run += x[i];
+    }
+    if (PART_BULK) {
+        uint4 *s4 = reinterpret_cast<uint4 *>(sm.rstart[q & 1]) + 2 * lane;
+        uint4 *r4 = reinterpret_cast<uint4 *>(sm.rcount[q & 1]) + 2 * lane;
+        s4[0] = make_uint4(off[0], off[1], off[2], off[3]);
+        s4[1] = make_uint4(off[4], off[5], off[6], off[7]);
+        r4[0] = make_uint4(x[0], x[1], x[2], x[3]);
+        r4[1] = make_uint4(x[4], x[5], x[6], x[7]);
     }
     c4[0] = make_uint4(off[0], off[1], off[2], off[3]);
     c4[1] = make_uint4(off[4], off[5], off[6], off[7]);
@@ -254,6 +284,7 @@ __device__ __forceinline__ void tile_stage(const TileGeo &g, uint32_t q, Dig dop
             buf[j] = Row{v[i].x, v[i].y};
         }
     }
+    if (PART_BULK) fence_proxy_async_smem();  // the staged rows become visible to the bulk stores
 }
 
 // Writes staged tile q (cnt rows) to out, by threads [t0, THREADS).
@@ -261,6 +292,46 @@ template <int THREADS, class Dig, int NB>
 __device__ __forceinline__ void tile_write(uint32_t q, uint32_t cnt, uint2 *__restrict__ out, uint32_t out_n,
                                            Dig dop, PartSmem<THREADS, NB> &sm, int t0, unsigned *err) {
     if ((int)threadIdx.x < t0) return;
+    if (PART_BULK) {
+        (void)cnt;
+        (void)dop;
+        const Row *buf = sm.buf[q % NB];
+        const uint32_t *dl = sm.delta[q & 1];
+        const uint32_t *rs = sm.rstart[q & 1], *rc = sm.rcount[q & 1];
+        const bool aligned = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+        bool issued = false;
+        for (int d = (int)threadIdx.x - t0; d < SCATTER_FMAX; d += THREADS - t0) {
+            uint32_t n = rc[d];
+            if (!n) continue;
+            uint32_t s = rs[d];
+            uint32_t gpos = dl[d] + s;
+            if ((uint64_t)gpos + n > out_n) {
+                atomicCAS(err, 0u, (unsigned)TBG_ERR_ARG);
+                continue;
+            }
+            if (!aligned) {
+                for (uint32_t r = 0; r < n; r++) out[gpos + r] = make_uint2(buf[s + r].key, buf[s + r].payload);
+                continue;
+            }
+            if (gpos & 1) {  // head row up to the 16-byte boundary (the staged start shares the phase)
+                out[gpos] = make_uint2(buf[s].key, buf[s].payload);
+                s++;
+                gpos++;
+                n--;
+            }
+            const uint32_t body = n & ~1u;
+            if (body) {
+                bulk_s2g(out + gpos, buf + s, body * 8);
+                issued = true;
+            }
+            if (n & 1) out[gpos + body] = make_uint2(buf[s + body].key, buf[s + body].payload);
+        }
+        if (issued) {
+            bulk_commit();
+            bulk_wait_read();  // the buffer is reloaded after the next barrier
+        }
+        return;
+    }
     const Row *buf = sm.buf[q % NB];
     const uint32_t *dl = sm.delta[q & 1];
 #pragma unroll 4
@@ -318,6 +389,7 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
         prev_cnt = g.cnt;
     }
     tile_write<THREADS, Dig>(kseq + ntiles - 1, prev_cnt, o, out_n, dop, sm, 0, err);
+    if (PART_BULK) bulk_wait_all();  // this thread's bulk stores have landed
     __syncthreads();  // every buffer is free again
     kseq += ntiles;
 }

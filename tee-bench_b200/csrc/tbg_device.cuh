@@ -185,6 +185,19 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         "l"(src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// this CTA's shared memory to global memory, in this thread's current bulk
+// group (no multicast).
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// This thread's bulk stores have read their shared-memory sources.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// This thread's bulk stores are complete (their global writes done).
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // Bounded wait for phase `parity` of `bar`; false when the limit ran out.
 // Bulk prefetch of [p, p + bytes) into L2 (TMA, no destination); the range
 // is rounded inward to 16-byte bounds, so it never reaches past the rows.
