@@ -78,23 +78,23 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     } while (0)
     ENSURE(w.aux[0], m * 4);                                         // sample keys
     ENSURE(w.aux[1], (size_t)tslots * 8);                            // count table: keys, counts
-    ENSURE(w.aux[2], (size_t)CC_BINS * (4 + 8 + 4 + 4 + 4));        // bins, training points, weights
+    ENSURE(w.aux[2], (size_t)CC_BINS * (4 + 8 + 4 + 4 + 4) + (HEAVY_MAX + 2) * 4);  // bins, points, weights, predictions
     ENSURE(w.aux[3], (size_t)MLP_PARAMS_PAD * 4 + sizeof(LrnDecision));
     ENSURE(w.aux[6], (size_t)kCandCap * sizeof(HeavyCand));
-    // heavy table: keys, R counts, starts, cursors, filter, inserted count, S counts
-    ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 5 + (1 << FILTER_LOG2) / 8 + 16);
+    // heavy table: keys, R counts, starts, cursors, inserted count, S counts
+    ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 5 + 16);
 #undef ENSURE
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
     LearnBufs lb;
     lb.keys = w.aux[0].as<uint32_t>();
-    lb.tkeys = w.aux[1].as<uint32_t>();
-    lb.tcnt = lb.tkeys + tslots;
+    lb.table = w.aux[1].as<unsigned long long>();
     lb.tmask = tslots - 1;
     lb.bin_rows = w.aux[2].as<unsigned long long>();
     lb.bin_keys = reinterpret_cast<unsigned *>(lb.bin_rows + CC_BINS);
     lb.xs = reinterpret_cast<float *>(lb.bin_keys + CC_BINS);
     lb.ys = lb.xs + CC_BINS;
     lb.cw = lb.ys + CC_BINS;
+    lb.lpred = lb.cw + CC_BINS;
     lb.params = w.aux[3].as<float>();
     lb.dec = reinterpret_cast<LrnDecision *>(lb.params + MLP_PARAMS_PAD);
     lb.cand = w.aux[6].as<HeavyCand>();
@@ -102,8 +102,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     lb.err = &ctrl->error;
     uint32_t *hkeys = w.aux[7].as<uint32_t>();
     unsigned *hcnt = hkeys + HEAVY_CAP, *hstart = hcnt + HEAVY_CAP, *hcur = hstart + HEAVY_CAP;
-    uint32_t *hfilter = hcur + HEAVY_CAP;
-    unsigned *hinserted = hfilter + (1 << FILTER_LOG2) / 32;
+    unsigned *hinserted = hcur + HEAVY_CAP;
     unsigned *hscnt = hinserted + 4;  // S rows per heavy slot (counting joins)
 
     // main stream: R's partitioning needs nothing from the model
@@ -116,12 +115,11 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
 
     // side stream: learn the heavy keys meanwhile
     if ((e = cudaStreamWaitEvent(s2, w.fork, 0)) != cudaSuccess) return cuda_error(e, "event");
-    if ((e = cudaMemsetAsync(lb.tkeys, 0xFF, (size_t)tslots * 4, s2)) != cudaSuccess ||
-        (e = cudaMemsetAsync(lb.tcnt, 0, (size_t)tslots * 4, s2)) != cudaSuccess ||
+    if ((e = cudaMemsetAsync(lb.table, 0xFF, (size_t)tslots * 8, s2)) != cudaSuccess ||
         (e = cudaMemsetAsync(lb.bin_rows, 0, (size_t)CC_BINS * 12, s2)) != cudaSuccess ||
         (e = cudaMemsetAsync(lb.dec, 0, sizeof(LrnDecision), s2)) != cudaSuccess ||
         (e = cudaMemsetAsync(hkeys, 0xFF, HEAVY_CAP * 4, s2)) != cudaSuccess ||
-        (e = cudaMemsetAsync(hcnt, 0, HEAVY_CAP * 4 * 4 + (1 << FILTER_LOG2) / 8 + 16, s2)) != cudaSuccess)
+        (e = cudaMemsetAsync(hcnt, 0, HEAVY_CAP * 4 * 4 + 16, s2)) != cudaSuccess)
         return cuda_error(e, "memset");
     const int steps = cfg.model == TBG_MODEL_MLP ? std::min(std::max(cfg.train_steps, 1), 500) : 0;
     const int use_model = cfg.model == TBG_MODEL_SAMPLE ? 0 : 1;
@@ -155,13 +153,13 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     SBypass bp;
     memset(&bp, 0, sizeof bp);
     if (bypass) {
-        if ((e = launch_heavy_build(lb, hkeys, hfilter, hinserted, s2)) != cudaSuccess)
+        if ((e = launch_heavy_build(lb, hkeys, hinserted, s2)) != cudaSuccess)
             return cuda_error(e, "heavy build");
         uint32_t *rpay = nullptr;
         if (mat) {
             // the S histogram emits heavy pairs on the spot: R's heavy rows
             // (counts, then payload lists of at most |R| entries) come first
-            if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, s2)) !=
+            if ((e = launch_heavy_r(dR, nR, hkeys, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, s2)) !=
                 cudaSuccess)
                 return cuda_error(e, "heavy R");
         } else {
@@ -170,7 +168,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
             if ((e = cudaEventRecord(w.table, s2)) != cudaSuccess ||
                 (e = cudaStreamWaitEvent(st, w.table, 0)) != cudaSuccess)
                 return cuda_error(e, "event");
-            if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, st)) !=
+            if ((e = launch_heavy_r(dR, nR, hkeys, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, st)) !=
                 cudaSuccess)
                 return cuda_error(e, "heavy R");
         }
@@ -178,12 +176,11 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
             if ((e = w.misc.ensure(std::max<uint64_t>(nR, 1) * 4 + 64)) != cudaSuccess)
                 return cuda_error(e, "cudaMalloc");
             rpay = w.misc.as<uint32_t>();
-            if ((e = launch_heavy_r(dR, nR, hkeys, hfilter, hcnt, hstart, hcur, rpay, 1, w.nsm, s2)) != cudaSuccess)
+            if ((e = launch_heavy_r(dR, nR, hkeys, hcnt, hstart, hcur, rpay, 1, w.nsm, s2)) != cudaSuccess)
                 return cuda_error(e, "heavy R");
         }
         if ((e = cudaMemcpyAsync(&ctrl->heavy_keys, hinserted, 4, cudaMemcpyDeviceToDevice, s2)) != cudaSuccess)
             return cuda_error(e, "copy");
-        bp.filter = hfilter;
         bp.keys = hkeys;
         bp.cnt = hcnt;
         bp.scnt = hscnt;

@@ -32,150 +32,261 @@ namespace tbg {
 // model
 // ---------------------------------------------------------------------------
 // parameter layout: W1[H], b1[H], W2[H][H] (row o, column i), b2[H], W3[H], b3
-__device__ __forceinline__ float tanh_f(float x) { return tanhf(x); }
+constexpr int P_W1 = 0, P_B1 = MLP_H, P_W2 = 2 * MLP_H, P_B2 = P_W2 + MLP_H * MLP_H, P_W3 = P_B2 + MLP_H,
+              P_B3 = P_W3 + MLP_H;
 
-__device__ float mlp_forward(const float *__restrict__ p, float x, float *h1, float *h2) {
-    const float *W1 = p, *b1 = p + MLP_H, *W2 = p + 2 * MLP_H, *b2 = W2 + MLP_H * MLP_H, *W3 = b2 + MLP_H,
-                *b3 = W3 + MLP_H;
+// tanh(x) = 1 - 2 / (e^(2x) + 1), through the fast exponential: about 1e-7
+// absolute error, a fraction of the instructions of tanhf.  |x| <= 15 keeps
+// e^(2x) finite; tanh(15) rounds to 1 in single precision.
+__device__ __forceinline__ float tanh_f(float x) {
+    x = fminf(fmaxf(x, -15.f), 15.f);
+    return 1.f - __fdividef(2.f, __expf(2.f * x) + 1.f);
+}
+
+// One evaluation by one thread (the decision's model evaluations).
+__device__ float mlp_eval(const float *__restrict__ p, float x) {
+    float h1[MLP_H];
 #pragma unroll
-    for (int i = 0; i < MLP_H; i++) h1[i] = tanh_f(W1[i] * x + b1[i]);
-    float out = b3[0];
+    for (int i = 0; i < MLP_H; i++) h1[i] = tanh_f(p[P_W1 + i] * x + p[P_B1 + i]);
+    float out = p[P_B3];
 #pragma unroll 4
     for (int o = 0; o < MLP_H; o++) {
-        float z = b2[o];
+        float z = p[P_B2 + o];
 #pragma unroll
-        for (int i = 0; i < MLP_H; i++) z += W2[o * MLP_H + i] * h1[i];
-        h2[o] = tanh_f(z);
-        out += W3[o] * h2[o];
+        for (int i = 0; i < MLP_H; i++) z += p[P_W2 + o * MLP_H + i] * h1[i];
+        out += p[P_W3 + o] * tanh_f(z);
     }
     return out;
 }
 
-__device__ float mlp_eval(const float *__restrict__ p, float x) {
-    float h1[MLP_H], h2[MLP_H];
-    return mlp_forward(p, x, h1, h2);
-}
+// A batch of MLP_BATCH_CTA samples is processed by MLP_TRAIN_THREADS threads
+// (16 warps).  Forward and backward: warp w serves samples 32 (w / 4) + lane
+// and hidden units [8 (w % 4), 8 (w % 4) + 8) of both layers, so the lanes of
+// a warp read every weight as a broadcast; the four warps of a sample group
+// exchange activations through shared memory under a named barrier.  The
+// per-sample rows have a stride of MLP_H + 1 floats: a warp's lanes (one
+// sample each) touch distinct banks.
+constexpr int RS = MLP_H + 1;
+constexpr int MLP_UNITS_WARP = MLP_H / 4;  // hidden units per warp
+constexpr int GR_SLICES = 8;               // sample slices of the parameter-gradient sums
+static_assert(MLP_TRAIN_THREADS == 4 * MLP_BATCH_CTA, "four warps per 32 samples");
+static_assert(MLP_TRAIN_THREADS == 64 * GR_SLICES && MLP_BATCH_CTA % GR_SLICES == 0, "gradient slices");
 
-// Backward of one sample for output gradient dout: fills dz2 (pre-activation
-// gradient of layer 2) and dz1 (of layer 1).
-__device__ void mlp_backward(const float *__restrict__ p, const float *h1, const float *h2, float dout,
-                             float *dz2, float *dz1) {
-    const float *W2 = p + 2 * MLP_H, *b2 = W2 + MLP_H * MLP_H, *W3 = b2 + MLP_H;
-#pragma unroll
-    for (int o = 0; o < MLP_H; o++) dz2[o] = dout * W3[o] * (1.f - h2[o] * h2[o]);
-#pragma unroll 4
-    for (int i = 0; i < MLP_H; i++) {
-        float dh = 0.f;
-#pragma unroll
-        for (int o = 0; o < MLP_H; o++) dh += W2[o * MLP_H + i] * dz2[o];
-        dz1[i] = dh * (1.f - h1[i] * h1[i]);
-    }
-}
-
-// Per-sample activations of a CTA's batch, stored for the parameter
-// gradient reductions: row s = sample s (padded to 33 floats against bank
-// conflicts).
 struct BatchSmem {
-    float h1[MLP_BATCH_CTA][MLP_H + 1];
-    float h2[MLP_BATCH_CTA][MLP_H + 1];
-    float dz2[MLP_BATCH_CTA][MLP_H + 1];
-    float dz1[MLP_BATCH_CTA][MLP_H + 1];
+    float h1[MLP_BATCH_CTA][RS];
+    float h2[MLP_BATCH_CTA][RS];
+    float dz2[MLP_BATCH_CTA][RS];
+    float dz1[MLP_BATCH_CTA][RS];
     float x[MLP_BATCH_CTA];
     float dout[MLP_BATCH_CTA];
+    float part[4][MLP_BATCH_CTA];  // output partial of each unit group
+    alignas(16) float red[GR_SLICES][MLP_PARAMS_PAD];  // per-slice gradient partials
 };
 
-// Sum over s < nb of a[s] * b[s] (or of a[s] when b is null) read with the
-// given row strides, in four independent partial sums (the loop is latency
-// bound otherwise).
-__device__ __forceinline__ float dot_rows(const float *a, int sa, const float *bb, int sb, int nb) {
-    float g0 = 0.f, g1 = 0.f, g2 = 0.f, g3 = 0.f;
-    int s = 0;
-    if (bb) {
-        for (; s + 4 <= nb; s += 4) {
-            g0 += a[s * sa] * bb[s * sb];
-            g1 += a[(s + 1) * sa] * bb[(s + 1) * sb];
-            g2 += a[(s + 2) * sa] * bb[(s + 2) * sb];
-            g3 += a[(s + 3) * sa] * bb[(s + 3) * sb];
-        }
-        for (; s < nb; s++) g0 += a[s * sa] * bb[s * sb];
-    } else {
-        for (; s + 4 <= nb; s += 4) {
-            g0 += a[s * sa];
-            g1 += a[(s + 1) * sa];
-            g2 += a[(s + 2) * sa];
-            g3 += a[(s + 3) * sa];
-        }
-        for (; s < nb; s++) g0 += a[s * sa];
+__device__ __forceinline__ float4 ld4(const float *a) { return *reinterpret_cast<const float4 *>(a); }
+
+// Barrier of the four warps of sample group g (named barriers 1 .. 4, given
+// as immediates so that the kernel reserves only those).
+__device__ __forceinline__ void group_sync(int g) {
+    switch (g) {
+        case 0: asm volatile("bar.sync 1, 128;" ::: "memory"); break;
+        case 1: asm volatile("bar.sync 2, 128;" ::: "memory"); break;
+        case 2: asm volatile("bar.sync 3, 128;" ::: "memory"); break;
+        default: asm volatile("bar.sync 4, 128;" ::: "memory"); break;
     }
-    return (g0 + g1) + (g2 + g3);
 }
 
-// Gradient of parameter q summed over the nb samples in `b`.
-__device__ __forceinline__ float param_grad(const BatchSmem &b, int q, int nb) {
-    constexpr int RS = MLP_H + 1;  // row stride of the activation arrays
-    if (q < MLP_H) return dot_rows(&b.dz1[0][q], RS, b.x, 1, nb);                 // W1[i]
-    if (q < 2 * MLP_H) return dot_rows(&b.dz1[0][q - MLP_H], RS, nullptr, 0, nb);  // b1[i]
-    if (q < 2 * MLP_H + MLP_H * MLP_H) {                                           // W2[o][i]
-        const int o = (q - 2 * MLP_H) / MLP_H, i = (q - 2 * MLP_H) % MLP_H;
-        return dot_rows(&b.dz2[0][o], RS, &b.h1[0][i], RS, nb);
-    }
-    if (q < 3 * MLP_H + MLP_H * MLP_H) return dot_rows(&b.dz2[0][q - 2 * MLP_H - MLP_H * MLP_H], RS, nullptr, 0, nb);
-    if (q < 4 * MLP_H + MLP_H * MLP_H) return dot_rows(b.dout, 1, &b.h2[0][q - 3 * MLP_H - MLP_H * MLP_H], RS, nb);
-    return dot_rows(b.dout, 1, nullptr, 0, nb);                                    // b3
-}
-
-// One sample's forward + backward, activations stored in row `s`.
-__device__ float sample_fwd_bwd(const float *p, float x, float y, float scale, BatchSmem &b, int s) {
-    float h1[MLP_H], h2[MLP_H], dz2[MLP_H], dz1[MLP_H];
-    const float out = mlp_forward(p, x, h1, h2);
-    const float r = out - y;
-    const float dout = 2.f * r * scale;
-    mlp_backward(p, h1, h2, dout, dz2, dz1);
+// Dot product of a 16-byte aligned shared row of MLP_H floats with v
+// (two accumulators).
+__device__ __forceinline__ float dot_row(const float *w, const float (&v)[MLP_H], float acc) {
+    float a0 = acc, a1 = 0.f;
 #pragma unroll
-    for (int i = 0; i < MLP_H; i++) {
-        b.h1[s][i] = h1[i];
-        b.h2[s][i] = h2[i];
-        b.dz2[s][i] = dz2[i];
-        b.dz1[s][i] = dz1[i];
+    for (int i = 0; i < MLP_H; i += 8) {
+        const float4 x = ld4(w + i), y = ld4(w + i + 4);
+        a0 = fmaf(x.x, v[i], a0);
+        a1 = fmaf(x.y, v[i + 1], a1);
+        a0 = fmaf(x.z, v[i + 2], a0);
+        a1 = fmaf(x.w, v[i + 3], a1);
+        a0 = fmaf(y.x, v[i + 4], a0);
+        a1 = fmaf(y.y, v[i + 5], a1);
+        a0 = fmaf(y.z, v[i + 6], a0);
+        a1 = fmaf(y.w, v[i + 7], a1);
     }
-    b.x[s] = x;
-    b.dout[s] = dout;
+    return a0 + a1;
+}
+
+// Forward and backward of sample s (input x, target y, loss weight scale) by
+// warp j of its sample group g, which owns hidden units [8j, 8j + 8).
+// Leaves the sample's activations, pre-activation gradients and output
+// gradient in row s; returns the squared error.  Every thread of the group
+// calls it (named barriers).
+__device__ float group_fwd_bwd(const float *p, BatchSmem &b, float x, float y, float scale, int s, int g, int j) {
+    constexpr int U = MLP_UNITS_WARP;
+    const int u0 = U * j;
+    float *h1 = b.h1[s], *h2 = b.h2[s], *dz2 = b.dz2[s], *dz1 = b.dz1[s];
+#pragma unroll
+    for (int t = 0; t < U; t++) h1[u0 + t] = tanh_f(p[P_W1 + u0 + t] * x + p[P_B1 + u0 + t]);
+    group_sync(g);
+    float v[MLP_H];
+#pragma unroll
+    for (int i = 0; i < MLP_H; i++) v[i] = h1[i];
+    float part = 0.f, g2[U];
+#pragma unroll
+    for (int t = 0; t < U; t++) {
+        const int u = u0 + t;
+        const float h = tanh_f(dot_row(p + P_W2 + u * MLP_H, v, p[P_B2 + u]));
+        h2[u] = h;
+        const float w3 = p[P_W3 + u];
+        part = fmaf(w3, h, part);
+        g2[t] = w3 * (1.f - h * h);
+    }
+    b.part[j][s] = part;
+    group_sync(g);
+    const float r = p[P_B3] + ((b.part[0][s] + b.part[1][s]) + (b.part[2][s] + b.part[3][s])) - y;
+    const float dout = 2.f * r * scale;
+#pragma unroll
+    for (int t = 0; t < U; t++) dz2[u0 + t] = dout * g2[t];
+    group_sync(g);
+#pragma unroll
+    for (int o = 0; o < MLP_H; o++) v[o] = dz2[o];
+    // dz1[i] = (1 - h1[i]^2) sum_o W2[o][i] dz2[o] for the warp's units i
+    float acc[U];
+#pragma unroll
+    for (int t = 0; t < U; t++) acc[t] = 0.f;
+#pragma unroll
+    for (int o = 0; o < MLP_H; o++) {
+        const float4 a = ld4(p + P_W2 + o * MLP_H + u0), c = ld4(p + P_W2 + o * MLP_H + u0 + 4);
+        acc[0] = fmaf(a.x, v[o], acc[0]);
+        acc[1] = fmaf(a.y, v[o], acc[1]);
+        acc[2] = fmaf(a.z, v[o], acc[2]);
+        acc[3] = fmaf(a.w, v[o], acc[3]);
+        acc[4] = fmaf(c.x, v[o], acc[4]);
+        acc[5] = fmaf(c.y, v[o], acc[5]);
+        acc[6] = fmaf(c.z, v[o], acc[6]);
+        acc[7] = fmaf(c.w, v[o], acc[7]);
+    }
+#pragma unroll
+    for (int t = 0; t < U; t++) {
+        const float a = h1[u0 + t];
+        dz1[u0 + t] = acc[t] * (1.f - a * a);
+    }
+    if (j == 0) {
+        b.x[s] = x;
+        b.dout[s] = dout;
+    }
     return r * r;
+}
+
+// Gradient of every parameter summed over samples 0 .. nb of the batch, into
+// g[0 .. MLP_PARAMS), by all MLP_TRAIN_THREADS threads (a __syncthreads
+// inside).  Slice k of GR_SLICES takes samples [16k, 16k + 16) on 64
+// threads: each sums one 4 x 4 tile of W2's gradient and two or three of the
+// other parameters over its slice into the slice's partials; then every
+// thread adds the slices' partials of its parameters.
+__device__ void batch_param_grad(BatchSmem &b, int nb, float *g) {
+    constexpr int SPAN = MLP_BATCH_CTA / GR_SLICES;
+    const int tid = threadIdx.x, sl = tid >> 6, t = tid & 63;
+    const int s0 = sl * SPAN, s1 = min(nb, s0 + SPAN);
+    float *red = b.red[sl];
+    {
+        const int o0 = (t >> 3) * 4, i0 = (t & 7) * 4;
+        float acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[a][c] = 0.f;
+        for (int s = s0; s < s1; s++) {
+            float d[4], h[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                d[k] = b.dz2[s][o0 + k];
+                h[k] = b.h1[s][i0 + k];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[a][c] = fmaf(d[a], h[c], acc[a][c]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+            *reinterpret_cast<float4 *>(red + P_W2 + (o0 + a) * MLP_H + i0) =
+                make_float4(acc[a][0], acc[a][1], acc[a][2], acc[a][3]);
+    }
+    // the slice's first warp: W1[i] and b2[i]; its second: b1[i] and W3[i];
+    // thread 0 also b3 (i = lane, MLP_H = 32)
+    {
+        static_assert(MLP_H == 32, "one lane per hidden unit");
+        const int i = t & 31;
+        float a = 0.f, c = 0.f;
+        if (t < 32) {
+            for (int s = s0; s < s1; s++) {
+                a = fmaf(b.dz1[s][i], b.x[s], a);
+                c += b.dz2[s][i];
+            }
+            red[P_W1 + i] = a;
+            red[P_B2 + i] = c;
+        } else {
+            for (int s = s0; s < s1; s++) {
+                a += b.dz1[s][i];
+                c = fmaf(b.dout[s], b.h2[s][i], c);
+            }
+            red[P_B1 + i] = a;
+            red[P_W3 + i] = c;
+        }
+        if (t == 0) {
+            float d = 0.f;
+            for (int s = s0; s < s1; s++) d += b.dout[s];
+            red[P_B3] = d;
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) {
+        float a = 0.f;
+#pragma unroll
+        for (int k = 0; k < GR_SLICES; k++) a += b.red[k][q];
+        g[q] = a;
+    }
 }
 
 // Full-batch gradient and loss sum over n samples (tests and the reported
 // training loss): CTAs take MLP_BATCH_CTA samples each and add their partial
 // gradients to grad[] with atomics.
-__global__ void __launch_bounds__(MLP_BATCH_CTA) k_mlp_grad(const float *__restrict__ params,
-                                                            const float *__restrict__ xs,
-                                                            const float *__restrict__ ys, uint32_t n,
-                                                            float *grad, float *loss_sum) {
+__global__ void __launch_bounds__(MLP_TRAIN_THREADS, 1) k_mlp_grad(const float *__restrict__ params,
+                                                                const float *__restrict__ xs,
+                                                                const float *__restrict__ ys, uint32_t n,
+                                                                float *grad, float *loss_sum) {
     extern __shared__ __align__(16) unsigned char smem[];
     float *p = reinterpret_cast<float *>(smem);
-    BatchSmem &b = *reinterpret_cast<BatchSmem *>(p + MLP_PARAMS_PAD);
-    for (int q = threadIdx.x; q < MLP_PARAMS; q += MLP_BATCH_CTA) p[q] = params[q];
+    float *gl = p + MLP_PARAMS_PAD;
+    BatchSmem &b = *reinterpret_cast<BatchSmem *>(gl + MLP_PARAMS_PAD);
+    const int tid = threadIdx.x, w = tid >> 5, g = w >> 2, j = w & 3, s = 32 * g + (tid & 31);
+    for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) p[q] = params[q];
     __syncthreads();
     const uint32_t s0 = blockIdx.x * MLP_BATCH_CTA;
     const int nb = (int)min((uint32_t)MLP_BATCH_CTA, n - s0);
-    float l = 0.f;
-    if ((int)threadIdx.x < nb) {
-        const uint32_t i = s0 + threadIdx.x;
-        l = sample_fwd_bwd(p, xs[i], ys[i], 1.f / (float)n, b, threadIdx.x);
-    }
+    const bool ok = s < nb;
+    // every group runs (named barriers); samples past n add nothing
+    const float l = group_fwd_bwd(p, b, ok ? xs[s0 + s] : 0.f, ok ? ys[s0 + s] : 0.f, 1.f / (float)n, s, g, j);
     __syncthreads();
-    for (int q = threadIdx.x; q < MLP_PARAMS; q += MLP_BATCH_CTA) atomicAdd(&grad[q], param_grad(b, q, nb));
-    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, l);
+    batch_param_grad(b, nb, gl);
+    __syncthreads();
+    for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) atomicAdd(&grad[q], gl[q]);
+    float lw = (ok && j == 0) ? l : 0.f;
+    for (int o = 16; o > 0; o >>= 1) lw += __shfl_xor_sync(0xffffffffu, lw, o);
+    if ((tid & 31) == 0) atomicAdd(loss_sum, lw);
 }
+
+// Training points staged in the trainer's shared memory (larger point sets
+// are read from global memory).
+constexpr int MLP_STAGE = CC_BINS;
 
 // Trainer: one cluster of MLP_CLUSTER CTAs, persistent over all steps.  Each
 // step every CTA draws MLP_BATCH_CTA seeded random training points (uniformly,
-// or in proportion to their weights), computes their forward/backward on its
-// first MLP_BATCH_CTA threads and its partial parameter gradient on all
-// MLP_TRAIN_THREADS; after a cluster
-// barrier CTA r sums the partials of its parameter slice from every CTA's
-// shared memory, applies Adam, and writes the new values into every CTA's
-// parameter copy; a second barrier ends the step.
+// or in proportion to their weights), runs their forward and backward passes
+// and its partial parameter gradient; after a
+// cluster barrier CTA r sums the partials of its parameter slice from every
+// CTA's shared memory, applies Adam, and writes the new values into every
+// CTA's parameter copy; a second barrier ends the step.
 __global__ void __cluster_dims__(MLP_CLUSTER, 1, 1) __launch_bounds__(MLP_TRAIN_THREADS)
     k_mlp_train(const float *__restrict__ xs, const float *__restrict__ ys, const float *__restrict__ cw,
                 const unsigned *n_dev, uint32_t n_host, float *params, int steps, float lr0, uint64_t seed) {
@@ -191,46 +302,60 @@ __global__ void __cluster_dims__(MLP_CLUSTER, 1, 1) __launch_bounds__(MLP_TRAIN_
     float *am = gpart + MLP_PARAMS_PAD;  // Adam moments of this CTA's slice
     float *av = am + MLP_SLICE;
     BatchSmem &b = *reinterpret_cast<BatchSmem *>(av + MLP_SLICE);
-    const int tid = threadIdx.x;
+    float *sx = reinterpret_cast<float *>(&b + 1), *sy = sx + MLP_STAGE, *scw = sy + MLP_STAGE;
+    const int tid = threadIdx.x, w = tid >> 5, g = w >> 2, j = w & 3, s = 32 * g + (tid & 31);
+    const bool staged = n <= (uint32_t)MLP_STAGE;
     for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) p[q] = params[q];
     for (int q = tid; q < MLP_SLICE; q += MLP_TRAIN_THREADS) am[q] = av[q] = 0.f;
+    if (staged)
+        for (uint32_t q = tid; q < n; q += MLP_TRAIN_THREADS) {
+            sx[q] = xs[q];
+            sy[q] = ys[q];
+            if (cw) scw[q] = cw[q];
+        }
+    const float *px = staged ? sx : xs, *py = staged ? sy : ys, *pw = staged ? scw : cw;
     cl.sync();
     const float b1c = 0.9f, b2c = 0.999f, eps = 1e-8f;
     const float scale = 1.f / (float)(MLP_BATCH_CTA * MLP_CLUSTER);
     const int q0 = rank * MLP_SLICE, q1 = min(MLP_PARAMS, q0 + MLP_SLICE);
-    const float wtot = cw ? cw[n - 1] : 0.f;
+    const float wtot = cw ? pw[n - 1] : 0.f;
     float pow1 = 1.f, pow2 = 1.f;
     for (int step = 0; step < steps; step++) {
-        if (tid < MLP_BATCH_CTA) {  // one sample per thread of the first warps
-            const uint64_t h = mix64(seed ^ mix64(((uint64_t)step << 20) | (uint64_t)(rank * MLP_BATCH_CTA + tid)));
+        // sample s: the group's first warp draws the point, the other three
+        // read it after the group barrier
+        if (j == 0) {
+            const uint64_t hsh = mix64(seed ^ mix64(((uint64_t)step << 20) | (uint64_t)(rank * MLP_BATCH_CTA + s)));
             uint32_t i;
             if (cw) {  // the first point whose cumulative weight exceeds u * total
-                const float u = (float)((h >> 40) * (1.0 / 16777216.0)) * wtot;
+                const float u = (float)((hsh >> 40) * (1.0 / 16777216.0)) * wtot;
                 uint32_t lo = 0, hi = n - 1;
                 while (lo < hi) {
                     const uint32_t mid = (lo + hi) >> 1;
-                    if (cw[mid] > u) hi = mid;
+                    if (pw[mid] > u) hi = mid;
                     else lo = mid + 1;
                 }
                 i = lo;
             } else {
-                i = (uint32_t)(h % n);
+                i = (uint32_t)(hsh % n);
             }
-            sample_fwd_bwd(p, xs[i], ys[i], scale, b, tid);
+            b.x[s] = px[i];
+            b.dout[s] = py[i];  // the target, until the backward pass overwrites it
         }
+        group_sync(g);
+        group_fwd_bwd(p, b, b.x[s], b.dout[s], scale, s, g, j);
         __syncthreads();
-        for (int q = tid; q < MLP_PARAMS; q += MLP_TRAIN_THREADS) gpart[q] = param_grad(b, q, MLP_BATCH_CTA);
+        batch_param_grad(b, MLP_BATCH_CTA, gpart);
         cl.sync();
         pow1 *= b1c;
         pow2 *= b2c;
         // cosine decay from lr0 to lr0 / 10
         const float lr = lr0 * (0.55f + 0.45f * cospif((float)step / (float)(steps > 1 ? steps - 1 : 1)));
         for (int q = q0 + tid; q < q1; q += MLP_TRAIN_THREADS) {
-            float g = 0.f;
-            for (int r = 0; r < MLP_CLUSTER; r++) g += cl.map_shared_rank(gpart, r)[q];
+            float gs = 0.f;
+            for (int r = 0; r < MLP_CLUSTER; r++) gs += cl.map_shared_rank(gpart, r)[q];
             const int k = q - q0;
-            am[k] = b1c * am[k] + (1.f - b1c) * g;
-            av[k] = b2c * av[k] + (1.f - b2c) * g * g;
+            am[k] = b1c * am[k] + (1.f - b1c) * gs;
+            av[k] = b2c * av[k] + (1.f - b2c) * gs * gs;
             const float mh = am[k] / (1.f - pow1), vh = av[k] / (1.f - pow2);
             const float np = p[q] - lr * mh / (sqrtf(vh) + eps);
             for (int r = 0; r < MLP_CLUSTER; r++) cl.map_shared_rank(p, r)[q] = np;
@@ -257,9 +382,9 @@ __global__ void k_mlp_init(float *params, uint64_t seed) {
 }
 
 size_t mlp_train_smem() {
-    return (size_t)(2 * MLP_PARAMS_PAD + 2 * MLP_SLICE) * 4 + sizeof(BatchSmem);
+    return (size_t)(2 * MLP_PARAMS_PAD + 2 * MLP_SLICE) * 4 + sizeof(BatchSmem) + (size_t)3 * MLP_STAGE * 4;
 }
-size_t mlp_grad_smem() { return (size_t)MLP_PARAMS_PAD * 4 + sizeof(BatchSmem); }
+size_t mlp_grad_smem() { return (size_t)2 * MLP_PARAMS_PAD * 4 + sizeof(BatchSmem); }
 
 cudaError_t launch_mlp_init(float *params, uint64_t seed, cudaStream_t st) {
     k_mlp_init<<<1, 256, 0, st>>>(params, seed);
@@ -275,7 +400,8 @@ cudaError_t launch_mlp_grad(const float *params, const float *xs, const float *y
     const size_t smem = mlp_grad_smem();
     e = smem_limit((const void *)k_mlp_grad, smem);
     if (e != cudaSuccess) return e;
-    k_mlp_grad<<<(n + MLP_BATCH_CTA - 1) / MLP_BATCH_CTA, MLP_BATCH_CTA, smem, st>>>(params, xs, ys, n, grad, loss_sum);
+    k_mlp_grad<<<(n + MLP_BATCH_CTA - 1) / MLP_BATCH_CTA, MLP_TRAIN_THREADS, smem, st>>>(params, xs, ys, n, grad,
+                                                                                         loss_sum);
     count_launch();
     return cudaGetLastError();
 }
@@ -324,15 +450,22 @@ cudaError_t launch_sample_blocks(const Row *S, uint64_t nS, uint32_t *keys, uint
 
 __device__ __forceinline__ uint32_t count_hash(uint32_t k) { return (k * 0x9E3779B1u) ^ (k >> 15); }
 
-// Adds c to key k's count in the global open-addressing table (tmask + 1
-// slots).  A full table drops the key: a key that is not counted is never
-// heavy, which only costs speed.
-__device__ __forceinline__ void table_add(uint32_t *tk, uint32_t *tc, uint32_t tmask, uint32_t k, uint32_t c) {
-    uint32_t h = count_hash(k) & tmask;
+// The global count table: one 64-bit word per slot, key << 32 | count, so a
+// new key is claimed and counted by one compare-and-swap.  CNT_EMPTY (all
+// ones) marks a free slot: its key is EMPTY_KEY, which is never counted.
+constexpr unsigned long long CNT_EMPTY = ~0ull;
+__device__ __forceinline__ unsigned long long cnt_word(uint32_t k, uint32_t c) {
+    return ((unsigned long long)k << 32) | c;
+}
+
+// Adds c to key k's count, probing from slot h.  A full table drops the key:
+// a key that is not counted is never heavy, which only costs speed.
+__device__ __forceinline__ void table_add(unsigned long long *t, uint32_t tmask, uint32_t k, uint32_t c, uint32_t h) {
     for (uint32_t probe = 0; probe <= tmask && probe < 4096; probe++) {
-        const uint32_t old = atomicCAS(&tk[h], EMPTY_KEY, k);
-        if (old == EMPTY_KEY || old == k) {
-            atomicAdd(&tc[h], c);
+        const unsigned long long old = atomicCAS(&t[h], CNT_EMPTY, cnt_word(k, c));
+        if (old == CNT_EMPTY) return;
+        if ((uint32_t)(old >> 32) == k) {
+            atomicAdd(&t[h], (unsigned long long)c);  // the count is the low word; it never carries
             return;
         }
         h = (h + 1) & tmask;
@@ -342,10 +475,13 @@ __device__ __forceinline__ void table_add(uint32_t *tk, uint32_t *tc, uint32_t t
 // Counts the sample's keys: CTA c aggregates keys [c * CNT_CHUNK, ...) in a
 // shared table (equal keys of a warp first combined with __match_any_sync,
 // so a hot key costs one shared atomic per warp), then adds each distinct
-// key once to the global table.  Key EMPTY_KEY is never counted.
-__global__ void __launch_bounds__(CNT_THREADS) k_count_keys(const uint32_t *__restrict__ keys, uint64_t m,
-                                                           uint32_t *tk, uint32_t *tc, uint32_t tmask) {
+// key once to the global table: every thread first issues the
+// compare-and-swap of each of its slots at the key's home slot, and only the
+// slots that met another key probe on.  Key EMPTY_KEY is never counted.
+__global__ void __launch_bounds__(CNT_THREADS, 2) k_count_keys(const uint32_t *__restrict__ keys, uint64_t m,
+                                                           unsigned long long *table, uint32_t tmask) {
     constexpr int SLOTS = 2 * CNT_CHUNK;
+    constexpr int PER = SLOTS / CNT_THREADS;
     __shared__ uint32_t lk[SLOTS];
     __shared__ uint32_t lc[SLOTS];
     for (int i = threadIdx.x; i < SLOTS; i += CNT_THREADS) {
@@ -373,14 +509,29 @@ __global__ void __launch_bounds__(CNT_THREADS) k_count_keys(const uint32_t *__re
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < SLOTS; i += CNT_THREADS)
-        if (lk[i] != EMPTY_KEY) table_add(tk, tc, tmask, lk[i], lc[i]);
+    uint32_t fk[PER], fc[PER], fh[PER];
+    unsigned long long old[PER];
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int i = q * CNT_THREADS + threadIdx.x;
+        fk[q] = lk[i];
+        fc[q] = lc[i];
+        fh[q] = count_hash(fk[q]) & tmask;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; q++)  // independent: the compare-and-swaps are all in flight at once
+        old[q] = fk[q] != EMPTY_KEY ? atomicCAS(&table[fh[q]], CNT_EMPTY, cnt_word(fk[q], fc[q])) : CNT_EMPTY;
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        if (fk[q] == EMPTY_KEY || old[q] == CNT_EMPTY) continue;
+        if ((uint32_t)(old[q] >> 32) == fk[q]) atomicAdd(&table[fh[q]], (unsigned long long)fc[q]);
+        else table_add(table, tmask, fk[q], fc[q], (fh[q] + 1) & tmask);
+    }
 }
 
 cudaError_t launch_count_keys(const LearnBufs &b, uint64_t m, cudaStream_t st) {
     if (!m) return cudaSuccess;
-    k_count_keys<<<(unsigned)((m + CNT_CHUNK - 1) / CNT_CHUNK), CNT_THREADS, 0, st>>>(b.keys, m, b.tkeys, b.tcnt,
-                                                                                      b.tmask);
+    k_count_keys<<<(unsigned)((m + CNT_CHUNK - 1) / CNT_CHUNK), CNT_THREADS, 0, st>>>(b.keys, m, b.table, b.tmask);
     count_launch();
     return cudaGetLastError();
 }
@@ -404,37 +555,87 @@ __host__ __device__ __forceinline__ uint32_t cc_bin_min(int b) {
 
 // Count-of-counts over the table (keys per bin, sample rows per bin) and the
 // candidate list: the keys the sample saw at least CAND_MIN_COUNT times.
+// Each thread reads STATS_PER consecutive slots per round.  Lanes whose count
+// falls in the same exact bin (most of them: counts 1, 2, 3 ...) add to it
+// once per warp (__match_any_sync); the candidates' list positions come
+// from one global atomic per CTA and round.
 constexpr int STATS_THREADS = 1024;
+constexpr int STATS_PER = 4;
 
-__global__ void __launch_bounds__(STATS_THREADS) k_count_stats(const uint32_t *__restrict__ tk, const uint32_t *__restrict__ tc,
-                                                    uint32_t tmask, unsigned *bin_keys,
-                                                    unsigned long long *bin_rows, HeavyCand *cand,
-                                                    unsigned cand_cap, LrnDecision *dec) {
+__global__ void __launch_bounds__(STATS_THREADS, 2) k_count_stats(const unsigned long long *__restrict__ table,
+                                                               uint32_t tmask, unsigned *bin_keys,
+                                                               unsigned long long *bin_rows, HeavyCand *cand,
+                                                               unsigned cand_cap, LrnDecision *dec) {
     __shared__ unsigned sk[CC_BINS];
     __shared__ unsigned long long sr[CC_BINS];
+    __shared__ unsigned wbase[STATS_THREADS / 32];
     for (int i = threadIdx.x; i < CC_BINS; i += STATS_THREADS) {
         sk[i] = 0;
         sr[i] = 0;
     }
     __syncthreads();
-    const uint64_t slots = (uint64_t)tmask + 1;
-    const int lane = threadIdx.x & 31;
-    for (uint64_t base = (uint64_t)blockIdx.x * STATS_THREADS; base < slots; base += (uint64_t)gridDim.x * STATS_THREADS) {
-        const uint64_t i = base + threadIdx.x;  // warp-uniform trip count (slots is a multiple of STATS_THREADS)
-        const uint32_t k = tk[i], c = tc[i];
-        const bool used = k != EMPTY_KEY && c > 0;
-        if (used) {
-            const int b = cc_bin(c);
-            atomicAdd(&sk[b], 1u);
-            atomicAdd(&sr[b], (unsigned long long)c);
+    const uint64_t groups = ((uint64_t)tmask + 1) / STATS_PER;  // a multiple of STATS_THREADS
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = lanemask_lt();
+    for (uint64_t base = (uint64_t)blockIdx.x * STATS_THREADS; base < groups;
+         base += (uint64_t)gridDim.x * STATS_THREADS) {
+        const uint64_t g = base + threadIdx.x;  // warp- and block-uniform trip count
+        const ulonglong2 a = reinterpret_cast<const ulonglong2 *>(table)[2 * g];
+        const ulonglong2 c = reinterpret_cast<const ulonglong2 *>(table)[2 * g + 1];
+        const unsigned long long wv[STATS_PER] = {a.x, a.y, c.x, c.y};
+        unsigned cm = 0;
+#pragma unroll
+        for (int q = 0; q < STATS_PER; q++) {
+            const uint32_t k = (uint32_t)(wv[q] >> 32), n = (uint32_t)wv[q];
+            const bool used = k != EMPTY_KEY && n > 0;
+            const bool exact = used && n < (uint32_t)CC_EXACT;
+            const unsigned peers = __match_any_sync(0xffffffffu, exact ? n : 0xFFFFFFFFu);
+            if (exact) {
+                if ((peers & lt) == 0) {
+                    const unsigned cnt = (unsigned)__popc(peers);
+                    atomicAdd(&sk[n], cnt);
+                    atomicAdd(&sr[n], (unsigned long long)cnt * n);
+                }
+            } else if (used) {
+                const int b = cc_bin(n);
+                atomicAdd(&sk[b], 1u);
+                atomicAdd(&sr[b], (unsigned long long)n);
+            }
+            if (used && n >= (uint32_t)CAND_MIN_COUNT) cm |= 1u << q;
         }
-        const bool is_cand = used && c >= (uint32_t)CAND_MIN_COUNT;
-        const unsigned bal = __ballot_sync(0xffffffffu, is_cand);
-        unsigned wb = 0;
-        if (lane == 0 && bal) wb = atomicAdd(&dec->ncand, (unsigned)__popc(bal));
-        wb = __shfl_sync(0xffffffffu, wb, 0);
-        const unsigned pos = wb + __popc(bal & lanemask_lt());
-        if (is_cand && pos < cand_cap) cand[pos] = HeavyCand{k, c};
+        // candidate positions: warp prefix, then one global atomic per CTA
+        uint32_t inc = (uint32_t)__popc(cm);
+        const uint32_t mine = inc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) wbase[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            const uint32_t t = wbase[lane];
+            uint32_t x = t;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            unsigned b0 = 0;
+            if (lane == 31 && x) b0 = atomicAdd(&dec->ncand, x);
+            b0 = __shfl_sync(0xffffffffu, b0, 31);
+            wbase[lane] = b0 + x - t;
+        }
+        __syncthreads();
+        unsigned pos = wbase[w] + inc - mine;
+#pragma unroll
+        for (int q = 0; q < STATS_PER; q++) {
+            if (cm >> q & 1) {
+                if (pos < cand_cap) cand[pos] = HeavyCand{(uint32_t)(wv[q] >> 32), (uint32_t)wv[q]};
+                pos++;
+            }
+        }
+        __syncthreads();  // wbase is rewritten next round
     }
     __syncthreads();
     for (int i = threadIdx.x; i < CC_BINS; i += STATS_THREADS) {
@@ -446,9 +647,11 @@ __global__ void __launch_bounds__(STATS_THREADS) k_count_stats(const uint32_t *_
 }
 
 cudaError_t launch_count_stats(const LearnBufs &b, cudaStream_t st) {
-    const uint64_t slots = (uint64_t)b.tmask + 1;
-    const unsigned g = (unsigned)umin64(slots / STATS_THREADS, 148);
-    k_count_stats<<<g, STATS_THREADS, 0, st>>>(b.tkeys, b.tcnt, b.tmask, b.bin_keys, b.bin_rows, b.cand, b.cand_cap, b.dec);
+    // four rounds per CTA, two CTAs per SM: one CTA's loads and barriers
+    // overlap the other's
+    const uint64_t groups = ((uint64_t)b.tmask + 1) / STATS_PER;
+    const unsigned g = (unsigned)std::max<uint64_t>(1, groups / (STATS_THREADS * 4));
+    k_count_stats<<<g, STATS_THREADS, 0, st>>>(b.table, b.tmask, b.bin_keys, b.bin_rows, b.cand, b.cand_cap, b.dec);
     count_launch();
     return cudaGetLastError();
 }
@@ -558,110 +761,152 @@ cudaError_t launch_rank_points(const LearnBufs &b, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// Model evaluations for the decision, spread over many CTAs (one evaluation
+// per thread): lpred[r] = log2 of the predicted S rows of sample rank r,
+// mu + sigma M(rank_feature(r)) + log2(nS / m), for r = 1 .. HEAVY_MAX + 1
+// (mu and sigma the points' normalisation), and the squared error of the
+// model on the training points, added to dec->loss_sum.
+constexpr int EVAL_THREADS = 256;
+constexpr int EVAL_RANKS = HEAVY_MAX + 1;
+
+__global__ void __launch_bounds__(EVAL_THREADS) k_model_eval(const float *__restrict__ params,
+                                                            const float *__restrict__ xs,
+                                                            const float *__restrict__ ys, double lscale,
+                                                            float *lpred, LrnDecision *dec) {
+    __shared__ float p[MLP_PARAMS];
+    for (int q = threadIdx.x; q < MLP_PARAMS; q += EVAL_THREADS) p[q] = params[q];
+    __syncthreads();
+    const unsigned np = dec->npoints;
+    const int g = blockIdx.x * EVAL_THREADS + threadIdx.x;
+    double err = 0.0;
+    if (g < EVAL_RANKS) {
+        const int r = g + 1;
+        lpred[r] = (float)((double)dec->y_mu + (double)dec->y_sigma * (double)mlp_eval(p, rank_feature((double)r)) +
+                           lscale);
+    } else if ((unsigned)(g - EVAL_RANKS) < np) {
+        const unsigned i = (unsigned)(g - EVAL_RANKS);
+        const double d = (double)mlp_eval(p, xs[i]) - (double)ys[i];
+        err = d * d;
+    }
+    for (int o = 16; o > 0; o >>= 1) err += __shfl_xor_sync(0xffffffffu, err, o);
+    if ((threadIdx.x & 31) == 0 && err > 0.0) atomicAdd(&dec->loss_sum, err);
+}
+
 // The decision (one block).  pred(r), the predicted S rows of the key of
-// sample rank r, comes from the model (2^(mu + sigma M(rank_feature(r))) nS / m,
-// mu and sigma the points' normalisation) or,
-// for the ablation, from the sample's own count at rank r.  k* = the ranks
+// sample rank r, comes from the model (lpred from k_model_eval) or, for the
+// ablation, from the sample's own count at rank r.  k* = the ranks
 // 1 .. HEAVY_MAX whose predicted rows reach tau_min; the heavy keys are the
 // sampled keys whose count is at least that of rank k* (the lowest count bin
 // that keeps their number <= k*).  Bypass when the model predicts those keys
-// to hold at least min_frac of S.  Also the model's loss on the points.
-constexpr int DECIDE_THREADS = 512;
+// to hold at least min_frac of S.  The bins are read in decreasing count
+// order (j = CC_BINS - 1 - bin); above[j] counts the keys of the bins before
+// j, so rank r lies in the last j with above[j] < r, found by binary search.
+constexpr int DECIDE_THREADS = 1024;
+constexpr int DECIDE_PER = (CC_BINS + DECIDE_THREADS - 1) / DECIDE_THREADS;
 
-__global__ void __launch_bounds__(DECIDE_THREADS) k_decide(const float *__restrict__ params, int use_model,
-                                                          const unsigned *__restrict__ bin_keys,
+__global__ void __launch_bounds__(DECIDE_THREADS) k_decide(int use_model, const unsigned *__restrict__ bin_keys,
                                                           const unsigned long long *__restrict__ bin_rows,
-                                                          const float *__restrict__ xs, const float *__restrict__ ys,
-                                                          double nS, double m, double tau_min, double min_frac,
+                                                          const float *__restrict__ lpred_model, double rows_scale,
+                                                          double nS, double tau_min, double min_frac,
                                                           LrnDecision *dec) {
-    __shared__ float p[MLP_PARAMS];
-    __shared__ uint32_t cnt_at[HEAVY_MAX + 2];  // sample count of rank r (r = 1 .. HEAVY_MAX + 1)
-    __shared__ float lpred[HEAVY_MAX + 2];      // log2 of the predicted S rows of rank r
-    // the bins, staged (dynamic shared memory) for the single-thread walks below
-    extern __shared__ __align__(16) unsigned char dsm[];
-    unsigned long long *sr = reinterpret_cast<unsigned long long *>(dsm);
-    unsigned *sk = reinterpret_cast<unsigned *>(sr + CC_BINS);
+    const double lscale = log2(rows_scale);  // log2(nS / m): sample rows to S rows
+    __shared__ float lp[EVAL_RANKS + 1];  // log2 of the predicted S rows of rank r (r = 1 .. HEAVY_MAX + 1)
+    __shared__ uint64_t scratch[DECIDE_THREADS / 32 + 1];
     __shared__ double red[DECIDE_THREADS / 32];
-    __shared__ unsigned s_kstar;
+    __shared__ unsigned s_kstar, s_jstar;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    unsigned long long *sr = reinterpret_cast<unsigned long long *>(dsm);  // rows, by j
+    unsigned *sk = reinterpret_cast<unsigned *>(sr + CC_BINS);             // keys, by j
+    unsigned *above = sk + CC_BINS;                                        // keys before j
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    for (int q = t; q < MLP_PARAMS; q += DECIDE_THREADS) p[q] = params[q];
-    for (int r = t; r <= HEAVY_MAX + 1; r += DECIDE_THREADS) cnt_at[r] = 0;
-    for (int b = t; b < CC_BINS; b += DECIDE_THREADS) {
-        sk[b] = bin_keys[b];
-        sr[b] = bin_rows[b];
+    uint64_t mine = 0;
+#pragma unroll
+    for (int q = 0; q < DECIDE_PER; q++) {
+        const int j = t * DECIDE_PER + q;
+        if (j < CC_BINS) {
+            sk[j] = bin_keys[CC_BINS - 1 - j];
+            sr[j] = bin_rows[CC_BINS - 1 - j];
+            mine += sk[j];
+        }
     }
-    if (t == 0) s_kstar = 0;
-    __syncthreads();
-    // ranks 1 .. HEAVY_MAX + 1 sit in the highest bins: thread 0 walks them
     if (t == 0) {
-        unsigned r = 1;
-        for (int b = CC_BINS - 1; b >= 1 && r <= (unsigned)HEAVY_MAX + 1; b--) {
-            const unsigned nk = sk[b];
-            if (!nk) continue;
-            const uint32_t c = (uint32_t)(sr[b] / nk);
-            for (unsigned j = 0; j < nk && r <= (unsigned)HEAVY_MAX + 1; j++) cnt_at[r++] = c;
+        s_kstar = 0;
+        s_jstar = 0;  // j* + 1 of the last heavy bin; 0: none
+    }
+    uint64_t total;
+    uint64_t run = block_excl_scan<DECIDE_THREADS>(mine, &total, scratch);
+#pragma unroll
+    for (int q = 0; q < DECIDE_PER; q++) {
+        const int j = t * DECIDE_PER + q;
+        if (j < CC_BINS) {
+            above[j] = (unsigned)run;
+            run += sk[j];
         }
     }
     __syncthreads();
-    const double lscale = log2(nS / m);
-    const double mu = dec->y_mu, sigma = dec->y_sigma;
-    for (int r = 1 + t; r <= HEAVY_MAX + 1; r += DECIDE_THREADS)
-        lpred[r] = use_model ? (float)(mu + sigma * (double)mlp_eval(p, rank_feature((double)r)) + lscale)
-                             : (cnt_at[r] ? (float)(log2((double)cnt_at[r]) + lscale) : -INFINITY);
-    __syncthreads();
-    // k*: the largest rank <= HEAVY_MAX predicted at or above tau_min among the
-    // ranks the sample saw at least CAND_MIN_COUNT times
+    // per rank: the sample count (mean of its bin), the prediction, and the
+    // largest rank <= HEAVY_MAX predicted at or above tau_min among the ranks
+    // the sample saw at least CAND_MIN_COUNT times
     const float ltau = (float)log2(tau_min);
     unsigned last_ok = 0;
-    for (int r = 1 + t; r <= HEAVY_MAX; r += DECIDE_THREADS)
-        if (lpred[r] >= ltau && cnt_at[r] >= (uint32_t)CAND_MIN_COUNT) last_ok = max(last_ok, (unsigned)r);
+    for (int r = 1 + t; r <= EVAL_RANKS; r += DECIDE_THREADS) {
+        uint32_t c = 0;
+        if ((uint64_t)r <= total) {
+            int lo = 0, hi = CC_BINS - 1;  // last j with above[j] < r
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (above[mid] < (unsigned)r) lo = mid;
+                else hi = mid - 1;
+            }
+            c = sk[lo] ? (uint32_t)(sr[lo] / sk[lo]) : 0u;
+        }
+        const float l = use_model ? lpred_model[r] : (c ? (float)(log2((double)c) + lscale) : -INFINITY);
+        lp[r] = l;
+        if (r <= HEAVY_MAX && l >= ltau && c >= (uint32_t)CAND_MIN_COUNT) last_ok = max(last_ok, (unsigned)r);
+    }
     for (int o = 16; o > 0; o >>= 1) last_ok = max(last_ok, __shfl_xor_sync(0xffffffffu, last_ok, o));
     if (lane == 0 && last_ok) atomicMax(&s_kstar, last_ok);
     __syncthreads();
     const unsigned kstar = s_kstar;
+    // predicted mass of ranks 1 .. k*
     double mass = 0.0;
-    for (int r = 1 + t; r <= (int)kstar; r += DECIDE_THREADS) mass += exp2((double)lpred[r]);
-    // the model's mean squared error on the training points
-    const unsigned np = dec->npoints;
-    double loss = 0.0;
-    for (unsigned i = t; i < np; i += DECIDE_THREADS) {
-        const double d = (double)mlp_eval(p, xs[i]) - (double)ys[i];
-        loss += d * d;
+    for (int r = 1 + t; r <= (int)kstar; r += DECIDE_THREADS) mass += exp2((double)lp[r]);
+    // heavy bins: the non-empty bins of count >= CAND_MIN_COUNT whose keys,
+    // with all before them, number <= k* (a prefix of j); j* the last of them
+#pragma unroll
+    for (int q = 0; q < DECIDE_PER; q++) {
+        const int j = t * DECIDE_PER + q;
+        if (j < CC_BINS && kstar && sk[j] && CC_BINS - 1 - j >= CAND_MIN_COUNT && above[j] + sk[j] <= kstar)
+            atomicMax(&s_jstar, (unsigned)j + 1);  // +1: 0 means none
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        mass += __shfl_xor_sync(0xffffffffu, mass, o);
-        loss += __shfl_xor_sync(0xffffffffu, loss, o);
-    }
+    for (int o = 16; o > 0; o >>= 1) mass += __shfl_xor_sync(0xffffffffu, mass, o);
     if (lane == 0) red[w] = mass;
     __syncthreads();
+    const unsigned jst = s_jstar;  // j* + 1, or 0
+    double rows = 0.0;
+#pragma unroll
+    for (int q = 0; q < DECIDE_PER; q++) {
+        const int j = t * DECIDE_PER + q;
+        if (j < CC_BINS && (unsigned)j < jst) rows += (double)sr[j];
+    }
     double pred_mass = 0.0;
     for (int i = 0; i < DECIDE_THREADS / 32; i++) pred_mass += red[i];
     __syncthreads();
-    if (lane == 0) red[w] = loss;
+    for (int o = 16; o > 0; o >>= 1) rows += __shfl_xor_sync(0xffffffffu, rows, o);
+    if (lane == 0) red[w] = rows;
     __syncthreads();
     if (t == 0) {
-        double lsum = 0;
-        for (int i = 0; i < DECIDE_THREADS / 32; i++) lsum += red[i];
-        // count threshold: the lowest bin whose keys, with all above it, number <= k*
-        unsigned above = 0, count_min = 0xFFFFFFFFu, heavy = 0;
-        unsigned long long rows = 0;
-        for (int b = CC_BINS - 1; b >= CAND_MIN_COUNT && kstar; b--) {
-            const unsigned nk = sk[b];
-            if (!nk) continue;
-            if (above + nk > kstar) break;
-            above += nk;
-            rows += sr[b];
-            count_min = cc_bin_min(b);
-            heavy = above;
-        }
+        double srows = 0.0;
+        for (int i = 0; i < DECIDE_THREADS / 32; i++) srows += red[i];
+        const unsigned heavy = jst ? above[jst - 1] + sk[jst - 1] : 0u;
         LrnDecision d = *dec;
         d.k_star = kstar;
-        d.count_min = count_min;
+        d.count_min = jst ? cc_bin_min(CC_BINS - (int)jst) : 0xFFFFFFFFu;
         d.heavy_sample = heavy;
         d.pred_mass = pred_mass;
-        d.sample_mass = (double)rows * (nS / m);
-        d.next_rows = kstar < (unsigned)HEAVY_MAX ? exp2((double)lpred[kstar + 1]) : 0.0;
-        d.loss = np ? (float)(lsum / np) : 0.f;
+        d.sample_mass = srows * rows_scale;
+        d.next_rows = kstar < (unsigned)HEAVY_MAX ? exp2((double)lp[kstar + 1]) : 0.0;
+        d.loss = d.npoints ? (float)(d.loss_sum / d.npoints) : 0.f;
         d.bypass = heavy > 0 && pred_mass >= min_frac * nS ? 1u : 0u;
         *dec = d;
     }
@@ -669,72 +914,90 @@ __global__ void __launch_bounds__(DECIDE_THREADS) k_decide(const float *__restri
 
 cudaError_t launch_decide(const LearnBufs &b, int use_model, double nS, double m, double tau_min, double min_frac,
                           cudaStream_t st) {
-    const size_t smem = (size_t)CC_BINS * 12;
-    cudaError_t e = smem_limit((const void *)k_decide, smem);
+    const double lscale = log2(nS / m);
+    k_model_eval<<<(EVAL_RANKS + CC_BINS + EVAL_THREADS - 1) / EVAL_THREADS, EVAL_THREADS, 0, st>>>(
+        b.params, b.xs, b.ys, lscale, b.lpred, b.dec);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_decide<<<1, DECIDE_THREADS, smem, st>>>(b.params, use_model, b.bin_keys, b.bin_rows, b.xs, b.ys, nS, m, tau_min, min_frac,
-                                 b.dec);
+    const size_t smem = (size_t)CC_BINS * 16;
+    e = smem_limit((const void *)k_decide, smem);
+    if (e != cudaSuccess) return e;
+    k_decide<<<1, DECIDE_THREADS, smem, st>>>(use_model, b.bin_keys, b.bin_rows, b.lpred, nS / m, nS, tau_min,
+                                              min_frac, b.dec);
     count_launch();
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// heavy table: HEAVY_BUCKETS buckets of 4 key slots; key EMPTY_KEY marks a
-// free slot (so EMPTY_KEY itself is never heavy).  A key goes to the first
-// free slot of its bucket, or of the next buckets when that one is full;
-// slots fill in order and are never freed, so a lookup stops at the first
-// bucket with a free slot (at <= 50% load almost always the first).  Slot s
-// = 4 * bucket + i indexes cnt (R rows with the key) and start (first of them
-// in the heavy R payload list, materialisation).
+// heavy table: two tables of HEAVY_BKT buckets of 2 key slots; key EMPTY_KEY
+// marks a free slot (so EMPTY_KEY itself is never heavy).  Key k lives in
+// bucket heavy_b1(k) of the first table (slots 0 .. HEAVY_CAP / 2) or in
+// bucket heavy_b2(k) of the second; slot s indexes cnt (R rows with the key),
+// scnt (S rows, counting joins) and start (first of the key's R rows in the
+// heavy R payload list, materialisation).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t heavy_bucket(uint32_t k) { return (k * 0x9E3779B1u) >> (32 - HEAVY_LOG2 + 2); }
-__device__ __forceinline__ uint32_t filter_bit(uint32_t k) { return (k * 0x85EBCA6Bu) >> (32 - FILTER_LOG2); }
-
-__device__ __forceinline__ int heavy_find(const uint32_t *keys, uint32_t k) {
-    if (k == EMPTY_KEY) return -1;
-    uint32_t b = heavy_bucket(k);
-    for (int probe = 0; probe < HEAVY_BUCKETS; probe++) {
-        const uint4 q = reinterpret_cast<const uint4 *>(keys)[b];
-        const int i = q.x == k ? 0 : q.y == k ? 1 : q.z == k ? 2 : q.w == k ? 3 : -1;
-        if (i >= 0) return (int)(4 * b) + i;
-        if (q.w == EMPTY_KEY) return -1;  // slots fill in order: a free last slot ends the search
-        b = (b + 1) & (HEAVY_BUCKETS - 1);
-    }
-    return -1;
+__device__ __forceinline__ uint32_t heavy_b1(uint32_t k) { return (k * 0x9E3779B1u) >> (32 - HEAVY_BKT_LOG2); }
+__device__ __forceinline__ uint32_t heavy_b2(uint32_t k) {
+    return HEAVY_BKT + (((k ^ (k >> 15)) * 0x85EBCA6Bu) >> (32 - HEAVY_BKT_LOG2));
 }
 
-__device__ __forceinline__ void heavy_insert(uint32_t *keys, uint32_t k) {
-    uint32_t b = heavy_bucket(k);
-    for (int probe = 0; probe < HEAVY_BUCKETS; probe++) {
-        for (int i = 0; i < 4; i++) {
-            const uint32_t old = atomicCAS(&keys[4 * b + i], EMPTY_KEY, k);
-            if (old == EMPTY_KEY || old == k) return;
-        }
-        b = (b + 1) & (HEAVY_BUCKETS - 1);
+// Slot of key k, or -1: both buckets are read and compared without branches.
+__device__ __forceinline__ int heavy_lookup(const uint32_t *keys, uint32_t k) {
+    const uint32_t b1 = heavy_b1(k), b2 = heavy_b2(k);
+    const uint2 x = reinterpret_cast<const uint2 *>(keys)[b1];
+    const uint2 y = reinterpret_cast<const uint2 *>(keys)[b2];
+    int s = -1;
+    s = y.y == k ? (int)(2 * b2 + 1) : s;
+    s = y.x == k ? (int)(2 * b2) : s;
+    s = x.y == k ? (int)(2 * b1 + 1) : s;
+    s = x.x == k ? (int)(2 * b1) : s;
+    return k == EMPTY_KEY ? -1 : s;
+}
+
+// Inserts k (a key not in the table) by cuckoo displacement: a free slot of
+// the key's bucket in the current table, else the key takes a slot whose
+// key moves on to its bucket in the other table.  Many threads insert at
+// once (atomics only).  Returns false when the walk gave up; the key it
+// then holds (k or a displaced one) is left out of the table, which only
+// makes that key light.
+__device__ bool heavy_insert(uint32_t *keys, uint32_t k) {
+    uint32_t cur = k;
+    int t = 0;
+    for (int it = 0; it < 128; it++) {
+        const uint32_t b = t ? heavy_b2(cur) : heavy_b1(cur);
+        uint32_t *s = keys + 2 * b;
+        if (atomicCAS(&s[0], EMPTY_KEY, cur) == EMPTY_KEY) return true;
+        if (atomicCAS(&s[1], EMPTY_KEY, cur) == EMPTY_KEY) return true;
+        const uint32_t old = atomicExch(&s[(it >> 1) & 1], cur);
+        if (old == EMPTY_KEY) return true;
+        cur = old;  // it sat in bucket b of table t: its other bucket is in table t ^ 1
+        t ^= 1;
     }
+    return false;
 }
 
 // Inserts the candidates whose sample count reaches the decision's
 // count_min (at most HEAVY_MAX of them; the decision keeps their number at
-// or below k* <= HEAVY_MAX) and sets their filter bits.
+// or below k* <= HEAVY_MAX); `inserted` ends as the number of keys placed.
 __global__ void k_heavy_build(const HeavyCand *__restrict__ cand, unsigned cand_cap, const LrnDecision *dec,
-                              uint32_t *keys, uint32_t *filter, unsigned *inserted) {
+                              uint32_t *keys, unsigned *inserted) {
     const unsigned n = min(dec->ncand, cand_cap);
     const unsigned cmin = dec->count_min;
     if (!dec->bypass) return;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HeavyCand c = cand[i];
         if (c.count < cmin || c.key == EMPTY_KEY) continue;
-        if (atomicAdd(inserted, 1u) >= (unsigned)HEAVY_MAX) continue;
-        const uint32_t fb = filter_bit(c.key);
-        atomicOr(&filter[fb >> 5], 1u << (fb & 31));
-        heavy_insert(keys, c.key);
+        if (atomicAdd(inserted, 1u) >= (unsigned)HEAVY_MAX) {
+            atomicSub(inserted, 1u);
+            continue;
+        }
+        if (!heavy_insert(keys, c.key)) atomicSub(inserted, 1u);
     }
 }
 
-cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, uint32_t *filter, unsigned *inserted,
-                               cudaStream_t st) {
-    k_heavy_build<<<148 * 2, 256, 0, st>>>(b.cand, b.cand_cap, b.dec, keys, filter, inserted);
+cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, unsigned *inserted, cudaStream_t st) {
+    k_heavy_build<<<148 * 2, 256, 0, st>>>(b.cand, b.cand_cap, b.dec, keys, inserted);
     count_launch();
     return cudaGetLastError();
 }
@@ -744,17 +1007,15 @@ cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, uint32_t *fil
 // cur[] the fill cursors).
 template <int PASS>
 __global__ void __launch_bounds__(512) k_heavy_r(const Row *__restrict__ R, uint64_t n, const uint32_t *__restrict__ gkeys,
-                                                 const uint32_t *__restrict__ gfilter, unsigned *gcnt,
-                                                 const unsigned *__restrict__ start, unsigned *cur, uint32_t *rpay) {
+                                                 unsigned *gcnt, const unsigned *__restrict__ start, unsigned *cur,
+                                                 uint32_t *rpay) {
     extern __shared__ __align__(16) unsigned char smem_hr[];
     uint32_t *keys = reinterpret_cast<uint32_t *>(smem_hr);
     unsigned *cnt = keys + HEAVY_CAP;
-    uint32_t *filt = cnt + HEAVY_CAP;
     for (int i = threadIdx.x; i < HEAVY_CAP; i += 512) {
         keys[i] = gkeys[i];
         cnt[i] = 0;
     }
-    for (int i = threadIdx.x; i < (1 << FILTER_LOG2) / 32; i += 512) filt[i] = gfilter[i];
     __syncthreads();
     // four rows in flight per thread
     const uint64_t stride = (uint64_t)gridDim.x * 512;
@@ -763,6 +1024,7 @@ __global__ void __launch_bounds__(512) k_heavy_r(const Row *__restrict__ R, uint
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const uint64_t i = i0 + u * stride;
+            x[u] = Row{EMPTY_KEY, 0};
             if (i < n) {
                 const uint2 v = ldg_stream(reinterpret_cast<const uint2 *>(R) + i);
                 x[u] = Row{v.x, v.y};
@@ -770,10 +1032,7 @@ __global__ void __launch_bounds__(512) k_heavy_r(const Row *__restrict__ R, uint
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            if (i0 + u * stride >= n) continue;
-            const uint32_t fb = filter_bit(x[u].key);
-            if (!(filt[fb >> 5] >> (fb & 31) & 1)) continue;
-            const int s = heavy_find(keys, x[u].key);
+            const int s = heavy_lookup(keys, x[u].key);  // the padding key EMPTY_KEY is never heavy
             if (s < 0) continue;
             if (PASS == 0) atomicAdd(&cnt[s], 1u);
             else rpay[start[s] + atomicAdd(&cur[s], 1u)] = x[u].payload;
@@ -804,20 +1063,20 @@ __global__ void k_heavy_prefix(const unsigned *cnt, unsigned *start, unsigned *c
 
 // stage 0: per-slot counts of R's heavy rows; stage 1 (materialisation):
 // prefix of the counts, then every heavy row's payload into rpay.
-cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const uint32_t *filter, unsigned *cnt,
-                           unsigned *start, unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st) {
+cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, unsigned *cnt, unsigned *start,
+                           unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st) {
     if (!n) return cudaSuccess;
     const unsigned g = (unsigned)umin64((n + 511) / 512, (uint64_t)nsm * 4);
-    const size_t smem = (size_t)HEAVY_CAP * 8 + (1 << FILTER_LOG2) / 8;
+    const size_t smem = (size_t)HEAVY_CAP * 8;
     cudaError_t e = smem_limit((const void *)k_heavy_r<0>, smem);
     if (e == cudaSuccess) e = smem_limit((const void *)k_heavy_r<1>, smem);
     if (e != cudaSuccess) return e;
     if (stage == 0) {
-        k_heavy_r<0><<<g, 512, smem, st>>>(R, n, keys, filter, cnt, nullptr, nullptr, nullptr);
+        k_heavy_r<0><<<g, 512, smem, st>>>(R, n, keys, cnt, nullptr, nullptr, nullptr);
         count_launch();
     } else {
         k_heavy_prefix<<<1, 1024, 0, st>>>(cnt, start, cur);
-        k_heavy_r<1><<<g, 512, smem, st>>>(R, n, keys, filter, cnt, start, cur, rpay);
+        k_heavy_r<1><<<g, 512, smem, st>>>(R, n, keys, cnt, start, cur, rpay);
         count_launch(2);
     }
     return cudaGetLastError();
@@ -829,21 +1088,13 @@ cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const
 // rows out), every other row is counted in its radix bin and appended to
 // the chunk's region of the compacted S (warp-aggregated, coalesced).
 // ---------------------------------------------------------------------------
-// Heavy check of one row against the filter and the table in shared memory:
-// the row's slot, or -1.
-__device__ __forceinline__ int heavy_slot(const uint32_t *filt, const uint32_t *hkeys, uint32_t k) {
-    const uint32_t fb = filter_bit(k);
-    if (!((filt[fb >> 5] >> (fb & 31)) & 1u)) return -1;
-    return heavy_find(hkeys, k);
-}
-
 // One row outside the vector body (the chunk's first row when it starts 8
 // bytes past a 16-byte boundary, or its last row): thread 0 only.
 template <bool MAT>
-__device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *filt, const uint32_t *hkeys,
-                                unsigned *hcnt, uint32_t *hist, unsigned *s_keep, uint2 *dst, Row x,
-                                unsigned long long &matches, unsigned long long &heavy_rows) {
-    const int s = heavy_slot(filt, hkeys, x.key);
+__device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *hkeys, unsigned *hcnt, uint32_t *hist,
+                                unsigned *s_keep, uint2 *dst, Row x, unsigned long long &matches,
+                                unsigned &heavy_rows) {
+    const int s = heavy_lookup(hkeys, x.key);
     if (s < 0) {
         atomicAdd(&hist[radix_f(a.rf, x.key)], 1u);
         dst[atomicAdd(s_keep, 1u)] = make_uint2(x.key, x.payload);
@@ -869,19 +1120,22 @@ __device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *filt, const
 // heavy slot instead (added to a.scnt at the end): the join's heavy matches
 // are sum_slot S rows x R rows, formed after R's heavy rows are counted on
 // the other stream (k_heavy_sum), so that count is off this kernel's path.
+// The next round's rows are loaded before the current round is processed
+// (one round of loads always in flight per thread).
+constexpr int BYP_THREADS = 1024;
+constexpr int BYP_U = 4;  // 16-byte row pairs per thread per round
+
 template <bool MAT>
-__global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
+__global__ void __launch_bounds__(BYP_THREADS, 1) k_hist_bypass(BypassArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t *hkeys = reinterpret_cast<uint32_t *>(smem);  // 16-byte aligned buckets
+    uint32_t *hkeys = reinterpret_cast<uint32_t *>(smem);  // 8-byte aligned buckets
     unsigned *hcnt = hkeys + HEAVY_CAP;
-    uint32_t *filt = hcnt + HEAVY_CAP;                     // 2^FILTER_LOG2 bits
-    uint32_t *hist = filt + (1 << FILTER_LOG2) / 32;
+    uint32_t *hist = hcnt + HEAVY_CAP;
     __shared__ unsigned s_keep;
-    __shared__ uint64_t scan_scratch[1024 / 32 + 1];
+    __shared__ uint64_t scan_scratch[BYP_THREADS / 32 + 1];
     const int tid = threadIdx.x, lane = tid & 31;
-    for (int i = tid; i < a.nbins; i += 1024) hist[i] = 0;
-    for (int i = tid; i < (1 << FILTER_LOG2) / 32; i += 1024) filt[i] = a.filter[i];
-    for (int i = tid; i < HEAVY_CAP; i += 1024) {
+    for (int i = tid; i < a.nbins; i += BYP_THREADS) hist[i] = 0;
+    for (int i = tid; i < HEAVY_CAP; i += BYP_THREADS) {
         hkeys[i] = a.hkeys[i];
         hcnt[i] = MAT ? a.hcnt[i] : 0u;
     }
@@ -896,48 +1150,54 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     const uint32_t npairs = (len - head) / 2;
     const bool tail = ((len - head) & 1) != 0;
     const uint4 *v = reinterpret_cast<const uint4 *>(src + head);
-    unsigned long long matches = 0, heavy_rows = 0;
-    // rounds of 4 row pairs per thread: pair p = base + u * 1024 + tid
-    for (uint32_t base = 0; base < npairs; base += 4 * 1024) {
-        uint32_t k[8], pv[8];
+    unsigned long long matches = 0;
+    unsigned heavy_rows = 0;
+    constexpr uint32_t ROUND = BYP_U * BYP_THREADS;
+    // counting: the next round's loads go out before this round's work;
+    // materialising (more live state for the pair output) loads each round
+    constexpr bool PREFETCH = !MAT;
+    uint4 nx[BYP_U];
+    auto load_round = [&](uint32_t base) {
+#pragma unroll
+        for (int u = 0; u < BYP_U; u++) {
+            const uint32_t p = base + u * BYP_THREADS + tid;
+            nx[u] = p < npairs ? ldg_stream(v + p) : make_uint4(EMPTY_KEY, 0, EMPTY_KEY, 0);
+        }
+    };
+    if (PREFETCH) load_round(0);
+    // rounds of BYP_U row pairs per thread: pair p = base + u * BYP_THREADS + tid
+    for (uint32_t base = 0; base < npairs; base += ROUND) {
+        if (!PREFETCH) load_round(base);
+        uint32_t k[2 * BYP_U], pv[2 * BYP_U];
         unsigned valid = 0;
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const uint32_t p = base + u * 1024 + tid;
-            k[2 * u] = k[2 * u + 1] = EMPTY_KEY;
-            pv[2 * u] = pv[2 * u + 1] = 0;
-            if (p < npairs) {
-                const uint4 x = ldg_stream(v + p);
-                k[2 * u] = x.x;
-                pv[2 * u] = x.y;
-                k[2 * u + 1] = x.z;
-                pv[2 * u + 1] = x.w;
-                valid |= 3u << (2 * u);
-            }
+        for (int u = 0; u < BYP_U; u++) {
+            k[2 * u] = nx[u].x;
+            pv[2 * u] = nx[u].y;
+            k[2 * u + 1] = nx[u].z;
+            pv[2 * u + 1] = nx[u].w;
+            if (base + u * BYP_THREADS + tid < npairs) valid |= 3u << (2 * u);
         }
-        int slot[8];
+        if (PREFETCH) load_round(base + ROUND);
+        int slot[2 * BYP_U];
+        unsigned hm = 0;
 #pragma unroll
-        for (int j = 0; j < 8; j++) slot[j] = (valid >> j & 1) ? heavy_slot(filt, hkeys, k[j]) : -1;
-        unsigned keep = 0;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            if (slot[j] >= 0) {
-                if (MAT) matches += hcnt[slot[j]];
-                heavy_rows++;
-            } else if (valid >> j & 1) {
-                keep |= 1u << j;
-            }
+        for (int j = 0; j < 2 * BYP_U; j++) {
+            slot[j] = heavy_lookup(hkeys, k[j]);
+            hm |= (slot[j] >= 0 && (valid >> j & 1)) ? 1u << j : 0u;
         }
+        const unsigned km = valid & ~hm;  // rows that go on to the partitions
+        heavy_rows += __popc(hm);
         if (!MAT) {  // S rows per heavy slot; a warp's rows of one hot key add once
-            const bool dup = warp_has_dups((uint32_t)slot[0], slot[0] >= 0);
+            const bool dup = warp_has_dups((uint32_t)slot[0], hm & 1u);
 #pragma unroll
-            for (int j = 0; j < 8; j++) hist_add_warp(hcnt, slot[j] >= 0 ? (uint32_t)slot[j] : 0u, slot[j] >= 0, dup);
+            for (int j = 0; j < 2 * BYP_U; j++) hist_add_warp(hcnt, (uint32_t)slot[j], hm >> j & 1, dup);
         }
         // coalesced compaction: one ballot per row slot, one shared atomic per warp
-        unsigned m[8], wtot = 0;
+        unsigned m[2 * BYP_U], wtot = 0;
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            m[j] = __ballot_sync(0xffffffffu, keep >> j & 1);
+        for (int j = 0; j < 2 * BYP_U; j++) {
+            m[j] = __ballot_sync(0xffffffffu, km >> j & 1);
             wtot += __popc(m[j]);
         }
         unsigned wb = 0;
@@ -945,8 +1205,8 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
         wb = __shfl_sync(0xffffffffu, wb, 0);
         const unsigned lt = lanemask_lt();
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            if (keep >> j & 1) {
+        for (int j = 0; j < 2 * BYP_U; j++) {
+            if (km >> j & 1) {
                 atomicAdd(&hist[radix_f(a.rf, k[j])], 1u);
                 dst[wb + __popc(m[j] & lt)] = make_uint2(k[j], pv[j]);
             }
@@ -954,13 +1214,15 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
         }
         if (MAT) {
             // heavy rows' output in (row slot, lane) order: coalesced stores
-            uint32_t c[8];
+            uint32_t c[2 * BYP_U];
 #pragma unroll
-            for (int j = 0; j < 8; j++) c[j] = slot[j] >= 0 ? hcnt[slot[j]] : 0;
-            uint64_t pos[8];
-            block_emit_positions<1024, 8>(c, pos, a.rows_ctr, scan_scratch);
+            for (int j = 0; j < 2 * BYP_U; j++) c[j] = (hm >> j & 1) ? hcnt[slot[j]] : 0;
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
+            for (int j = 0; j < 2 * BYP_U; j++) matches += c[j];
+            uint64_t pos[2 * BYP_U];
+            block_emit_positions<BYP_THREADS, 2 * BYP_U>(c, pos, a.rows_ctr, scan_scratch);
+#pragma unroll
+            for (int j = 0; j < 2 * BYP_U; j++) {
                 if (c[j]) {
                     // R-row starts stay in global memory: only heavy rows read them
                     const unsigned st0 = a.hstart[slot[j]];
@@ -973,17 +1235,17 @@ __global__ void __launch_bounds__(1024) k_hist_bypass(BypassArgs a) {
     }
     __syncthreads();  // every vector row is counted: the edge rows take the next output slots
     if (tid == 0) {
-        if (head) bypass_edge_row<MAT>(a, filt, hkeys, hcnt, hist, &s_keep, dst, src[0], matches, heavy_rows);
-        if (tail) bypass_edge_row<MAT>(a, filt, hkeys, hcnt, hist, &s_keep, dst, src[len - 1], matches, heavy_rows);
+        if (head) bypass_edge_row<MAT>(a, hkeys, hcnt, hist, &s_keep, dst, src[0], matches, heavy_rows);
+        if (tail) bypass_edge_row<MAT>(a, hkeys, hcnt, hist, &s_keep, dst, src[len - 1], matches, heavy_rows);
     }
     __syncthreads();
     uint32_t *hdst = a.hist + (uint64_t)blockIdx.x * a.nbins;
-    for (int i = tid; i < a.nbins; i += 1024) hdst[i] = hist[i];
+    for (int i = tid; i < a.nbins; i += BYP_THREADS) hdst[i] = hist[i];
     if (!MAT)
-        for (int i = tid; i < HEAVY_CAP; i += 1024)
+        for (int i = tid; i < HEAVY_CAP; i += BYP_THREADS)
             if (hcnt[i]) atomicAdd(&a.scnt[i], hcnt[i]);
     if (tid == 0) a.kept[blockIdx.x] = s_keep;
-    const unsigned long long wm = warp_sum_u64(matches), wh = warp_sum_u64(heavy_rows);
+    const unsigned long long wm = warp_sum_u64(matches), wh = warp_sum_u64((unsigned long long)heavy_rows);
     if (lane == 0) {
         if (wm) atomicAdd(a.matches, wm);
         if (wh) atomicAdd(a.heavy_rows, wh);
@@ -1007,8 +1269,8 @@ cudaError_t launch_heavy_sum(const unsigned *rcnt, const unsigned *scnt, unsigne
 }
 
 size_t bypass_smem(int nbins, bool mat) {
-    (void)mat;  // heavy keys + counts + filter + 2^15 bins: 204,800 B at most
-    return (size_t)HEAVY_CAP * 4 * 2 + (1 << FILTER_LOG2) / 8 + (size_t)nbins * 4;
+    (void)mat;  // heavy keys + counts + 2^15 bins: 196,608 B at most
+    return (size_t)HEAVY_CAP * 4 * 2 + (size_t)nbins * 4;
 }
 
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st) {
@@ -1016,9 +1278,10 @@ cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st) {
     auto kern = mat ? k_hist_bypass<true> : k_hist_bypass<false>;
     cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
-    kern<<<a.G, 1024, smem, st>>>(a);
+    kern<<<a.G, BYP_THREADS, smem, st>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
 }  // namespace tbg
+

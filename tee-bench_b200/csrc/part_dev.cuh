@@ -88,6 +88,11 @@ constexpr int PART_NBUF = 3;
 #define TBG_BULK_STORE 0
 #endif
 constexpr bool PART_BULK = TBG_BULK_STORE != 0;
+// A third barrier at the end of every tile (the layout before the tile loop
+// was shown not to need it; kept as a build option for A/B timing).
+#ifndef TBG_TILE_END_BARRIER
+#define TBG_TILE_END_BARRIER 0
+#endif
 constexpr int PART_PAD = PART_BULK ? SCATTER_FMAX : 0;  // spare slots per staged tile
 
 template <int THREADS, int NBUF = PART_NBUF>
@@ -228,6 +233,7 @@ __device__ __forceinline__ void tile_scan(uint32_t q, int F, PartSmem<THREADS, N
     uint32_t sum = 0;
 #pragma unroll
     for (int i = 0; i < PER; i++) sum += x[i];
+    if (PART_BULK) sum += PER;  // the lane's digits take one spare slot each
     uint32_t inc = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -350,7 +356,7 @@ __device__ __forceinline__ TileGeo range_tile(const Row *in, uint64_t lo, uint64
 }
 
 // Scatters rows [lo, hi) of `in` (in_n rows), digit by digit, to out[sm.cursor[d]...];
-// the caller initialises sm.cursor[0..F) and synchronises.  Three barriers
+// the caller initialises sm.cursor[0..F) and synchronises.  Two barriers
 // per tile; the bulk copies run NB - 1 tiles ahead.  `kseq` is the CTA's
 // running tile count (see above), and the barriers mbar[0..NB) are
 // initialised once by the caller.
@@ -385,9 +391,14 @@ __device__ void part_tiles(const Row *__restrict__ in, uint64_t lo, uint64_t hi,
                        &mbar[(q + NB - 1) % NB]);
         if (g.cnt == T) tile_stage<THREADS, true, Dig>(g, q, dop, sm, v, rank);
         else tile_stage<THREADS, false, Dig>(g, q, dop, sm, v, rank);
-        __syncthreads();
+        // No barrier here: tile q + 1's load and ranking touch neither tile
+        // q's buffer nor its counters, and the next iteration's first barrier
+        // orders this staging before tile q's write-out and before the scan
+        // that clears cnt[q & 1].
+        if (TBG_TILE_END_BARRIER) __syncthreads();
         prev_cnt = g.cnt;
     }
+    __syncthreads();  // the last tile is staged
     tile_write<THREADS, Dig>(kseq + ntiles - 1, prev_cnt, o, out_n, dop, sm, 0, err);
     if (PART_BULK) bulk_wait_all();  // this thread's bulk stores have landed
     __syncthreads();  // every buffer is free again

@@ -21,13 +21,17 @@ constexpr int MLP_SLICE = 152;        // parameters updated by each CTA
 static_assert(MLP_PARAMS <= MLP_PARAMS_PAD, "parameter stride");
 static_assert(MLP_SLICE * MLP_CLUSTER >= MLP_PARAMS, "every parameter belongs to a slice");
 
-// Heavy-key table: HEAVY_CAP slots in buckets of 4 (one 16-byte load).
+// Heavy-key table: two tables of HEAVY_BKT buckets of 2 key slots (one
+// 8-byte load each); a key lives in its bucket of the first table or in its
+// bucket of the second (two-choice cuckoo hashing), so a lookup is two loads
+// and four compares, without branches.  Slot s (0 .. HEAVY_CAP) indexes the
+// per-key arrays (R rows, S rows, payload list starts).
 constexpr int HEAVY_LOG2 = 13;
 constexpr int HEAVY_CAP = 1 << HEAVY_LOG2;
-constexpr int HEAVY_BUCKETS = HEAVY_CAP / 4;
-constexpr int HEAVY_MAX = HEAVY_CAP / 2;  // at most half full
+constexpr int HEAVY_BKT_LOG2 = HEAVY_LOG2 - 2;
+constexpr int HEAVY_BKT = 1 << HEAVY_BKT_LOG2;  // buckets per table
+constexpr int HEAVY_MAX = HEAVY_CAP / 2;        // at most half full
 constexpr uint32_t EMPTY_KEY = 0xFFFFFFFFu;
-constexpr int FILTER_LOG2 = 16;  // bit filter in front of the heavy table (8 KB)
 
 #ifdef __CUDACC__
 #define TBG_HD __host__ __device__
@@ -72,6 +76,7 @@ struct LrnDecision {
     float loss;               // mean squared error of the model on the (normalised) points
     float y_mu, y_sigma;      // the points' targets are (log2(count) - y_mu) / y_sigma
     unsigned pad;
+    double loss_sum;          // squared error of the model summed over the points
 };
 
 struct BypassArgs {
@@ -84,7 +89,6 @@ struct BypassArgs {
     Row *out;             // compacted S: chunk c's kept rows at [c * chunk, c * chunk + kept[c])
     uint32_t *hist;       // [G][nbins]
     uint32_t *kept;       // [G]
-    const uint32_t *filter;
     const uint32_t *hkeys;
     const unsigned *hcnt;       // materialising: R rows per heavy slot
     unsigned *scnt;             // counting: S rows per heavy slot (added to)
@@ -107,7 +111,7 @@ cudaError_t launch_mlp_train(const float *xs, const float *ys, const float *cw, 
 // Learning stage of LRN (all on the device, learned.cu).
 struct LearnBufs {
     uint32_t *keys;             // sample keys [m]
-    uint32_t *tkeys, *tcnt;     // global count table [slots]
+    unsigned long long *table;  // global count table [slots]: key << 32 | count
     uint32_t tmask;             // slots - 1
     unsigned *bin_keys;         // [CC_BINS]
     unsigned long long *bin_rows;  // [CC_BINS]
@@ -115,6 +119,7 @@ struct LearnBufs {
     unsigned cand_cap;
     float *xs, *ys;             // training points [CC_BINS]
     float *cw;                  // their cumulative sampling weights [CC_BINS]
+    float *lpred;               // log2 predicted S rows of ranks 0 .. HEAVY_MAX + 1 (entry 0 unused)
     float *params;              // MLP parameters
     LrnDecision *dec;
     unsigned *err;
@@ -126,9 +131,8 @@ cudaError_t launch_count_stats(const LearnBufs &b, cudaStream_t st);
 cudaError_t launch_rank_points(const LearnBufs &b, cudaStream_t st);
 cudaError_t launch_decide(const LearnBufs &b, int use_model, double nS, double m, double tau_min, double min_frac,
                           cudaStream_t st);
-cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, uint32_t *filter, unsigned *inserted,
-                               cudaStream_t st);
-cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, const uint32_t *filter, unsigned *cnt,
+cudaError_t launch_heavy_build(const LearnBufs &b, uint32_t *keys, unsigned *inserted, cudaStream_t st);
+cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, unsigned *cnt,
                            unsigned *start, unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st);
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st);
 cudaError_t launch_heavy_sum(const unsigned *rcnt, const unsigned *scnt, unsigned long long *matches, cudaStream_t st);

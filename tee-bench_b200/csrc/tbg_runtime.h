@@ -69,7 +69,6 @@ int finish_join(const tbg_config &cfg, Workspace &w, cudaStream_t st, const Join
 
 // Heavy-key table used by the S histogram of the learned path (device pointers).
 struct SBypass {
-    const uint32_t *filter;
     const uint32_t *keys;
     const unsigned *cnt;
     unsigned *scnt;
