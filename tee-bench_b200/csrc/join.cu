@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     t.layout = a.layout;
     t.hcap = floor_pow2((uint32_t)a.capR + 2);
     const int tid = threadIdx.x;
-    const unsigned nitems = *a.nitems;
+    const unsigned nitems = *a.err ? 0u : *a.nitems;  // a planner error leaves the item list unusable
     unsigned long long local = 0;
 
     // an item is claimed one step ahead, and its R rows are prefetched into

@@ -30,6 +30,16 @@
 namespace tbg {
 
 static constexpr double kMinHeavyFraction = 0.05;
+
+// 0 (default): R's partitioning is queued before the learning stage's
+// kernels; 1: after them.  Measured at |R| = 2^26, |S| = 2^29, z = 1: 5.41 -
+// 5.49 ms against 5.65 ms.  Queued first, the learning stage ends sooner
+// (0.68 against 0.79 - 0.88 ms) but pushes R's partitioning into S's
+// bandwidth-bound phase; queued after, R's passes use the bandwidth the
+// latency-bound learning kernels leave idle.  A build option for A/B timing.
+#ifndef TBG_LRN_LEARN_FIRST
+#define TBG_LRN_LEARN_FIRST 0
+#endif
 static constexpr unsigned kCandCap = 1u << 20;
 
 int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
@@ -85,6 +95,13 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 5 + 16);
 #undef ENSURE
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
+    // main stream: R's partitioning needs nothing from the model
+    auto partition_r = [&]() -> int {
+        int r;
+        if ((r = part_histogram(0, g, dR, cfg, w, st, nullptr))) return r;
+        if ((r = part_pass(0, 1, g, dR, w, st, false))) return r;
+        return part_pass(0, 2, g, dR, w, st, false);
+    };
     LearnBufs lb;
     lb.keys = w.aux[0].as<uint32_t>();
     lb.table = w.aux[1].as<unsigned long long>();
@@ -105,15 +122,14 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     unsigned *hinserted = hcur + HEAVY_CAP;
     unsigned *hscnt = hinserted + 4;  // S rows per heavy slot (counting joins)
 
-    // main stream: R's partitioning needs nothing from the model
     if (timing) cudaEventRecord(w.ev[0], st);
     if ((e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st)) != cudaSuccess) return cuda_error(e, "memset");
     if ((e = cudaEventRecord(w.fork, st)) != cudaSuccess) return cuda_error(e, "event");
-    if ((rc = part_histogram(0, g, dR, cfg, w, st, nullptr))) return rc;
-    if ((rc = part_pass(0, 1, g, dR, w, st, false))) return rc;
-    if ((rc = part_pass(0, 2, g, dR, w, st, false))) return rc;
+    if (!TBG_LRN_LEARN_FIRST && (rc = partition_r()))
+        return rc;
 
-    // side stream: learn the heavy keys meanwhile
+    // side stream: learn the heavy keys (on the high-priority stream, while
+    // R is partitioned)
     if ((e = cudaStreamWaitEvent(s2, w.fork, 0)) != cudaSuccess) return cuda_error(e, "event");
     if ((e = cudaMemsetAsync(lb.table, 0xFF, (size_t)tslots * 8, s2)) != cudaSuccess ||
         (e = cudaMemsetAsync(lb.bin_rows, 0, (size_t)CC_BINS * 12, s2)) != cudaSuccess ||
@@ -133,9 +149,10 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
         (e = launch_decide(lb, use_model, (double)nS, (double)m, tau_min, kMinHeavyFraction, s2)) != cudaSuccess)
         return cuda_error(e, "learning stage");
     LrnDecision *hd = static_cast<LrnDecision *>(w.host_small);
-    if ((e = cudaMemcpyAsync(hd, lb.dec, sizeof(LrnDecision), cudaMemcpyDeviceToHost, s2)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(s2)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(hd, lb.dec, sizeof(LrnDecision), cudaMemcpyDeviceToHost, s2)) != cudaSuccess)
         return cuda_error(e, "learning stage");
+    if (TBG_LRN_LEARN_FIRST && (rc = partition_r())) return rc;
+    if ((e = cudaStreamSynchronize(s2)) != cudaSuccess) return cuda_error(e, "learning stage");
     const LrnDecision dec = *hd;
     run->train_steps = steps;
     run->train_loss = dec.loss;

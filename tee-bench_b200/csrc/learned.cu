@@ -481,9 +481,9 @@ __device__ __forceinline__ void table_add(unsigned long long *t, uint32_t tmask,
 __global__ void __launch_bounds__(CNT_THREADS, 2) k_count_keys(const uint32_t *__restrict__ keys, uint64_t m,
                                                            unsigned long long *table, uint32_t tmask) {
     constexpr int SLOTS = 2 * CNT_CHUNK;
-    constexpr int PER = SLOTS / CNT_THREADS;
-    __shared__ uint32_t lk[SLOTS];
-    __shared__ uint32_t lc[SLOTS];
+    constexpr int PER = 4;  // flush: slots per thread per batch of compare-and-swaps
+    extern __shared__ __align__(16) uint32_t cnt_smem[];
+    uint32_t *lk = cnt_smem, *lc = cnt_smem + SLOTS;
     for (int i = threadIdx.x; i < SLOTS; i += CNT_THREADS) {
         lk[i] = EMPTY_KEY;
         lc[i] = 0;
@@ -509,29 +509,33 @@ __global__ void __launch_bounds__(CNT_THREADS, 2) k_count_keys(const uint32_t *_
         }
     }
     __syncthreads();
-    uint32_t fk[PER], fc[PER], fh[PER];
-    unsigned long long old[PER];
+    for (int base = 0; base < SLOTS; base += PER * CNT_THREADS) {
+        uint32_t fk[PER];
+        unsigned long long old[PER];
 #pragma unroll
-    for (int q = 0; q < PER; q++) {
-        const int i = q * CNT_THREADS + threadIdx.x;
-        fk[q] = lk[i];
-        fc[q] = lc[i];
-        fh[q] = count_hash(fk[q]) & tmask;
-    }
+        for (int q = 0; q < PER; q++) {  // independent: the compare-and-swaps are all in flight at once
+            const int i = base + q * CNT_THREADS + threadIdx.x;
+            fk[q] = lk[i];
+            old[q] = fk[q] != EMPTY_KEY
+                         ? atomicCAS(&table[count_hash(fk[q]) & tmask], CNT_EMPTY, cnt_word(fk[q], lc[i]))
+                         : CNT_EMPTY;
+        }
 #pragma unroll
-    for (int q = 0; q < PER; q++)  // independent: the compare-and-swaps are all in flight at once
-        old[q] = fk[q] != EMPTY_KEY ? atomicCAS(&table[fh[q]], CNT_EMPTY, cnt_word(fk[q], fc[q])) : CNT_EMPTY;
-#pragma unroll
-    for (int q = 0; q < PER; q++) {
-        if (fk[q] == EMPTY_KEY || old[q] == CNT_EMPTY) continue;
-        if ((uint32_t)(old[q] >> 32) == fk[q]) atomicAdd(&table[fh[q]], (unsigned long long)fc[q]);
-        else table_add(table, tmask, fk[q], fc[q], (fh[q] + 1) & tmask);
+        for (int q = 0; q < PER; q++) {
+            if (fk[q] == EMPTY_KEY || old[q] == CNT_EMPTY) continue;
+            const uint32_t h = count_hash(fk[q]) & tmask, c = lc[base + q * CNT_THREADS + threadIdx.x];
+            if ((uint32_t)(old[q] >> 32) == fk[q]) atomicAdd(&table[h], (unsigned long long)c);
+            else table_add(table, tmask, fk[q], c, (h + 1) & tmask);
+        }
     }
 }
 
 cudaError_t launch_count_keys(const LearnBufs &b, uint64_t m, cudaStream_t st) {
     if (!m) return cudaSuccess;
-    k_count_keys<<<(unsigned)((m + CNT_CHUNK - 1) / CNT_CHUNK), CNT_THREADS, 0, st>>>(b.keys, m, b.table, b.tmask);
+    const size_t smem = (size_t)CNT_CHUNK * 2 * 8;
+    cudaError_t e = smem_limit((const void *)k_count_keys, smem);
+    if (e != cudaSuccess) return e;
+    k_count_keys<<<(unsigned)((m + CNT_CHUNK - 1) / CNT_CHUNK), CNT_THREADS, smem, st>>>(b.keys, m, b.table, b.tmask);
     count_launch();
     return cudaGetLastError();
 }
@@ -584,24 +588,42 @@ __global__ void __launch_bounds__(STATS_THREADS, 2) k_count_stats(const unsigned
         const ulonglong2 c = reinterpret_cast<const ulonglong2 *>(table)[2 * g + 1];
         const unsigned long long wv[STATS_PER] = {a.x, a.y, c.x, c.y};
         unsigned cm = 0;
+        // counts 1 and 2 (most keys) by two ballots; a warp holding a larger
+        // count groups those lanes by count (__match_any_sync)
+        unsigned n1 = 0, n2 = 0;
 #pragma unroll
         for (int q = 0; q < STATS_PER; q++) {
             const uint32_t k = (uint32_t)(wv[q] >> 32), n = (uint32_t)wv[q];
             const bool used = k != EMPTY_KEY && n > 0;
-            const bool exact = used && n < (uint32_t)CC_EXACT;
-            const unsigned peers = __match_any_sync(0xffffffffu, exact ? n : 0xFFFFFFFFu);
-            if (exact) {
-                if ((peers & lt) == 0) {
-                    const unsigned cnt = (unsigned)__popc(peers);
-                    atomicAdd(&sk[n], cnt);
-                    atomicAdd(&sr[n], (unsigned long long)cnt * n);
+            n1 += __popc(__ballot_sync(0xffffffffu, used && n == 1));
+            n2 += __popc(__ballot_sync(0xffffffffu, used && n == 2));
+            const bool big = used && n > 2;
+            if (__ballot_sync(0xffffffffu, big)) {
+                const bool exact = big && n < (uint32_t)CC_EXACT;
+                const unsigned peers = __match_any_sync(0xffffffffu, exact ? n : 0xFFFFFFFFu);
+                if (exact) {
+                    if ((peers & lt) == 0) {
+                        const unsigned cnt = (unsigned)__popc(peers);
+                        atomicAdd(&sk[n], cnt);
+                        atomicAdd(&sr[n], (unsigned long long)cnt * n);
+                    }
+                } else if (big) {
+                    const int b = cc_bin(n);
+                    atomicAdd(&sk[b], 1u);
+                    atomicAdd(&sr[b], (unsigned long long)n);
                 }
-            } else if (used) {
-                const int b = cc_bin(n);
-                atomicAdd(&sk[b], 1u);
-                atomicAdd(&sr[b], (unsigned long long)n);
             }
             if (used && n >= (uint32_t)CAND_MIN_COUNT) cm |= 1u << q;
+        }
+        if (lane == 0) {
+            if (n1) {
+                atomicAdd(&sk[1], n1);
+                atomicAdd(&sr[1], (unsigned long long)n1);
+            }
+            if (n2) {
+                atomicAdd(&sk[2], n2);
+                atomicAdd(&sr[2], 2ull * n2);
+            }
         }
         // candidate positions: warp prefix, then one global atomic per CTA
         uint32_t inc = (uint32_t)__popc(cm);
@@ -939,10 +961,11 @@ cudaError_t launch_decide(const LearnBufs &b, int use_model, double nS, double m
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t heavy_b1(uint32_t k) { return (k * 0x9E3779B1u) >> (32 - HEAVY_BKT_LOG2); }
 __device__ __forceinline__ uint32_t heavy_b2(uint32_t k) {
-    return HEAVY_BKT + (((k ^ (k >> 15)) * 0x85EBCA6Bu) >> (32 - HEAVY_BKT_LOG2));
+    return HEAVY_BKT + ((k * 0x85EBCA6Bu) >> (32 - HEAVY_BKT_LOG2));
 }
 
-// Slot of key k, or -1: both buckets are read and compared without branches.
+// Slot of key k, or -1: both buckets are read and compared without branches
+// (a key sits in at most one slot).
 __device__ __forceinline__ int heavy_lookup(const uint32_t *keys, uint32_t k) {
     const uint32_t b1 = heavy_b1(k), b2 = heavy_b2(k);
     const uint2 x = reinterpret_cast<const uint2 *>(keys)[b1];

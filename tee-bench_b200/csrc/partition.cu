@@ -202,12 +202,14 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan_bases(const uint32_t *tot
 }
 
 // Join work items from both relations' totals and bases (written by
-// k_plan_bases).  Thread t plans partitions t, t + 1024, ... (coalesced
-// reads); its items are written contiguously at its block-scan offset, so
-// the item list is grouped by thread, not sorted by partition.
+// k_plan_bases), planned by P / PLAN_THREADS CTAs.  Every CTA first counts
+// the items of all partitions (one coalesced read of both totals, from L2) to
+// take the same split decision; then thread t of CTA c plans partition
+// c * PLAN_THREADS + t, and each warp reserves its items with one atomic on
+// ctrl->nitems (zeroed by the launcher).  The item list is in reservation
+// order, not sorted by partition.
 __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
     __shared__ uint64_t scratch[PLAN_THREADS / 32 + 1];
-    __shared__ int s_split;
     const int P = 1 << a.P_log2;
     // S sides larger than capS are split (skew) for every R chunk of the
     // partition; if that would overflow the item buffer, partitions whose R
@@ -216,33 +218,44 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
         if (!a.capS || (nrc > 1 && !split_all)) return 1;
         return (hs + a.capS - 1) / a.capS;
     };
-    uint64_t cnt_all = 0, cnt_one = 0, nonempty = 0;
+    uint64_t cnt_all = 0;
     for (int f = threadIdx.x; f < P; f += PLAN_THREADS) {
         const uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
         if (hr == 0 || hs == 0) continue;
         const uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
         cnt_all += nrc * s_chunks(hs, nrc, true);
-        cnt_one += nrc * s_chunks(hs, nrc, false);
-        nonempty++;
     }
-    uint64_t total_all, total;
+    uint64_t total_all;
     block_excl_scan<PLAN_THREADS>(cnt_all, &total_all, scratch);
-    if (threadIdx.x == 0) s_split = total_all <= a.item_cap;
-    __syncthreads();
-    const bool split_all = s_split != 0;
-    uint64_t off = block_excl_scan<PLAN_THREADS>(split_all ? cnt_all : cnt_one, &total, scratch);
-    if (total > a.item_cap) {  // cannot happen with the host's bound; guard anyway
-        if (threadIdx.x == 0) {
-            atomicCAS(&a.ctrl->error, 0u, (unsigned)TBG_ERR_CAPACITY);
-            a.ctrl->nitems = 0;
+    const bool split_all = total_all <= a.item_cap;
+    const int f = blockIdx.x * PLAN_THREADS + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    uint32_t hr = 0, hs = 0;
+    uint64_t nrc = 0, nsc = 0;
+    if (f < P) {
+        hr = a.r.hist[f];
+        hs = a.s.hist[f];
+        if (hr && hs) {
+            nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
+            nsc = s_chunks(hs, nrc, split_all);
         }
-        return;
     }
-    for (int f = threadIdx.x; f < P; f += PLAN_THREADS) {
-        const uint32_t hr = a.r.hist[f], hs = a.s.hist[f];
-        if (hr == 0 || hs == 0) continue;
-        const uint64_t nrc = (hr + (uint64_t)a.capR - 1) / a.capR;
-        const uint64_t nsc = s_chunks(hs, nrc, split_all);
+    const uint64_t mine = nrc * nsc;
+    // warp prefix of the item counts, one reservation per warp
+    uint64_t inc = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    const uint64_t wtot = __shfl_sync(0xffffffffu, inc, 31);
+    unsigned wb = 0;
+    if (lane == 31 && wtot) wb = atomicAdd(&a.ctrl->nitems, (unsigned)wtot);
+    wb = __shfl_sync(0xffffffffu, wb, 31);
+    uint64_t off = (uint64_t)wb + inc - mine;
+    const bool fits = off + mine <= a.item_cap;  // always, with the host's bound; guarded anyway
+    if (mine && !fits) atomicCAS(&a.ctrl->error, 0u, (unsigned)TBG_ERR_CAPACITY);
+    if (mine && fits) {
         const uint64_t sstep = (hs + nsc - 1) / nsc;
         const uint64_t rb = a.r.base[f], sb = a.s.base[f];
         for (uint64_t rc = 0; rc < nrc; rc++) {
@@ -257,9 +270,8 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(PlanArgs a) {
             }
         }
     }
-    unsigned long long ne = warp_sum_u64(nonempty);
-    if ((threadIdx.x & 31) == 0 && ne) atomicAdd(&a.ctrl->nonempty, ne);
-    if (threadIdx.x == 0) a.ctrl->nitems = (unsigned)total;
+    const unsigned ne = __popc(__ballot_sync(0xffffffffu, mine != 0));
+    if (lane == 0 && ne) atomicAdd(&a.ctrl->nonempty, (unsigned long long)ne);
 }
 
 // ---------------------------------------------------------------------------
@@ -389,7 +401,10 @@ cudaError_t launch_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2
 }
 
 cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st) {
-    k_plan<<<1, PLAN_THREADS, 0, st>>>(a);
+    cudaError_t e = cudaMemsetAsync(&a.ctrl->nitems, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    const int P = 1 << a.P_log2;
+    k_plan<<<(P + PLAN_THREADS - 1) / PLAN_THREADS, PLAN_THREADS, 0, st>>>(a);
     count_launch();
     return cudaGetLastError();
 }

@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm(JoinArgs a) {
     __shared__ uint64_t scan_scratch[RSM_THREADS / 32 + 1];
     __shared__ uint32_t red[2];
     const int tid = threadIdx.x;
-    const unsigned nitems = *a.nitems;
+    const unsigned nitems = *a.err ? 0u : *a.nitems;  // a planner error leaves the item list unusable
     unsigned long long local = 0;
     for (;;) {
         if (tid == 0) s_item = atomicAdd(a.item_ctr, 1u);
@@ -526,7 +526,7 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
     __shared__ uint64_t scan_scratch[RSM_THREADS / 32 + 1];
     __shared__ uint32_t red[2];
     const int tid = threadIdx.x;
-    const unsigned nitems = *a.nitems;
+    const unsigned nitems = *a.err ? 0u : *a.nitems;  // a planner error leaves the item list unusable
     unsigned long long local = 0;
     uint32_t key[8];
     for (;;) {

@@ -48,9 +48,10 @@ TBG_HD inline float rank_feature(double rank) { return (float)(log2(rank + 1.0) 
 // Sample of S: blocks of SAMPLE_BLOCK consecutive rows (coalesced reads).
 constexpr int SAMPLE_BLOCK = 64;
 // Per-CTA shared-memory aggregation of the sample's keys before the global
-// count table: CNT_CHUNK keys per CTA into 2 * CNT_CHUNK slots.
+// count table: CNT_CHUNK keys per CTA into 2 * CNT_CHUNK slots (64 KB: two
+// CTAs per SM).
 constexpr int CNT_THREADS = 1024;
-constexpr int CNT_CHUNK = 2048;
+constexpr int CNT_CHUNK = 4096;
 // Count-of-counts bins: exact below CC_EXACT, then CC_OCT bins per octave.
 constexpr int CC_EXACT = 2048;
 constexpr int CC_OCT = 16;
