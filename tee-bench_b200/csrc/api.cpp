@@ -207,8 +207,52 @@ RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int ca
     g.ch[1] = ((nS + g.G[1] - 1) / g.G[1] + 1) & ~1ull;
     g.n[0] = nR;
     g.n[1] = nS;
+    // f = (key & (F1 - 1)) << b2 | (key >> b1) & (F2 - 1): pass 1 by the low b1
+    // bits, pass 2 by the next b2
     g.rf = g.passes == 1 ? RadixF{(uint32_t)(g.P - 1), 0, 0, 0}
                          : RadixF{(uint32_t)(g.F1 - 1), (uint32_t)g.b1, (uint32_t)((1u << g.b2) - 1), (uint32_t)g.b2};
+    g.d1 = DigitOp{0u, (uint32_t)(g.F1 - 1)};
+    g.d2 = DigitOp{(uint32_t)g.b1, (uint32_t)((1u << g.b2) - 1)};
+    return g;
+}
+
+// Geometry of an MSD partitioning of R and S by the top B bits of key - sub
+// (PSM): final partition f = (key - sub) >> lowbits holds a contiguous key
+// range, and partitions in order hold increasing keys.  Pass 1 takes the top
+// b1 bits of f, pass 2 the low b2 (one pass when B <= 8).  Chunking as in
+// radix_geometry.
+RadixGeom radix_geometry_msd(uint64_t nR, uint64_t nS, uint32_t sub, int B, int lowbits, Workspace &w) {
+    RadixGeom g;
+    g.B = B;
+    g.passes = B <= 8 ? 1 : 2;
+    g.b1 = g.passes == 2 ? B / 2 : B;
+    g.b2 = B - g.b1;
+    g.P = 1ull << B;
+    g.F1 = 1ull << g.b1;
+    g.capR = 0;
+    g.join_grid = 0;
+    g.capS = 0;
+    g.item_cap = 16;
+    const uint64_t min_chunk = std::max<uint64_t>(4096, g.P);
+    auto chunks = [&](uint64_t n) {
+        uint64_t c = std::min<uint64_t>((uint64_t)w.nsm * PASS1_CHUNKS_PER_SM, (n + min_chunk - 1) / min_chunk);
+        return (int)std::max<uint64_t>(c, 1);
+    };
+    g.G[0] = chunks(nR);
+    g.G[1] = chunks(nS);
+    g.ch[0] = ((nR + g.G[0] - 1) / g.G[0] + 1) & ~1ull;
+    g.ch[1] = ((nS + g.G[1] - 1) / g.G[1] + 1) & ~1ull;
+    g.n[0] = nR;
+    g.n[1] = nS;
+    g.rf = RadixF{0u, (uint32_t)lowbits, (uint32_t)(g.P - 1), 0u};
+    g.rf.sub = sub;
+    if (g.passes == 2) {
+        g.d1 = DigitOp{(uint32_t)(lowbits + g.b2), (uint32_t)(g.F1 - 1), sub};
+        g.d2 = DigitOp{(uint32_t)lowbits, (uint32_t)((1u << g.b2) - 1), sub};
+    } else {
+        g.d1 = DigitOp{(uint32_t)lowbits, (uint32_t)(g.P - 1), sub};
+        g.d2 = DigitOp{0u, 0u, sub};
+    }
     return g;
 }
 
@@ -308,6 +352,8 @@ int part_pass(int rel, int which, const RadixGeom &g, const Row *d, Workspace &w
     a.b1 = g.b1;
     a.b2 = g.b2;
     a.rf = g.rf;
+    a.d1 = g.d1;
+    a.d2 = g.d2;
     a.pre = (rel ? w.histS : w.histR).as<uint32_t>();
     a.totals = (rel ? w.totS : w.totR).as<uint32_t>();
     a.base = (rel ? w.baseS : w.baseR).as<uint64_t>();

@@ -112,10 +112,6 @@ struct PartSmem {
 
 // Digit of a pass: a bit field of the key (pass 1: bits [0, b1); pass 2:
 // bits [b1, b1 + b2); one pass: bits [0, B)).
-struct DigitOp {
-    uint32_t shift, mask;
-    __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return (key >> shift) & mask; }
-};
 
 // Destination shard of a key for a join split over n shards (n <= 256): the
 // top bits of a multiplicative hash, range-reduced by a multiply-shift, so

@@ -330,8 +330,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_part_pass1(PartArgs
     __syncthreads();
     const uint64_t lo = (uint64_t)c * a.chunk;
     const uint64_t hi = a.chunk_len ? lo + a.chunk_len[c] : umin64(a.n, lo + a.chunk);
-    DigitOp dop{0u, (uint32_t)F - 1};
-    part_range<THREADS>(a.in, lo, hi, a.n, a.out, (uint32_t)a.n, dop, F, sm, a.err);
+    part_range<THREADS>(a.in, lo, hi, a.n, a.out, (uint32_t)a.n, a.d1, F, sm, a.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -357,8 +356,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_part_pass2(PartArgs
         sm.cursor[d] = (uint32_t)a.base[f] + a.pre[(uint64_t)c0 * P + f];
     }
     __syncthreads();
-    DigitOp dop{(uint32_t)a.b1, (uint32_t)F2 - 1};
-    part_range<THREADS>(a.in, lo, hi, a.n, a.out, (uint32_t)a.n, dop, F2, sm, a.err);
+    part_range<THREADS>(a.in, lo, hi, a.n, a.out, (uint32_t)a.n, a.d2, F2, sm, a.err);
 }
 
 // ---------------------------------------------------------------------------

@@ -3,8 +3,11 @@
 // RSM (Joins/radix_sortmerge_join.c:102-105) shares RHO's radix partitioning
 // and swaps the build/probe kernel for a per-partition sort + merge-path join.
 // PSM (Joins/psm/parallel_sortmerge_join.h:61-111) sorts both relations by key
-// (LSD radix sort over the bits of key - min that vary, 7- to 9-bit digits,
-// chunked stable passes) and merges them.
+// and merges them.  The sort is MSD: RHO's histogram and passes partition by
+// the top bits of key - min (at most 15), then every bucket is sorted by the
+// remaining 12 or 13 bits in one counting pass.  Relations whose key range
+// leaves more low bits, or with a bucket over a million rows (a heavy key),
+// take an LSD radix sort (7- to 9-bit digits, chunked stable passes).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -116,6 +119,57 @@ int lsd_sort_chunked(const Row *in, uint64_t n, uint32_t kmin, uint32_t kmax, De
     return TBG_OK;
 }
 
+cudaError_t launch_bucket_sort(const Row *in, Row *out, const uint64_t *base, uint32_t nb, uint32_t sub, int lowbits,
+                               int nsm, cudaStream_t st);
+
+// MSD sort of both relations: radix partitioning by the top B bits of
+// key - sub (RHO's histogram and passes), then each bucket sorted by the low
+// `lowbits` bits (k_bucket_sort), into sorted[0] (R) and sorted[1] (S).  A
+// relation with a bucket over kBucketMax rows (a heavy key) is left for the
+// LSD sort instead: msd_done[rel] says which ones were sorted.
+static constexpr uint64_t kBucketMax = 1u << 20;
+static constexpr int kLowBits = 12, kLowBitsMax = 13;
+
+static int msd_sort(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS, uint32_t sub,
+                    int span, Row *sorted[2], bool msd_done[2], Workspace &w, cudaStream_t st, JoinRun *run) {
+    msd_done[0] = msd_done[1] = false;
+    int lowbits = std::min(span, kLowBits), B = span - lowbits;
+    if (B > 15) {
+        B = 15;
+        lowbits = span - B;
+    }
+    if (B < 1 || lowbits > kLowBitsMax) return TBG_OK;  // the LSD sort takes both
+    const RadixGeom g = radix_geometry_msd(nR, nS, sub, B, lowbits, w);
+    int rc = ensure_radix_buffers(g, false, w);
+    if (rc) return rc;
+    Ctrl *ctrl = w.ctrl.as<Ctrl>();
+    if ((rc = part_histogram(0, g, dR, cfg, w, st, nullptr)) || (rc = part_histogram(1, g, dS, cfg, w, st, nullptr)))
+        return rc;
+    // the largest bucket of each relation decides between this sort and LSD
+    unsigned long long *hm = static_cast<unsigned long long *>(w.host_small);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(hm, &ctrl->max_part_R, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_error(e, "bucket sizes");
+    const unsigned long long maxp[2] = {hm[0], hm[1]};
+    const Row *in[2] = {dR, dS};
+    for (int rel = 0; rel < 2; rel++) {
+        if (maxp[rel] > kBucketMax) continue;
+        if ((rc = part_pass(rel, 1, g, in[rel], w, st, false)) || (rc = part_pass(rel, 2, g, in[rel], w, st, false)))
+            return rc;
+        const Row *part = (rel ? w.partS : w.partR).as<Row>();
+        const uint64_t *base = (rel ? w.baseS : w.baseR).as<uint64_t>();
+        if ((e = launch_bucket_sort(part, sorted[rel], base, (uint32_t)g.P, sub, lowbits, w.nsm, st)) != cudaSuccess)
+            return cuda_error(e, "bucket sort");
+        msd_done[rel] = true;
+        mark_ev(w, cfg.timing != 0, 2 + rel, st);
+    }
+    run->B = B;
+    run->passes = g.passes + 1;
+    run->P = g.P;
+    return TBG_OK;
+}
+
 int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                  tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st, JoinRun *run) {
     const bool timing = cfg.timing != 0;
@@ -147,21 +201,31 @@ int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *d
         return cuda_error(e, "key range");
     const uint32_t rmin = hm[0], rmax = hm[1], smin = hm[2], smax = hm[3];
     mark_ev(w, timing, 1, st);
-    const Row *sR = nullptr, *sS = nullptr;
+    // MSD sort over the keys of both relations (empty relations have min > max)
+    const uint32_t lo = std::min(nR ? rmin : smin, nS ? smin : rmin), hi = std::max(nR ? rmax : smax, nS ? smax : rmax);
+    const int span = (nR || nS) && hi > lo ? 32 - __builtin_clz(hi - lo) : 0;
+    Row *sorted[2] = {w.aux[0].as<Row>(), w.aux[2].as<Row>()};
+    bool msd_done[2] = {false, false};
+    run->B = 8;
+    run->P = 0;
+    run->passes = 0;
+    int rc = nR && nS ? msd_sort(cfg, dR, nR, dS, nS, lo, span, sorted, msd_done, w, st, run) : TBG_OK;
+    if (rc) return rc;
+    const Row *sR = sorted[0], *sS = sorted[1];
     int pr = 0, ps = 0;
-    int rc = lsd_sort_chunked(dR, nR, rmin, rmax, w.aux[0], w.aux[1], w, st, &sR, &pr);
-    if (rc) return rc;
-    mark_ev(w, timing, 2, st);
-    rc = lsd_sort_chunked(dS, nS, smin, smax, w.aux[2], w.aux[3], w, st, &sS, &ps);
-    if (rc) return rc;
-    mark_ev(w, timing, 3, st);
+    if (!msd_done[0]) {
+        if ((rc = lsd_sort_chunked(dR, nR, rmin, rmax, w.aux[0], w.aux[1], w, st, &sR, &pr))) return rc;
+        mark_ev(w, timing, 2, st);
+    }
+    if (!msd_done[1]) {
+        if ((rc = lsd_sort_chunked(dS, nS, smin, smax, w.aux[2], w.aux[3], w, st, &sS, &ps))) return rc;
+        mark_ev(w, timing, 3, st);
+    }
     e = launch_merge_join(sR, nR, sS, nS, w.aux[6].as<uint64_t>(), &ctrl->matches, &ctrl->rows, d_rows,
                           d_rows ? cap : 0, cfg.materialize != 0, st);
     if (e != cudaSuccess) return cuda_error(e, "merge join");
     mark_ev(w, timing, 4, st);
-    run->B = 8;
-    run->passes = std::max(pr, ps);
-    run->P = 0;
+    if (!msd_done[0] || !msd_done[1]) run->passes = std::max(run->passes, std::max(pr, ps));
     run->timed = timing;
     return TBG_OK;
 }

@@ -647,8 +647,15 @@ cudaError_t launch_key_range(const Row *in, uint64_t n, uint32_t *minmax, int ns
 // shared store, splits its D diagonals evenly over threads and walks them.
 // A run of equal R keys that continues past the tile is finished in global
 // memory.
-constexpr int MERGE_THREADS = 256;
-constexpr int MERGE_PER_THREAD = 16;
+// Merge tile shape (build options for A/B timing).
+#ifndef TBG_MERGE_THREADS
+#define TBG_MERGE_THREADS 256
+#endif
+#ifndef TBG_MERGE_PER_THREAD
+#define TBG_MERGE_PER_THREAD 16
+#endif
+constexpr int MERGE_THREADS = TBG_MERGE_THREADS;
+constexpr int MERGE_PER_THREAD = TBG_MERGE_PER_THREAD;
 constexpr int MERGE_TILE = MERGE_THREADS * MERGE_PER_THREAD;
 
 __global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row *__restrict__ S, uint64_t ns,
@@ -671,8 +678,9 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_join(const Row *__restr
     // keys (and payloads when materialising) of the tile's R rows [0, nrt),
     // then of its S rows; one spare slot so a walk may read one row past
     // either side without a guard
-    __shared__ uint32_t K[MERGE_TILE + 1];
-    __shared__ uint32_t Pay[MAT ? MERGE_TILE : 1];
+    extern __shared__ __align__(16) uint32_t merge_smem[];
+    uint32_t *K = merge_smem;                 // MERGE_TILE + 1 keys
+    uint32_t *Pay = merge_smem + MERGE_TILE + 1;  // MERGE_TILE payloads (materialising)
     __shared__ unsigned long long s_base;
     __shared__ uint64_t scan_scratch[MERGE_THREADS / 32 + 1];
     const uint64_t L = nr + ns;
@@ -778,10 +786,11 @@ cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t 
     if (!grid) return cudaSuccess;
     const uint64_t nsplits = grid + 1;
     k_merge_splits<<<(unsigned)((nsplits + 255) / 256), 256, 0, st>>>(R, nr, S, ns, splits, nsplits);
-    if (mat)
-        k_merge_join<true><<<(unsigned)grid, MERGE_THREADS, 0, st>>>(R, nr, S, ns, splits, matches, rows_ctr, out, cap);
-    else
-        k_merge_join<false><<<(unsigned)grid, MERGE_THREADS, 0, st>>>(R, nr, S, ns, splits, matches, rows_ctr, out, cap);
+    const size_t smem = (size_t)(MERGE_TILE + 1 + (mat ? MERGE_TILE : 0)) * 4;
+    auto kern = mat ? k_merge_join<true> : k_merge_join<false>;
+    cudaError_t e = smem_limit((const void *)kern, smem);
+    if (e != cudaSuccess) return e;
+    kern<<<(unsigned)grid, MERGE_THREADS, smem, st>>>(R, nr, S, ns, splits, matches, rows_ctr, out, cap);
     count_launch(2);
     return cudaGetLastError();
 }

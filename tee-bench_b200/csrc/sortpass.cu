@@ -196,4 +196,177 @@ cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// PSM bucket sort.  After the partitioning passes by the top bits of
+// key - sub (final partition f = (key - sub) >> lowbits), bucket b holds
+// rows [base[b], base[b + 1]) whose keys agree above bit `lowbits`; sorting
+// every bucket by the low `lowbits` bits leaves the relation sorted.  One CTA
+// per SM walks the buckets.  Per bucket:
+//   1. the bucket's histogram over 2^lowbits bins in shared memory (the one
+//      read from DRAM) and its exclusive scan;
+//   2. the bins are cut into 2^pbits parts of consecutive bins, each small
+//      enough (as the histogram shows) to stage in shared memory: per part,
+//      a re-read of the bucket (from L2) places the part's rows at their
+//      sorted positions in the stage, which is then written out with
+//      coalesced stores (a 32K-row bucket: two parts).  A part too large
+//      for the stage (a heavy key) has its rows written straight to their
+//      sorted positions instead.
+// Staging row indices instead (4 bytes, one part per bucket, the rows
+// gathered back from L2 at the write-out) measured 12.8 against 8.3 ms for
+// 2^30 rows: the gather's scattered 8-byte reads cost more L2 sectors than
+// the second part's stream.
+// Rows of equal keys land in any order, which the merge does not need (a
+// join's rows are a multiset).
+// ---------------------------------------------------------------------------
+// Threads, CTAs per SM and shared memory of the bucket sort (build options
+// for A/B timing; the CTAs of one SM hold the buckets in flight in L2).
+#ifndef TBG_BSORT_THREADS
+#define TBG_BSORT_THREADS 1024
+#endif
+#ifndef TBG_BSORT_CTAS
+#define TBG_BSORT_CTAS 1
+#endif
+constexpr int BSORT_THREADS = TBG_BSORT_THREADS;
+constexpr int BSORT_CTAS = TBG_BSORT_CTAS;
+constexpr int BSORT_PAIRS = 2;                                   // 16-byte row pairs per thread per round
+constexpr size_t BSORT_SMEM = (BSORT_CTAS == 1 ? 200 : 100) * 1024;  // stage + bins
+
+__device__ __forceinline__ uint32_t bsort_bin(uint32_t key, uint32_t sub, uint32_t mask) { return (key - sub) & mask; }
+
+// Calls fn(row, index, valid, dup) for every row of the bucket (index: its
+// place in the bucket), in block-uniform rounds (so fn may use warp
+// collectives); `dup` says the warp saw repeated bins in the round's first
+// row slot (skew).  The next round's loads are issued before the current
+// round is handed to fn.  The bucket's edge rows (outside the 16-byte
+// aligned body) come in a last round of warp 0.
+template <class Fn>
+__device__ __forceinline__ void bsort_stream(const Row *src, uint32_t len, uint32_t sub, uint32_t mask, Fn fn) {
+    const int tid = threadIdx.x;
+    const uint32_t head = (reinterpret_cast<uintptr_t>(src) & 15) ? 1u : 0u;
+    const uint32_t npairs = (len - head) / 2;
+    const bool tail = ((len - head) & 1) != 0;
+    const uint4 *v = reinterpret_cast<const uint4 *>(src + head);
+    constexpr uint32_t ROUND = BSORT_PAIRS * BSORT_THREADS;
+    uint4 nx[BSORT_PAIRS];
+    auto load = [&](uint32_t p0) {
+#pragma unroll
+        for (int u = 0; u < BSORT_PAIRS; u++) {
+            const uint32_t p = p0 + u * BSORT_THREADS + tid;
+            nx[u] = p < npairs ? __ldcg(v + p) : make_uint4(0, 0, 0, 0);
+        }
+    };
+    load(0);
+    for (uint32_t p0 = 0; p0 < npairs; p0 += ROUND) {
+        uint4 x[BSORT_PAIRS];
+#pragma unroll
+        for (int u = 0; u < BSORT_PAIRS; u++) x[u] = nx[u];
+        load(p0 + ROUND);
+        const bool dup = warp_has_dups(bsort_bin(x[0].x, sub, mask), p0 + tid < npairs);
+#pragma unroll
+        for (int u = 0; u < BSORT_PAIRS; u++) {
+            const uint32_t p = p0 + u * BSORT_THREADS + tid;
+            const bool ok = p < npairs;
+            fn(Row{x[u].x, x[u].y}, head + 2 * p, ok, dup);
+            fn(Row{x[u].z, x[u].w}, head + 2 * p + 1, ok, dup);
+        }
+    }
+    if (tid < 32) {
+        const int lane = tid;
+        const bool ok = (lane == 0 && head) || (lane == 1 && tail);
+        const uint32_t i = lane == 0 ? 0u : len - 1;
+        const Row r = ok ? src[i] : Row{0, 0};
+        fn(r, i, ok, false);
+    }
+}
+
+__global__ void __launch_bounds__(BSORT_THREADS, BSORT_CTAS) k_bucket_sort(const Row *__restrict__ in, Row *__restrict__ out,
+                                                                const uint64_t *__restrict__ base, uint32_t nb,
+                                                                uint32_t sub, int lowbits) {
+    extern __shared__ __align__(16) unsigned char bsmem[];
+    const uint32_t bins = 1u << lowbits, mask = bins - 1;
+    uint32_t *h = reinterpret_cast<uint32_t *>(bsmem);          // bins
+    uint2 *stage = reinterpret_cast<uint2 *>(bsmem + 4 * bins);  // cap rows
+    const uint32_t cap = (uint32_t)((BSORT_SMEM - 4 * (size_t)bins) / 8);
+    __shared__ uint64_t scratch[BSORT_THREADS / 32 + 1];
+    const int tid = threadIdx.x;
+    const uint32_t per = (bins + BSORT_THREADS - 1) / BSORT_THREADS;
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const uint64_t lo = base[b], hi = base[b + 1];  // the same for every thread
+        if (hi <= lo) continue;
+        const Row *src = in + lo;
+        uint2 *dst = reinterpret_cast<uint2 *>(out + lo);
+        const uint32_t len = (uint32_t)(hi - lo);  // a bucket holds < 2^32 rows
+        if (len == 1) {
+            if (tid == 0) dst[0] = make_uint2(src[0].key, src[0].payload);
+            continue;
+        }
+        for (uint32_t q = tid; q < bins; q += BSORT_THREADS) h[q] = 0;
+        __syncthreads();
+        // 1. histogram and exclusive scan
+        bsort_stream(src, len, sub, mask, [&](Row r, uint32_t, bool ok, bool dup) {
+            hist_add_warp(h, ok ? bsort_bin(r.key, sub, mask) : 0u, ok, dup);
+        });
+        __syncthreads();
+        {
+            const uint32_t b0 = min(bins, tid * per), b1 = min(bins, b0 + per);
+            uint32_t sum = 0;
+            for (uint32_t q = b0; q < b1; q++) sum += h[q];
+            uint64_t tot;
+            uint32_t run = (uint32_t)block_excl_scan<BSORT_THREADS>(sum, &tot, scratch);
+            for (uint32_t q = b0; q < b1; q++) {
+                const uint32_t c = h[q];
+                h[q] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+        // 2. parts of 2^(lowbits - pbits) bins, an even share of the bucket
+        // each filling at most 7/8 of the stage
+        int pbits = 0;
+        while (pbits < lowbits && ((uint64_t)len >> pbits) > cap - cap / 8) pbits++;
+        const int pshift = lowbits - pbits;
+        for (uint32_t part = 0; part < (1u << pbits); part++) {
+            const uint32_t pb0 = part << pshift, pb1 = (part + 1) << pshift;
+            // the part's sorted rows: [h[pb0], h[pb1]) before any of them is ranked
+            const uint32_t r0 = h[pb0], r1 = pb1 < bins ? h[pb1] : len;
+            __syncthreads();  // every thread has read the part's bounds
+            if (r1 == r0) continue;
+            const bool staged = r1 - r0 <= cap;
+            bsort_stream(src, len, sub, mask, [&](Row r, uint32_t, bool ok, bool dup) {
+                const uint32_t d = bsort_bin(r.key, sub, mask);
+                const bool mine = ok && d >= pb0 && d < pb1;
+                const uint32_t pos = rank_warp(h, mine ? d : 0u, mine, dup);
+                if (mine) {
+                    if (staged) stage[pos - r0] = make_uint2(r.key, r.payload);
+                    else dst[pos] = make_uint2(r.key, r.payload);
+                }
+            });
+            __syncthreads();
+            if (staged)
+                for (uint32_t q = tid; q < r1 - r0; q += BSORT_THREADS) dst[r0 + q] = stage[q];
+            __syncthreads();  // the stage is refilled by the next part
+        }
+    }
+}
+
+size_t bucket_sort_smem(int lowbits) {
+    (void)lowbits;  // the stage takes what the bins leave
+    return BSORT_SMEM;
+}
+
+cudaError_t launch_bucket_sort(const Row *in, Row *out, const uint64_t *base, uint32_t nb, uint32_t sub, int lowbits,
+                               int nsm, cudaStream_t st) {
+    if (!nb) return cudaSuccess;
+    if (lowbits > 14) return cudaErrorInvalidValue;  // the bins must leave room for a stage
+    const size_t smem = bucket_sort_smem(lowbits);
+    cudaError_t e = smem_limit((const void *)k_bucket_sort, smem);
+    if (e != cudaSuccess) return e;
+    // one CTA per SM: the buckets in flight (each read from DRAM once and
+    // re-read per part) stay within L2
+    const unsigned g = (unsigned)std::min<uint64_t>(nb, (uint64_t)nsm * BSORT_CTAS);
+    k_bucket_sort<<<g, BSORT_THREADS, smem, st>>>(in, out, base, nb, sub, lowbits);
+    count_launch();
+    return cudaGetLastError();
+}
+
 }  // namespace tbg

@@ -65,6 +65,18 @@ struct RadixF {
     uint32_t sub = 0;  // digits are taken from key - sub (an order-preserving offset for sorts)
 };
 
+// Digit of a key in one partitioning pass: ((key - sub) >> shift) & mask.
+struct DigitOp {
+    uint32_t shift, mask;
+    uint32_t sub = 0;
+#ifdef __CUDACC__
+    __host__ __device__
+#endif
+        uint32_t operator()(uint32_t key) const {
+        return ((key - sub) >> shift) & mask;
+    }
+};
+
 // Per-relation partition plan written by the planner kernel.
 struct RelPlan {
     uint32_t *hist;       // [P]   final partition sizes
@@ -82,6 +94,7 @@ struct PartArgs {
     int group;                // pass 2: consecutive chunks per unit
     int b1, b2;               // digit bits of pass 1 and pass 2 (b2 = 0: one pass)
     RadixF rf;
+    DigitOp d1, d2;           // digit of pass 1 and of pass 2 (consistent with rf: f = d1 << b2 | d2)
     const uint32_t *pre;      // [G][P] rows of partition f in chunks before c
     const uint32_t *totals;   // [P]
     const uint64_t *base;     // [P+1]

@@ -85,9 +85,11 @@ struct RadixGeom {
     int G[2];          // chunks of R, S
     uint64_t ch[2];    // rows per chunk
     uint64_t n[2];     // rows of R, S
-    RadixF rf;
+    RadixF rf;         // final partition f of a key (histograms)
+    DigitOp d1, d2;    // pass-1 and pass-2 digits: f = d1 << b2 | d2
 };
 RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int capR, Workspace &w);
+RadixGeom radix_geometry_msd(uint64_t nR, uint64_t nS, uint32_t sub, int B, int lowbits, Workspace &w);
 int ensure_radix_buffers(const RadixGeom &g, bool bypass, Workspace &w);
 int part_histogram(int rel, const RadixGeom &g, const Row *d, const tbg_config &cfg, Workspace &w, cudaStream_t st,
                    const SBypass *bypass);

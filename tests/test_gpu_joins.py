@@ -236,12 +236,28 @@ def test_join_table_size_gate(tbg, oracle, cuda, algo, bits):
 PSM_PLANS = [(12, 0), (20, 0), (21, 0), (27, 0), (28, 0), (32, 0), (27, 1), (20, 3_000_000_000)]
 
 
+def psm_passes(bits):
+    """Passes PSM reports for a key range of `bits` bits above its minimum:
+    MSD (radix passes over the top B <= 15 bits, then one bucket-sort pass
+    over the low 12, at most 13, bits) when the range has bits above the low
+    ones; otherwise the LSD sort's passes of at most 9 bits."""
+    low = min(bits, 12)
+    B = bits - low
+    if B > 15:
+        B, low = 15, bits - 15
+    if B < 1 or low > 13:
+        return (bits + 8) // 9
+    return (1 if B <= 8 else 2) + 1
+
+
 @pytest.mark.parametrize("span,low", PSM_PLANS, ids=[f"span{s}-low{lo}" for s, lo in PSM_PLANS])
 def test_psm_digit_plans(tbg, oracle, cuda, span, low):
-    """PSM's LSD sort covers the bits of key - min that vary: 9-bit digits when
-    they save a pass (a 27-bit range: 3 passes), 7-bit digits at an equal pass
-    count (20, 21, 28 bits).  Keys 1..2^27 (low = 1) span 28 bits raw but 27
-    above their minimum, so they take 3 passes; a range high in the key space
+    """PSM's sort covers the bits of key - min that vary.  Ranges of 13 to 28
+    bits take the MSD sort (one or two radix passes over the top bits, one
+    bucket sort over the low 12 or 13); a 12-bit range (no bits above the low
+    ones) and a 32-bit one (too many low bits) take the LSD sort (9-bit digits
+    when they save a pass, 7-bit at an equal count).  Keys 1..2^27 (low = 1)
+    span 28 bits raw but 27 above their minimum; a range high in the key space
     takes the passes its width needs.  Every plan must give the oracle's count
     and rows."""
     rng = np.random.default_rng(span)
@@ -260,10 +276,37 @@ def test_psm_digit_plans(tbg, oracle, cuda, span, low):
     m, _, st = run_join(tbg, cuda, "PSM", R, S)
     assert m == ref
     bits = int(width - 1).bit_length()
-    assert st.passes == (bits + 8) // 9, (bits, st.passes)
+    assert st.passes == psm_passes(bits), (bits, st.passes)
     m, rows, _ = run_join(tbg, cuda, "PSM", R, S, materialize=True, cap=ref)
     assert m == ref
     assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+
+
+@pytest.mark.parametrize("materialize", [False, True])
+def test_psm_heavy_key_takes_lsd(tbg, oracle, cuda, materialize):
+    """A Zipf S whose hottest key fills one MSD bucket past a million rows is
+    sorted by the LSD passes, while R keeps the MSD sort; count and rows match
+    the oracle either way."""
+    import torch
+
+    nR, nS = 1 << 18, 1 << 22
+    st = torch.cuda.current_stream().cuda_stream
+    tR = torch.empty(nR, dtype=torch.int64, device="cuda")
+    tS = torch.empty(nS, dtype=torch.int64, device="cuda")
+    tbg.gen_pk(tR.data_ptr(), nR, 3, st)
+    tbg.gen_zipf(tS.data_ptr(), nS, nR, 1.5, 0, 4, st)
+    R = tR.cpu().numpy().view(oracle.ROW)
+    S = tS.cpu().numpy().view(oracle.ROW)
+    assert np.bincount(S["key"]).max() > 1 << 20
+    if materialize:
+        ref, ref_rows = oracle.rho(R, S, materialize=True)
+        m, rows, _ = run_join(tbg, cuda, "PSM", R, S, materialize=True, cap=ref)
+        assert m == ref
+        assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+    else:
+        ref = oracle.rho(R, S)
+        m, _, _ = run_join(tbg, cuda, "PSM", R, S)
+        assert m == ref == nS
 
 
 @pytest.mark.parametrize("materialize", [False, True])
