@@ -142,6 +142,9 @@ static int ceil_log2(uint64_t x) {
 
 void choose_radix(const tbg_config &cfg, uint64_t nR, int capR, int *B, int *passes) {
     int b = cfg.radix_bits;
+#ifdef TBG_RADIX_BITS_FORCE  // a build option for A/B timing of other geometries
+    if (b <= 0) b = TBG_RADIX_BITS_FORCE;
+#endif
     if (b <= 0) {
         // R partitions of about capR / 2 rows: room for uneven radix buckets
         uint64_t target = (uint64_t)capR / 2;
@@ -163,11 +166,25 @@ void mark(Workspace &w, bool timing, int i, cudaStream_t st) {
 
 // Geometry of the chunked radix partitioning of R and S into 2^B final
 // partitions (shared by RHO, RHT, RSM and LRN).
-// R rows per shared-memory join table: JOIN_CAPR_DEFAULT (three CTAs per SM)
-// while R's partitions at the largest radix (15 bits) fit it, else the next
-// power of two, up to 16384 (one CTA per SM), so a partition of R is built
-// once and S is not probed twice.
-int join_capacity(uint64_t nR) {
+// R rows per shared-memory join table that the planner plans with (R
+// partitions larger than that are joined in chunks).  choose_radix aims the
+// average R partition at half of it.
+//   Counting joins, |R| <= 2^28: JOIN_CAPR_WIDE, so the radix geometry is the
+//   one whose average R partition fills a JOIN_CAPR_FIT-row table (14 bits,
+//   7 + 7, at |R| = 2^27, where half-full 5120-row tables need 15 bits,
+//   7 + 8).  The join then launches a JOIN_CAPR_FIT-row table kernel and a
+//   JOIN_CAPR_WIDE one, each gated on the largest R partition (device
+//   memory).  Measured at 2^27 x 2^30: 11.41 ms against 12.28 ms; the
+//   8-bit fan-out of the second pass costs more than the bigger tables.
+//   Otherwise: JOIN_CAPR_DEFAULT (three CTAs per SM) while R's partitions at
+//   the largest radix (15 bits) fit it, else the next power of two, up to
+//   16384 (one CTA per SM), so a partition of R is built once and S is not
+//   probed twice.
+int join_capacity(uint64_t nR, bool counting) {
+#ifdef TBG_JOIN_CAPR_FORCE  // a build option for A/B timing of other table sizes
+    if (nR) return TBG_JOIN_CAPR_FORCE;
+#endif
+    if (counting && nR <= ((uint64_t)JOIN_CAPR_FIT << 15)) return JOIN_CAPR_WIDE;
     const uint64_t per = (nR + (1u << 15) - 1) >> 15;
     if (per <= (uint64_t)JOIN_CAPR_DEFAULT) return JOIN_CAPR_DEFAULT;
     uint64_t c = 8192;
@@ -178,7 +195,12 @@ int join_capacity(uint64_t nR) {
 RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int capR, Workspace &w) {
     RadixGeom g;
     choose_radix(cfg, nR, capR, &g.B, &g.passes);
-    g.b1 = g.passes == 2 ? g.B / 2 : g.B;
+    // an odd B gives pass 1 the smaller digit (7 + 8 at 15 bits), or with
+    // TBG_PASS1_WIDER the larger (8 + 7); a build option for A/B timing
+#ifndef TBG_PASS1_WIDER
+#define TBG_PASS1_WIDER 0
+#endif
+    g.b1 = g.passes == 2 ? (TBG_PASS1_WIDER ? (g.B + 1) / 2 : g.B / 2) : g.B;
     g.b2 = g.B - g.b1;
     g.P = 1ull << g.B;
     g.F1 = 1ull << g.b1;
@@ -427,7 +449,7 @@ int radix_partition(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row
 int run_radix_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                    tbg_row_out *d_rows, uint64_t cap, Workspace &w, cudaStream_t st,
                    JoinRun *run) {
-    const int capR = join_capacity(nR);
+    const int capR = join_capacity(nR, !cfg.materialize);
     int join_grid = 0;
     int rc = radix_partition(cfg, dR, nR, dS, nS, capR, w, st, run, &join_grid);
     if (rc) return rc;
@@ -449,7 +471,7 @@ int run_radix_join_sliced(const tbg_config &cfg, const Row *dR, uint64_t nR, con
                           int nslices, const std::function<int(int)> &issue, cudaEvent_t r_ready,
                           const cudaEvent_t *s_ready, tbg_row_out *d_rows, uint64_t cap, Workspace &w,
                           cudaStream_t st, JoinRun *run) {
-    const int capR = join_capacity(nR);
+    const int capR = join_capacity(nR, !cfg.materialize);
     uint64_t smax = 1;
     for (int k = 0; k < nslices; k++) smax = std::max(smax, s_lo[k + 1] - s_lo[k]);
     const RadixGeom gmax = radix_geometry(cfg, nR, smax, capR, w);
@@ -508,21 +530,26 @@ int radix_join_phase(const tbg_config &cfg, tbg_row_out *d_rows, uint64_t cap, W
     ja.gate_max = 0;
     ja.gate_le = 0;
     cudaError_t e;
-    if (!cfg.materialize && capR == JOIN_CAPR_DEFAULT) {
-        // Counting with 4096-row tables takes less shared memory per CTA and
-        // is faster, but only fits when no R partition is larger; that size
-        // is known on the device only (the planner's max_part_R).  So both
-        // table sizes are launched, each gated on it: one does the join, the
-        // other returns at once, and no host read-back is needed.
+    // Counting with a smaller table takes less shared memory per CTA and is
+    // faster, but only fits when no R partition is larger; that size is
+    // known on the device only (the planner's max_part_R).  So both table
+    // sizes are launched, each gated on it: one does the join, the other
+    // returns at once, and no host read-back is needed.  The geometry of
+    // JOIN_CAPR_WIDE plans aims R's partitions at JOIN_CAPR_FIT rows.
+    const int small_cap = cfg.materialize ? 0
+                          : capR == JOIN_CAPR_WIDE    ? JOIN_CAPR_FIT
+                          : capR == JOIN_CAPR_DEFAULT ? JOIN_CAPR_SMALL
+                                                      : 0;
+    if (small_cap) {
         JoinArgs small = ja;
-        small.capR = JOIN_CAPR_SMALL;
+        small.capR = small_cap;
         small.gate = &ctrl->max_part_R;
-        small.gate_max = JOIN_CAPR_SMALL;
+        small.gate_max = (unsigned long long)small_cap;
         small.gate_le = 1;
-        if ((e = launch_join(small, false, w.nsm * join_ctas_per_sm(JOIN_CAPR_SMALL), st)) != cudaSuccess)
+        if ((e = launch_join(small, false, w.nsm * join_ctas_per_sm(small_cap), st)) != cudaSuccess)
             return cuda_error(e, "join");
         ja.gate = small.gate;
-        ja.gate_max = JOIN_CAPR_SMALL;
+        ja.gate_max = (unsigned long long)small_cap;
         ja.gate_le = 0;
     }
     e = launch_join(ja, cfg.materialize != 0, join_grid, st);

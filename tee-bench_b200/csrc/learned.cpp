@@ -74,7 +74,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     const uint64_t m = nb * SAMPLE_BLOCK;
     uint32_t tslots = 1u << 16;
     while (tslots < m + m / 2 && tslots < (1u << 24)) tslots <<= 1;
-    const int capR = join_capacity(nR);
+    const int capR = join_capacity(nR, !cfg.materialize);
     const RadixGeom g = radix_geometry(cfg, nR, nS, capR, w);
     run->B = g.B;
     run->passes = g.passes;

@@ -52,6 +52,8 @@ constexpr int PART_ITEMS = 8;
 // Shared-memory table capacity of the build/probe kernels (rows of R_p).
 constexpr int JOIN_THREADS = 512;
 constexpr int JOIN_CAPR_DEFAULT = 5120;
+constexpr int JOIN_CAPR_FIT = 8192;    // counting joins: the average R partition fills this table
+constexpr int JOIN_CAPR_WIDE = 16384;  // ... and partitions up to this size are joined whole
 constexpr int JOIN_CAPR_SMALL = 4096;  // count-only tables when every R partition fits it
 
 // Bounded device waits: iterations before a wait gives up with TBG_ERR_TIMEOUT.

@@ -59,7 +59,7 @@ Workspace *workspace_for(cudaStream_t st);
 int set_error(int code, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
 void choose_radix(const tbg_config &cfg, uint64_t nR, int capR, int *B, int *passes);
-int join_capacity(uint64_t nR);
+int join_capacity(uint64_t nR, bool counting);
 
 int join_device_impl(const tbg_config *cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS,
                      tbg_row_out *d_rows, uint64_t rows_cap, cudaStream_t st, JoinRun *run,
