@@ -59,6 +59,7 @@ WORKLOADS = {
     "radix_c3_z1": ("RHO", 26, 29, "zipf", 1.0),
     "plain_c3_z1": ("RHO", 26, 29, "zipf", 1.0, {"skew_split": 0}),
     "lrn_c3_z1": ("LRN", 26, 29, "zipf", 1.0),
+    "radix_c3_z15": ("RHO", 26, 29, "zipf", 1.5),
     "plain_c3_z15": ("RHO", 26, 29, "zipf", 1.5, {"skew_split": 0}),
     "lrn_c3_z15": ("LRN", 26, 29, "zipf", 1.5),
     "rho_c1": ("RHO", 21, 21, "fk", 100),

@@ -34,13 +34,14 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
     t.heads = t.pay + a.capR;
     t.next = reinterpret_cast<uint16_t *>(t.heads + a.capR + 2);
     t.head64 = nullptr;
+    t.hcap = floor_pow2((uint32_t)a.capR + 2);
     if (!MAT && a.layout == 0) {  // count only: keys, packed heads (capR * 4 is a multiple of 8), links
+        t.hcap = count_head_slots(a.capR);
         t.head64 = reinterpret_cast<uint64_t *>(t.key + a.capR);
-        t.next = reinterpret_cast<uint16_t *>(t.head64 + floor_pow2((uint32_t)a.capR + 2));
+        t.next = reinterpret_cast<uint16_t *>(t.head64 + t.hcap);
     }
     t.hs = a.hash_shift;
     t.layout = a.layout;
-    t.hcap = floor_pow2((uint32_t)a.capR + 2);
     const int tid = threadIdx.x;
     const unsigned nitems = *a.err ? 0u : *a.nitems;  // a planner error leaves the item list unusable
     unsigned long long local = 0;
@@ -133,18 +134,27 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
 size_t join_smem_bytes(int capR) {
     return (size_t)capR * 4 * 2 + ((size_t)capR + 2) * 4 + (size_t)capR * 2 + 16;
 }
+// Shared memory of a k_join launch: counting bucket-chain tables hold keys,
+// packed heads and links only.
+size_t join_launch_smem(int capR, bool materialize, int layout) {
+    if (!materialize && layout == 0)
+        return (size_t)capR * 4 + (size_t)count_head_slots(capR) * 8 + (size_t)capR * 2 + 16;
+    return join_smem_bytes(capR);
+}
 
-// Resident CTAs per SM at a table of capR rows, cached per (device, capR):
-// the occupancy query runs once per size.
-int join_ctas_per_sm(int capR) {
+// Resident CTAs per SM at a table of capR rows (counting: the bucket-chain
+// table of a counting join), cached per (device, capR, counting): the
+// occupancy query runs once per size.
+int join_ctas_per_sm(int capR, bool counting) {
     static std::mutex mu;
     static std::map<std::pair<int, int>, int> cache;
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> g(mu);
-    auto it = cache.find(std::make_pair(dev, capR));
+    const int key = counting ? -capR : capR;
+    auto it = cache.find(std::make_pair(dev, key));
     if (it != cache.end()) return it->second;
-    const size_t smem = join_smem_bytes(capR);
+    const size_t smem = join_launch_smem(capR, !counting, 0);
     int n = 0;
     if (smem_limit((const void *)k_join<false>, smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join<false>, JOIN_THREADS, smem) != cudaSuccess) {
@@ -152,12 +162,12 @@ int join_ctas_per_sm(int capR) {
         return 1;  // not cached: a later call retries
     }
     n = n < 1 ? 1 : n;
-    cache[std::make_pair(dev, capR)] = n;
+    cache[std::make_pair(dev, key)] = n;
     return n;
 }
 
 cudaError_t launch_join(const JoinArgs &a, bool materialize, int grid, cudaStream_t st) {
-    const size_t smem = join_smem_bytes(a.capR);
+    const size_t smem = join_launch_smem(a.capR, materialize, a.layout);
     auto kern = materialize ? k_join<true> : k_join<false>;
     cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;

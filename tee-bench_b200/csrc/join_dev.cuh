@@ -14,6 +14,18 @@ __host__ __device__ __forceinline__ uint32_t floor_pow2(uint32_t x) {
     return p;
 }
 
+// Bucket heads of a count-only bucket-chain table of capR rows: the largest
+// power of two <= capR + 2, divided by TBG_COUNT_HEAD_DIV (a build option for
+// A/B timing: fewer heads, longer chains, a smaller table and so more CTAs
+// per SM).
+#ifndef TBG_COUNT_HEAD_DIV
+#define TBG_COUNT_HEAD_DIV 1
+#endif
+__host__ __device__ __forceinline__ uint32_t count_head_slots(int capR) {
+    const uint32_t h = floor_pow2((uint32_t)capR + 2) / TBG_COUNT_HEAD_DIV;
+    return h ? h : 1;
+}
+
 // Packed bucket head of a count-only bucket-chain table: the head entry's
 // key, its 1-based row and its 1-based next link in one 64-bit word, so a
 // probe whose chain has one entry costs one shared load.
