@@ -334,16 +334,13 @@ int part_histogram(int rel, const RadixGeom &g, const Row *d, const tbg_config &
         ba.out = w.sc.as<Row>();
         ba.hist = hist.as<uint32_t>();
         ba.kept = w.kept.as<uint32_t>();
+        ba.hkept = bypass->hkept;
+        ba.hpairs = bypass->hpairs;
         ba.hkeys = bypass->keys;
         ba.hcnt = bypass->cnt;
         ba.scnt = bypass->scnt;
-        ba.hstart = bypass->start;
-        ba.rpay = bypass->rpay;
         ba.matches = &ctrl->matches;
         ba.heavy_rows = &ctrl->heavy_rows_S;
-        ba.rows_ctr = &ctrl->rows;
-        ba.rows = bypass->rows;
-        ba.cap = bypass->rows ? bypass->cap : 0;
         e = launch_hist_bypass(ba, cfg.materialize != 0, st);
     }
     if (e != cudaSuccess) return cuda_error(e, "histogram");

@@ -13,7 +13,11 @@
 //      bypass would not pay for its set-up and plain radix runs);
 //   4. with the bypass: build the heavy table, count (and, materialising,
 //      collect) R's heavy rows, radix partition R and the non-heavy rows of S
-//      (the S histogram joins heavy rows on the spot) and join the partitions.
+//      and join the partitions.  The S histogram takes the heavy rows out of
+//      S: counting, it counts them per key (matches = S rows x R rows per
+//      key); materialising, it sets them aside per chunk and totals their
+//      output rows, and k_heavy_emit writes their pairs on the main stream
+//      while S's kept rows are partitioned.
 // Steps 1-3 run on a second stream while R is partitioned, and the host reads
 // the decision back once.
 #include <algorithm>
@@ -61,7 +65,8 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
             (e = cudaStreamCreateWithPriority(&w.side, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&w.joined, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&w.table, cudaEventDisableTiming)) != cudaSuccess)
+            (e = cudaEventCreateWithFlags(&w.table, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&w.emit, cudaEventDisableTiming)) != cudaSuccess)
             return cuda_error(e, "stream");
     }
     cudaStream_t s2 = w.side;
@@ -93,6 +98,7 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     ENSURE(w.aux[6], (size_t)kCandCap * sizeof(HeavyCand));
     // heavy table: keys, R counts, starts, cursors, inserted count, S counts
     ENSURE(w.aux[7], (size_t)HEAVY_CAP * 4 * 5 + 16);
+    ENSURE(w.aux[5], (size_t)g.G[1] * (8 + 8 + 4) + 16);  // materialising: per chunk heavy pairs, bases, rows
 #undef ENSURE
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
     // main stream: R's partitioning needs nothing from the model
@@ -121,6 +127,9 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     unsigned *hcnt = hkeys + HEAVY_CAP, *hstart = hcnt + HEAVY_CAP, *hcur = hstart + HEAVY_CAP;
     unsigned *hinserted = hcur + HEAVY_CAP;
     unsigned *hscnt = hinserted + 4;  // S rows per heavy slot (counting joins)
+    unsigned long long *hpairs = w.aux[5].as<unsigned long long>();  // materialising, per S chunk
+    unsigned long long *hbase = hpairs + g.G[1];
+    uint32_t *hkeptc = reinterpret_cast<uint32_t *>(hbase + g.G[1]);
 
     if (timing) cudaEventRecord(w.ev[0], st);
     if ((e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st)) != cudaSuccess) return cuda_error(e, "memset");
@@ -172,11 +181,18 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
     if (bypass) {
         if ((e = launch_heavy_build(lb, hkeys, hinserted, s2)) != cudaSuccess)
             return cuda_error(e, "heavy build");
-        uint32_t *rpay = nullptr;
         if (mat) {
-            // the S histogram emits heavy pairs on the spot: R's heavy rows
-            // (counts, then payload lists of at most |R| entries) come first
+            // the S histogram totals each chunk's heavy output rows: R's rows
+            // per heavy key are counted first; their payload lists are built
+            // on the main stream meanwhile (after R's passes)
             if ((e = launch_heavy_r(dR, nR, hkeys, hcnt, nullptr, nullptr, nullptr, 0, w.nsm, s2)) !=
+                    cudaSuccess ||
+                (e = w.misc.ensure(std::max<uint64_t>(nR, 1) * 4 + 64)) != cudaSuccess)
+                return cuda_error(e, "heavy R");
+            if ((e = cudaEventRecord(w.table, s2)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(st, w.table, 0)) != cudaSuccess)
+                return cuda_error(e, "event");
+            if ((e = launch_heavy_r(dR, nR, hkeys, hcnt, hstart, hcur, w.misc.as<uint32_t>(), 1, w.nsm, st)) !=
                 cudaSuccess)
                 return cuda_error(e, "heavy R");
         } else {
@@ -189,28 +205,40 @@ int run_learned_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Ro
                 cudaSuccess)
                 return cuda_error(e, "heavy R");
         }
-        if (mat) {  // heavy R payload lists: at most |R| entries, so no count read-back
-            if ((e = w.misc.ensure(std::max<uint64_t>(nR, 1) * 4 + 64)) != cudaSuccess)
-                return cuda_error(e, "cudaMalloc");
-            rpay = w.misc.as<uint32_t>();
-            if ((e = launch_heavy_r(dR, nR, hkeys, hcnt, hstart, hcur, rpay, 1, w.nsm, s2)) != cudaSuccess)
-                return cuda_error(e, "heavy R");
-        }
         if ((e = cudaMemcpyAsync(&ctrl->heavy_keys, hinserted, 4, cudaMemcpyDeviceToDevice, s2)) != cudaSuccess)
             return cuda_error(e, "copy");
         bp.keys = hkeys;
         bp.cnt = hcnt;
         bp.scnt = hscnt;
-        bp.start = hstart;
-        bp.rpay = rpay;
-        bp.rows = d_rows;
-        bp.cap = d_rows ? cap : 0;
+        bp.hpairs = hpairs;
+        bp.hkept = hkeptc;
     } else {
         run->used_fallback = 1;  // no heavy mass: S is partitioned whole, as in RHO
     }
     if (timing) cudaEventRecord(w.ev[6], s2);
-    // S: histogram (joining heavy rows on the way), passes
+    // S: histogram (heavy rows joined or set aside on the way), passes
     if ((rc = part_histogram(1, g, dS, cfg, w, s2, bypass ? &bp : nullptr))) return rc;
+    if (bypass && mat) {
+        // the heavy pairs: output places reserved here, written on the main
+        // stream while S's kept rows are partitioned
+        HeavyEmitArgs ea;
+        ea.hs = w.sc.as<Row>();
+        ea.n = g.n[1];
+        ea.chunk = g.ch[1];
+        ea.G = g.G[1];
+        ea.hkept = hkeptc;
+        ea.hbase = hbase;
+        ea.hkeys = hkeys;
+        ea.hcnt = hcnt;
+        ea.hstart = hstart;
+        ea.rpay = w.misc.as<uint32_t>();
+        ea.rows = d_rows;
+        ea.cap = d_rows ? cap : 0;
+        if ((e = launch_heavy_plan(hpairs, g.G[1], hbase, &ctrl->rows, s2)) != cudaSuccess ||
+            (e = cudaEventRecord(w.emit, s2)) != cudaSuccess || (e = cudaStreamWaitEvent(st, w.emit, 0)) != cudaSuccess ||
+            (e = launch_heavy_emit(ea, w.nsm, st)) != cudaSuccess)
+            return cuda_error(e, "heavy pairs");
+    }
     if ((rc = part_pass(1, 1, g, dS, w, s2, bypass))) return rc;
     if ((rc = part_pass(1, 2, g, dS, w, s2, bypass))) return rc;
     if ((e = cudaEventRecord(w.joined, s2)) != cudaSuccess) return cuda_error(e, "event");

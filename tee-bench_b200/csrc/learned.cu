@@ -1106,17 +1106,21 @@ cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, unsig
 }
 
 // ---------------------------------------------------------------------------
-// S histogram with the heavy bypass: per chunk (as k_hist_chunks), rows whose
-// key is heavy are joined on the spot against the heavy table (count, or
-// rows out), every other row is counted in its radix bin and appended to
-// the chunk's region of the compacted S (warp-aggregated, coalesced).
+// S histogram with the heavy bypass: per chunk (as k_hist_chunks), every row
+// whose key is not heavy is counted in its radix bin and appended to the
+// chunk's region of the compacted S (warp-aggregated, coalesced).  Heavy rows
+// are joined without partitioning: counting, the kernel counts S rows per
+// heavy key (the matches are sum over keys of S rows x R rows, k_heavy_sum);
+// materialising, it appends them to the same region from the chunk's end
+// down and totals the output rows they make (R rows of their keys), and
+// k_heavy_emit writes the pairs while S's kept rows are partitioned.
 // ---------------------------------------------------------------------------
 // One row outside the vector body (the chunk's first row when it starts 8
 // bytes past a 16-byte boundary, or its last row): thread 0 only.
 template <bool MAT>
 __device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *hkeys, unsigned *hcnt, uint32_t *hist,
-                                unsigned *s_keep, uint2 *dst, Row x, unsigned long long &matches,
-                                unsigned &heavy_rows) {
+                                unsigned *s_keep, unsigned *s_heavy, uint2 *dst, uint2 *dst_end, Row x,
+                                unsigned long long &pairs, unsigned &heavy_rows) {
     const int s = heavy_lookup(hkeys, x.key);
     if (s < 0) {
         atomicAdd(&hist[radix_f(a.rf, x.key)], 1u);
@@ -1128,25 +1132,37 @@ __device__ void bypass_edge_row(const BypassArgs &a, const uint32_t *hkeys, unsi
         atomicAdd(&hcnt[s], 1u);
         return;
     }
-    const unsigned c = hcnt[s];
-    matches += c;
-    if (c) {
-        uint64_t op = atomicAdd(a.rows_ctr, (unsigned long long)c);
-        const unsigned st0 = a.hstart[s];
-        for (unsigned q = 0; q < c; q++, op++)
-            if (op < a.cap) a.rows[op] = tbg_row_out{x.key, a.rpay[st0 + q], x.payload};
-    }
+    pairs += hcnt[s];
+    dst_end[-1 - (int64_t)atomicAdd(s_heavy, 1u)] = make_uint2(x.key, x.payload);
 }
 
-// Materialising, hcnt holds R's rows per heavy slot and every heavy S row
-// emits its pairs on the spot.  Counting, it counts this block's S rows per
-// heavy slot instead (added to a.scnt at the end): the join's heavy matches
-// are sum_slot S rows x R rows, formed after R's heavy rows are counted on
-// the other stream (k_heavy_sum), so that count is off this kernel's path.
 // The next round's rows are loaded before the current round is processed
 // (one round of loads always in flight per thread).
 constexpr int BYP_THREADS = 1024;
 constexpr int BYP_U = 4;  // 16-byte row pairs per thread per round
+
+// Appends the rows of mask `sel` (bit j: row slot j of this lane) to a
+// warp-aggregated region: one ballot per row slot, one shared atomic per
+// warp on `ctr`; slot j's rows go to put(j, index).
+template <class Put>
+__device__ __forceinline__ void warp_append(unsigned sel, unsigned *ctr, Put put) {
+    const int lane = threadIdx.x & 31;
+    unsigned m[2 * BYP_U], wtot = 0;
+#pragma unroll
+    for (int j = 0; j < 2 * BYP_U; j++) {
+        m[j] = __ballot_sync(0xffffffffu, sel >> j & 1);
+        wtot += __popc(m[j]);
+    }
+    unsigned wb = 0;
+    if (lane == 0 && wtot) wb = atomicAdd(ctr, wtot);
+    wb = __shfl_sync(0xffffffffu, wb, 0);
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int j = 0; j < 2 * BYP_U; j++) {
+        if (sel >> j & 1) put(j, wb + __popc(m[j] & lt));
+        wb += __popc(m[j]);
+    }
+}
 
 template <bool MAT>
 __global__ void __launch_bounds__(BYP_THREADS, 1) k_hist_bypass(BypassArgs a) {
@@ -1154,31 +1170,33 @@ __global__ void __launch_bounds__(BYP_THREADS, 1) k_hist_bypass(BypassArgs a) {
     uint32_t *hkeys = reinterpret_cast<uint32_t *>(smem);  // 8-byte aligned buckets
     unsigned *hcnt = hkeys + HEAVY_CAP;
     uint32_t *hist = hcnt + HEAVY_CAP;
-    __shared__ unsigned s_keep;
-    __shared__ uint64_t scan_scratch[BYP_THREADS / 32 + 1];
+    __shared__ unsigned s_keep, s_heavy;
+    __shared__ unsigned long long s_pairs;
     const int tid = threadIdx.x, lane = tid & 31;
     for (int i = tid; i < a.nbins; i += BYP_THREADS) hist[i] = 0;
     for (int i = tid; i < HEAVY_CAP; i += BYP_THREADS) {
         hkeys[i] = a.hkeys[i];
         hcnt[i] = MAT ? a.hcnt[i] : 0u;
     }
-    if (tid == 0) s_keep = 0;
+    if (tid == 0) {
+        s_keep = 0;
+        s_heavy = 0;
+        s_pairs = 0;
+    }
     __syncthreads();
     const uint64_t lo = (uint64_t)blockIdx.x * a.chunk;
     const uint64_t hi = umin64(a.n, lo + a.chunk);
     const uint32_t len = hi > lo ? (uint32_t)(hi - lo) : 0u;  // a chunk holds < 2^32 rows
     const Row *src = a.in + lo;
     uint2 *dst = reinterpret_cast<uint2 *>(a.out + lo);
+    uint2 *dst_end = reinterpret_cast<uint2 *>(a.out + (lo + len));  // heavy rows, materialising
     const uint32_t head = (len && (reinterpret_cast<uintptr_t>(src) & 15)) ? 1u : 0u;
     const uint32_t npairs = (len - head) / 2;
     const bool tail = ((len - head) & 1) != 0;
     const uint4 *v = reinterpret_cast<const uint4 *>(src + head);
-    unsigned long long matches = 0;
+    unsigned long long pairs = 0;  // materialising: output rows of this thread's heavy rows
     unsigned heavy_rows = 0;
     constexpr uint32_t ROUND = BYP_U * BYP_THREADS;
-    // counting: the next round's loads go out before this round's work;
-    // materialising (more live state for the pair output) loads each round
-    constexpr bool PREFETCH = !MAT;
     uint4 nx[BYP_U];
     auto load_round = [&](uint32_t base) {
 #pragma unroll
@@ -1187,10 +1205,9 @@ __global__ void __launch_bounds__(BYP_THREADS, 1) k_hist_bypass(BypassArgs a) {
             nx[u] = p < npairs ? ldg_stream(v + p) : make_uint4(EMPTY_KEY, 0, EMPTY_KEY, 0);
         }
     };
-    if (PREFETCH) load_round(0);
+    load_round(0);
     // rounds of BYP_U row pairs per thread: pair p = base + u * BYP_THREADS + tid
     for (uint32_t base = 0; base < npairs; base += ROUND) {
-        if (!PREFETCH) load_round(base);
         uint32_t k[2 * BYP_U], pv[2 * BYP_U];
         unsigned valid = 0;
 #pragma unroll
@@ -1201,7 +1218,7 @@ __global__ void __launch_bounds__(BYP_THREADS, 1) k_hist_bypass(BypassArgs a) {
             pv[2 * u + 1] = nx[u].w;
             if (base + u * BYP_THREADS + tid < npairs) valid |= 3u << (2 * u);
         }
-        if (PREFETCH) load_round(base + ROUND);
+        load_round(base + ROUND);  // the next round's loads go out before this round's work
         int slot[2 * BYP_U];
         unsigned hm = 0;
 #pragma unroll
@@ -1215,64 +1232,46 @@ __global__ void __launch_bounds__(BYP_THREADS, 1) k_hist_bypass(BypassArgs a) {
             const bool dup = warp_has_dups((uint32_t)slot[0], hm & 1u);
 #pragma unroll
             for (int j = 0; j < 2 * BYP_U; j++) hist_add_warp(hcnt, (uint32_t)slot[j], hm >> j & 1, dup);
-        }
-        // coalesced compaction: one ballot per row slot, one shared atomic per warp
-        unsigned m[2 * BYP_U], wtot = 0;
-#pragma unroll
-        for (int j = 0; j < 2 * BYP_U; j++) {
-            m[j] = __ballot_sync(0xffffffffu, km >> j & 1);
-            wtot += __popc(m[j]);
-        }
-        unsigned wb = 0;
-        if (lane == 0 && wtot) wb = atomicAdd(&s_keep, wtot);
-        wb = __shfl_sync(0xffffffffu, wb, 0);
-        const unsigned lt = lanemask_lt();
-#pragma unroll
-        for (int j = 0; j < 2 * BYP_U; j++) {
-            if (km >> j & 1) {
-                atomicAdd(&hist[radix_f(a.rf, k[j])], 1u);
-                dst[wb + __popc(m[j] & lt)] = make_uint2(k[j], pv[j]);
-            }
-            wb += __popc(m[j]);
-        }
-        if (MAT) {
-            // heavy rows' output in (row slot, lane) order: coalesced stores
-            uint32_t c[2 * BYP_U];
-#pragma unroll
-            for (int j = 0; j < 2 * BYP_U; j++) c[j] = (hm >> j & 1) ? hcnt[slot[j]] : 0;
-#pragma unroll
-            for (int j = 0; j < 2 * BYP_U; j++) matches += c[j];
-            uint64_t pos[2 * BYP_U];
-            block_emit_positions<BYP_THREADS, 2 * BYP_U>(c, pos, a.rows_ctr, scan_scratch);
+        } else {  // heavy rows from the chunk's end down, and the output rows they make
 #pragma unroll
             for (int j = 0; j < 2 * BYP_U; j++) {
-                if (c[j]) {
-                    // R-row starts stay in global memory: only heavy rows read them
-                    const unsigned st0 = a.hstart[slot[j]];
-                    uint64_t op = pos[j];
-                    for (unsigned q = 0; q < c[j]; q++, op++)
-                        if (op < a.cap) a.rows[op] = tbg_row_out{k[j], a.rpay[st0 + q], pv[j]};
-                }
+                const unsigned c = hcnt[slot[j] >= 0 ? slot[j] : 0];
+                pairs += (hm >> j & 1) ? c : 0u;
             }
+            warp_append(hm, &s_heavy,
+                        [&](int j, unsigned i) { dst_end[-1 - (int64_t)i] = make_uint2(k[j], pv[j]); });
         }
+        // kept rows: counted in their radix bin and appended (coalesced)
+        warp_append(km, &s_keep, [&](int j, unsigned i) {
+            atomicAdd(&hist[radix_f(a.rf, k[j])], 1u);
+            dst[i] = make_uint2(k[j], pv[j]);
+        });
     }
-    __syncthreads();  // every vector row is counted: the edge rows take the next output slots
+    __syncthreads();  // every vector row is placed: the edge rows take the next slots
     if (tid == 0) {
-        if (head) bypass_edge_row<MAT>(a, hkeys, hcnt, hist, &s_keep, dst, src[0], matches, heavy_rows);
-        if (tail) bypass_edge_row<MAT>(a, hkeys, hcnt, hist, &s_keep, dst, src[len - 1], matches, heavy_rows);
+        if (head)
+            bypass_edge_row<MAT>(a, hkeys, hcnt, hist, &s_keep, &s_heavy, dst, dst_end, src[0], pairs, heavy_rows);
+        if (tail)
+            bypass_edge_row<MAT>(a, hkeys, hcnt, hist, &s_keep, &s_heavy, dst, dst_end, src[len - 1], pairs,
+                                 heavy_rows);
     }
+    const unsigned long long wp = warp_sum_u64(pairs), wh = warp_sum_u64((unsigned long long)heavy_rows);
+    if (MAT && lane == 0 && wp) atomicAdd(&s_pairs, wp);
     __syncthreads();
     uint32_t *hdst = a.hist + (uint64_t)blockIdx.x * a.nbins;
     for (int i = tid; i < a.nbins; i += BYP_THREADS) hdst[i] = hist[i];
     if (!MAT)
         for (int i = tid; i < HEAVY_CAP; i += BYP_THREADS)
             if (hcnt[i]) atomicAdd(&a.scnt[i], hcnt[i]);
-    if (tid == 0) a.kept[blockIdx.x] = s_keep;
-    const unsigned long long wm = warp_sum_u64(matches), wh = warp_sum_u64((unsigned long long)heavy_rows);
-    if (lane == 0) {
-        if (wm) atomicAdd(a.matches, wm);
-        if (wh) atomicAdd(a.heavy_rows, wh);
+    if (tid == 0) {
+        a.kept[blockIdx.x] = s_keep;
+        if (MAT) {
+            a.hkept[blockIdx.x] = s_heavy;
+            a.hpairs[blockIdx.x] = s_pairs;
+            if (s_pairs) atomicAdd(a.matches, s_pairs);
+        }
     }
+    if (lane == 0 && wh) atomicAdd(a.heavy_rows, wh);
 }
 
 // Heavy matches of a counting join: sum over slots of R rows x S rows.
@@ -1287,6 +1286,115 @@ __global__ void __launch_bounds__(1024) k_heavy_sum(const unsigned *__restrict__
 cudaError_t launch_heavy_sum(const unsigned *rcnt, const unsigned *scnt, unsigned long long *matches,
                              cudaStream_t st) {
     k_heavy_sum<<<1, 1024, 0, st>>>(rcnt, scnt, matches);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// First output row of each chunk's heavy pairs (one CTA): exclusive prefix
+// of the per-chunk totals, offset by one reservation of their sum.
+__global__ void __launch_bounds__(1024) k_heavy_plan(const unsigned long long *__restrict__ hpairs, int G,
+                                                    unsigned long long *hbase, unsigned long long *rows_ctr) {
+    __shared__ uint64_t scratch[1024 / 32 + 1];
+    __shared__ unsigned long long s_base;
+    const int per = (G + 1023) / 1024;
+    const int c0 = min(G, (int)threadIdx.x * per), c1 = min(G, c0 + per);
+    uint64_t sum = 0;
+    for (int c = c0; c < c1; c++) sum += hpairs[c];
+    uint64_t tot;
+    uint64_t run = block_excl_scan<1024>(sum, &tot, scratch);
+    if (threadIdx.x == 0) s_base = tot ? atomicAdd(rows_ctr, (unsigned long long)tot) : 0ull;
+    __syncthreads();
+    for (int c = c0; c < c1; c++) {
+        hbase[c] = s_base + run;
+        run += hpairs[c];
+    }
+}
+
+cudaError_t launch_heavy_plan(const unsigned long long *hpairs, int G, unsigned long long *hbase,
+                              unsigned long long *rows_ctr, cudaStream_t st) {
+    k_heavy_plan<<<1, 1024, 0, st>>>(hpairs, G, hbase, rows_ctr);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// The heavy pairs of a materialising bypass: CTA c reads chunk c's heavy S
+// rows (compacted from the chunk's end down), finds each key's slot in the
+// heavy table and writes one output row per R row of the key, at
+// hbase[c] + a place reserved by its warp (a shared atomic per warp and
+// round, no block barriers).  Chunk c's rows fill [hbase[c], hbase[c] +
+// hpairs[c]) exactly.  A key's first R payload comes from shared memory
+// when it has one R row (the common case: R a key permutation), else its
+// list in rpay.
+constexpr int EMIT_THREADS = 512;
+constexpr int EMIT_U = 4;  // heavy rows per thread per round
+
+__global__ void __launch_bounds__(EMIT_THREADS, 2) k_heavy_emit(HeavyEmitArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_he[];
+    uint32_t *hkeys = reinterpret_cast<uint32_t *>(smem_he);
+    unsigned *hcnt = hkeys + HEAVY_CAP;
+    unsigned *hstart = hcnt + HEAVY_CAP;
+    __shared__ unsigned long long s_next;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int i = tid; i < HEAVY_CAP; i += EMIT_THREADS) {
+        hkeys[i] = a.hkeys[i];
+        hcnt[i] = a.hcnt[i];
+        hstart[i] = a.hstart[i];
+    }
+    const int c = blockIdx.x;
+    if (tid == 0) s_next = a.hbase[c];
+    __syncthreads();
+    const uint64_t lo = (uint64_t)c * a.chunk;
+    const uint64_t end = umin64(a.n, lo + a.chunk);
+    const uint32_t nh = a.hkept[c];
+    const uint2 *src = reinterpret_cast<const uint2 *>(a.hs) + (end - nh);
+    constexpr uint32_t ROUND = EMIT_U * EMIT_THREADS;
+    for (uint32_t base = 0; base < nh; base += ROUND) {
+        uint2 x[EMIT_U];
+        uint32_t cnt[EMIT_U], st[EMIT_U];
+#pragma unroll
+        for (int u = 0; u < EMIT_U; u++) {
+            const uint32_t i = base + u * EMIT_THREADS + tid;
+            x[u] = i < nh ? ldg_stream(src + i) : make_uint2(EMPTY_KEY, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < EMIT_U; u++) {
+            const int s = heavy_lookup(hkeys, x[u].x);  // every compacted row is heavy; padding is not
+            cnt[u] = s >= 0 ? hcnt[s] : 0u;
+            st[u] = s >= 0 ? hstart[s] : 0u;
+        }
+        // places in (row slot, lane) order, so consecutive lanes store
+        // consecutive rows; one reservation per warp and round
+        uint32_t pre[EMIT_U], wsum = 0;
+#pragma unroll
+        for (int u = 0; u < EMIT_U; u++) {
+            uint32_t inc = cnt[u];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            pre[u] = wsum + inc - cnt[u];
+            wsum += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        unsigned long long wb = 0;
+        if (lane == 0 && wsum) wb = atomicAdd(&s_next, (unsigned long long)wsum);
+        wb = __shfl_sync(0xffffffffu, wb, 0);
+#pragma unroll
+        for (int u = 0; u < EMIT_U; u++) {
+            uint64_t op = wb + pre[u];
+            for (uint32_t q = 0; q < cnt[u]; q++, op++)
+                if (op < a.cap) a.rows[op] = tbg_row_out{x[u].x, a.rpay[st[u] + q], x[u].y};
+        }
+    }
+}
+
+cudaError_t launch_heavy_emit(const HeavyEmitArgs &a, int nsm, cudaStream_t st) {
+    (void)nsm;
+    if (!a.G) return cudaSuccess;
+    const size_t smem = (size_t)HEAVY_CAP * 4 * 3;
+    cudaError_t e = smem_limit((const void *)k_heavy_emit, smem);
+    if (e != cudaSuccess) return e;
+    k_heavy_emit<<<a.G, EMIT_THREADS, smem, st>>>(a);
     count_launch();
     return cudaGetLastError();
 }

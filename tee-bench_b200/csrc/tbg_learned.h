@@ -87,17 +87,31 @@ struct BypassArgs {
     int G;
     int nbins;
     RadixF rf;
-    Row *out;             // compacted S: chunk c's kept rows at [c * chunk, c * chunk + kept[c])
+    Row *out;             // compacted S: chunk c's kept rows at [c * chunk, c * chunk + kept[c]);
+                          // materialising, its heavy rows from the chunk's end down
     uint32_t *hist;       // [G][nbins]
     uint32_t *kept;       // [G]
+    uint32_t *hkept;      // materialising: [G] heavy rows of chunk c
+    unsigned long long *hpairs;  // materialising: [G] heavy output rows of chunk c
     const uint32_t *hkeys;
     const unsigned *hcnt;       // materialising: R rows per heavy slot
     unsigned *scnt;             // counting: S rows per heavy slot (added to)
-    const unsigned *hstart;
-    const uint32_t *rpay;
     unsigned long long *matches;
     unsigned long long *heavy_rows;
-    unsigned long long *rows_ctr;
+};
+
+// Output of a materialising bypass: heavy S rows (in the compacted S, from
+// each chunk's end down) paired with their keys' R rows.
+struct HeavyEmitArgs {
+    const Row *hs;              // the compacted S buffer
+    uint64_t n, chunk;
+    int G;
+    const uint32_t *hkept;      // [G] heavy rows of chunk c (at [end - hkept[c], end))
+    const unsigned long long *hbase;  // [G] first output row of chunk c
+    const uint32_t *hkeys;
+    const unsigned *hcnt;       // R rows per heavy slot
+    const unsigned *hstart;     // first of them in rpay
+    const uint32_t *rpay;
     tbg_row_out *rows;
     uint64_t cap;
 };
@@ -137,6 +151,11 @@ cudaError_t launch_heavy_r(const Row *R, uint64_t n, const uint32_t *keys, unsig
                            unsigned *start, unsigned *cur, uint32_t *rpay, int stage, int nsm, cudaStream_t st);
 cudaError_t launch_hist_bypass(const BypassArgs &a, bool mat, cudaStream_t st);
 cudaError_t launch_heavy_sum(const unsigned *rcnt, const unsigned *scnt, unsigned long long *matches, cudaStream_t st);
+// Exclusive prefix of the chunks' heavy output rows plus one reservation of
+// their total from rows_ctr: hbase[c] = first output row of chunk c.
+cudaError_t launch_heavy_plan(const unsigned long long *hpairs, int G, unsigned long long *hbase,
+                              unsigned long long *rows_ctr, cudaStream_t st);
+cudaError_t launch_heavy_emit(const HeavyEmitArgs &a, int nsm, cudaStream_t st);
 size_t bypass_smem(int nbins, bool mat);
 
 }  // namespace tbg

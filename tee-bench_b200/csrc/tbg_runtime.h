@@ -38,7 +38,7 @@ struct Workspace {
     void *host_small = nullptr;  // pinned HOST_SMALL_BYTES: mid-call read-backs (LRN's decision, shard totals)
     cudaEvent_t ev[8];
     cudaStream_t side = nullptr;       // second stream (learned path), created on first use
-    cudaEvent_t fork = nullptr, joined = nullptr, table = nullptr;
+    cudaEvent_t fork = nullptr, joined = nullptr, table = nullptr, emit = nullptr;
 };
 
 // What one join call did (for stats).
@@ -70,12 +70,10 @@ int finish_join(const tbg_config &cfg, Workspace &w, cudaStream_t st, const Join
 // Heavy-key table used by the S histogram of the learned path (device pointers).
 struct SBypass {
     const uint32_t *keys;
-    const unsigned *cnt;
-    unsigned *scnt;
-    const unsigned *start;
-    const uint32_t *rpay;
-    tbg_row_out *rows;
-    uint64_t cap;
+    const unsigned *cnt;           // R rows per heavy slot (materialising)
+    unsigned *scnt;                // S rows per heavy slot (counting)
+    uint32_t *hkept;               // materialising: [G] heavy S rows per chunk
+    unsigned long long *hpairs;    // materialising: [G] heavy output rows per chunk
 };
 struct RadixGeom {
     int B, passes, b1, b2;
