@@ -661,12 +661,13 @@ def main():
         # whole join: LRN's learning and bypass run on two streams and PSM's
         # sort passes are not radix passes, so the pipeline is the unit
         if algo == "PSM" and st.partitions:
-            # MSD sort: key range, histogram, radix passes by the top bits,
-            # one bucket-sort pass (its second read of a bucket comes from L2)
+            # MSD sort: R's key range, histogram (it checks S's keys against
+            # R's range), radix passes by the top bits, one bucket-sort pass
+            # (its re-reads of a bucket come from L2), merge
             sp = st.passes
-            alg = (8 + 8 + 16 * sp + 8) * rows
-            model = (f"PSM (MSD sort): key range 8 + histogram 8 + {sp - 1} radix passes x 16 + bucket sort 16 "
-                     f"+ merge read 8 B/row")
+            alg = 8 * nR + (8 + 16 * sp + 8) * rows
+            model = (f"PSM (MSD sort): R's key range 8 B per R row + histogram 8 + {sp - 1} radix passes x 16 + "
+                     f"bucket sort 16 + merge read 8 B/row")
         elif algo == "PSM":
             sp = st.passes or 4  # key-range read, per pass histogram read + scatter, merge read
             alg = (8 + 24 * sp + 8) * rows

@@ -322,7 +322,9 @@ int part_histogram(int rel, const RadixGeom &g, const Row *d, const tbg_config &
     DevBuf &base = rel ? w.baseS : w.baseR;
     cudaError_t e;
     if (!bypass) {
-        e = launch_hist_chunks(d, g.n[rel], g.ch[rel], g.G[rel], hist.as<uint32_t>(), g.B, g.rf, st);
+        const bool check = rel == 1 && g.s_range_max != 0xFFFFFFFFu;
+        e = launch_hist_chunks(d, g.n[rel], g.ch[rel], g.G[rel], hist.as<uint32_t>(), g.B, g.rf, st,
+                               check ? &ctrl->out_of_range : nullptr, g.s_range_max);
     } else {
         BypassArgs ba;
         ba.in = d;

@@ -47,9 +47,14 @@ using PassSmem = PartSmem<THREADS, PASS_NBUF>;
 // ---------------------------------------------------------------------------
 constexpr int HIST_THREADS = 1024;
 
+// With `oor` set, keys whose key - rf.sub exceeds range_max are also
+// counted into *oor (the histogram of a relation binned by another's key
+// range: a non-zero count means the bins are not valid).
 __global__ void __launch_bounds__(HIST_THREADS) k_hist_chunks(const Row *__restrict__ in, uint64_t n,
                                                              uint64_t chunk, uint32_t *__restrict__ hist,
-                                                             int nbins, RadixF rf) {
+                                                             int nbins, RadixF rf, unsigned long long *oor,
+                                                             uint32_t range_max) {
+    unsigned outside = 0;
     extern __shared__ uint32_t sh[];
     for (int i = threadIdx.x; i < nbins; i += HIST_THREADS) sh[i] = 0;
     __syncthreads();
@@ -76,6 +81,7 @@ __global__ void __launch_bounds__(HIST_THREADS) k_hist_chunks(const Row *__restr
             for (int u = 0; u < 4; u++) {
                 f[2 * u] = ok[u] ? radix_f(rf, x[u].x) : 0;
                 f[2 * u + 1] = ok[u] ? radix_f(rf, x[u].z) : 0;
+                if (oor && ok[u]) outside += (x[u].x - rf.sub > range_max) + (x[u].z - rf.sub > range_max);
             }
             const bool dup = warp_has_dups(f[0], ok[0]);
 #pragma unroll
@@ -85,9 +91,19 @@ __global__ void __launch_bounds__(HIST_THREADS) k_hist_chunks(const Row *__restr
             }
         }
         if (threadIdx.x == 0) {
-            if (head) atomicAdd(&sh[radix_f(rf, in[lo].key)], 1u);
-            if (body & 1) atomicAdd(&sh[radix_f(rf, in[hi - 1].key)], 1u);
+            if (head) {
+                atomicAdd(&sh[radix_f(rf, in[lo].key)], 1u);
+                outside += oor && in[lo].key - rf.sub > range_max;
+            }
+            if (body & 1) {
+                atomicAdd(&sh[radix_f(rf, in[hi - 1].key)], 1u);
+                outside += oor && in[hi - 1].key - rf.sub > range_max;
+            }
         }
+    }
+    if (oor) {
+        const unsigned long long wo = warp_sum_u64((unsigned long long)outside);
+        if ((threadIdx.x & 31) == 0 && wo) atomicAdd(oor, wo);
     }
     __syncthreads();
     uint32_t *dst = hist + (uint64_t)blockIdx.x * nbins;
@@ -371,12 +387,12 @@ int hist_ctas_per_sm(int P_log2) {
 }
 
 cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G, uint32_t *hist,
-                               int P_log2, RadixF rf, cudaStream_t st) {
+                               int P_log2, RadixF rf, cudaStream_t st, unsigned long long *oor, uint32_t range_max) {
     const int nbins = 1 << P_log2;
     const size_t smem = (size_t)nbins * 4;
     cudaError_t e = smem_limit((const void *)k_hist_chunks, smem);
     if (e != cudaSuccess) return e;
-    k_hist_chunks<<<G, HIST_THREADS, smem, st>>>(in, n, chunk, hist, nbins, rf);
+    k_hist_chunks<<<G, HIST_THREADS, smem, st>>>(in, n, chunk, hist, nbins, rf, oor, range_max);
     count_launch();
     return cudaGetLastError();
 }

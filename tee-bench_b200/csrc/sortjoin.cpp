@@ -130,27 +130,39 @@ cudaError_t launch_bucket_sort(const Row *in, Row *out, const uint64_t *base, ui
 static constexpr uint64_t kBucketMax = 1u << 20;
 static constexpr int kLowBits = 12, kLowBitsMax = 13;
 
+// With check_s, the range [sub, sub + 2^span) is R's alone: S's histogram
+// also counts S's keys outside it, and if there are any, nothing is sorted
+// and *s_outside is set (the caller then takes both relations' range).
 static int msd_sort(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *dS, uint64_t nS, uint32_t sub,
-                    int span, Row *sorted[2], bool msd_done[2], Workspace &w, cudaStream_t st, JoinRun *run) {
+                    int span, bool check_s, Row *sorted[2], bool msd_done[2], bool *s_outside, Workspace &w,
+                    cudaStream_t st, JoinRun *run) {
     msd_done[0] = msd_done[1] = false;
+    *s_outside = false;
     int lowbits = std::min(span, kLowBits), B = span - lowbits;
     if (B > 15) {
         B = 15;
         lowbits = span - B;
     }
     if (B < 1 || lowbits > kLowBitsMax) return TBG_OK;  // the LSD sort takes both
-    const RadixGeom g = radix_geometry_msd(nR, nS, sub, B, lowbits, w);
+    RadixGeom g = radix_geometry_msd(nR, nS, sub, B, lowbits, w);
+    if (check_s) g.s_range_max = (uint32_t)((1ull << span) - 1);
     int rc = ensure_radix_buffers(g, false, w);
     if (rc) return rc;
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(&ctrl->max_part_R, 0, 24, st)) != cudaSuccess) return cuda_error(e, "memset");
     if ((rc = part_histogram(0, g, dR, cfg, w, st, nullptr)) || (rc = part_histogram(1, g, dS, cfg, w, st, nullptr)))
         return rc;
-    // the largest bucket of each relation decides between this sort and LSD
+    // the largest bucket of each relation decides between this sort and LSD;
+    // S's keys outside R's range void the histograms
     unsigned long long *hm = static_cast<unsigned long long *>(w.host_small);
-    cudaError_t e;
-    if ((e = cudaMemcpyAsync(hm, &ctrl->max_part_R, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+    if ((e = cudaMemcpyAsync(hm, &ctrl->max_part_R, 24, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return cuda_error(e, "bucket sizes");
+    if (check_s && hm[2]) {
+        *s_outside = true;
+        return TBG_OK;
+    }
     const unsigned long long maxp[2] = {hm[0], hm[1]};
     const Row *in[2] = {dR, dS};
     for (int rel = 0; rel < 2; rel++) {
@@ -189,28 +201,46 @@ int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *d
 #undef ENSURE
     Ctrl *ctrl = w.ctrl.as<Ctrl>();
     uint32_t *mm = w.aux[4].as<uint32_t>();  // min, max of R's keys, then of S's
+    uint32_t *hm = static_cast<uint32_t *>(w.host_small);
     mark_ev(w, timing, 0, st);
     if ((e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st)) != cudaSuccess) return cuda_error(e, "memset");
-    if ((e = launch_key_range(dR, nR, mm, w.nsm, st)) != cudaSuccess ||
-        (e = launch_key_range(dS, nS, mm + 2, w.nsm, st)) != cudaSuccess)
-        return cuda_error(e, "key range");
-    // the key ranges decide the passes and so the buffer chain: read them back
-    uint32_t *hm = static_cast<uint32_t *>(w.host_small);
-    if ((e = cudaMemcpyAsync(hm, mm, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(st)) != cudaSuccess)
-        return cuda_error(e, "key range");
-    const uint32_t rmin = hm[0], rmax = hm[1], smin = hm[2], smax = hm[3];
+    // R's key range decides the MSD geometry (S's keys usually lie inside it:
+    // S's histogram checks that, so S's own range read is only needed when
+    // they do not, or for the LSD sort)
+    uint32_t rmin = 0, rmax = 0, smin = 0, smax = 0;
+    bool have_s = false;
+    auto read_range = [&](const Row *d, uint64_t n, uint32_t *lo, uint32_t *hi) -> int {
+        if ((e = launch_key_range(d, n, mm, w.nsm, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(hm, mm, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return cuda_error(e, "key range");
+        *lo = hm[0];
+        *hi = hm[1];
+        return TBG_OK;
+    };
+    auto span_of = [](uint32_t lo, uint32_t hi) { return hi > lo ? 32 - __builtin_clz(hi - lo) : 0; };
+    int rc = read_range(dR, nR, &rmin, &rmax);
+    if (rc) return rc;
     mark_ev(w, timing, 1, st);
-    // MSD sort over the keys of both relations (empty relations have min > max)
-    const uint32_t lo = std::min(nR ? rmin : smin, nS ? smin : rmin), hi = std::max(nR ? rmax : smax, nS ? smax : rmax);
-    const int span = (nR || nS) && hi > lo ? 32 - __builtin_clz(hi - lo) : 0;
     Row *sorted[2] = {w.aux[0].as<Row>(), w.aux[2].as<Row>()};
     bool msd_done[2] = {false, false};
     run->B = 8;
     run->P = 0;
     run->passes = 0;
-    int rc = nR && nS ? msd_sort(cfg, dR, nR, dS, nS, lo, span, sorted, msd_done, w, st, run) : TBG_OK;
-    if (rc) return rc;
+    if (nR && nS) {
+        bool s_outside = false;
+        if ((rc = msd_sort(cfg, dR, nR, dS, nS, rmin, span_of(rmin, rmax), true, sorted, msd_done, &s_outside, w, st,
+                           run)))
+            return rc;
+        if (s_outside) {  // both relations' range, histograms again
+            if ((rc = read_range(dS, nS, &smin, &smax))) return rc;
+            have_s = true;
+            const uint32_t lo = std::min(rmin, smin), hi = std::max(rmax, smax);
+            if ((rc = msd_sort(cfg, dR, nR, dS, nS, lo, span_of(lo, hi), false, sorted, msd_done, &s_outside, w,
+                               st, run)))
+                return rc;
+        }
+    }
     const Row *sR = sorted[0], *sS = sorted[1];
     int pr = 0, ps = 0;
     if (!msd_done[0]) {
@@ -218,6 +248,7 @@ int run_psm_join(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row *d
         mark_ev(w, timing, 2, st);
     }
     if (!msd_done[1]) {
+        if (!have_s && (rc = read_range(dS, nS, &smin, &smax))) return rc;
         if ((rc = lsd_sort_chunked(dS, nS, smin, smax, w.aux[2], w.aux[3], w, st, &sS, &ps))) return rc;
         mark_ev(w, timing, 3, st);
     }

@@ -36,10 +36,11 @@ struct Ctrl {
     unsigned int tiles[16];       // tile tickets, one slot per scatter launch
     unsigned int item_ctr[4];     // work-item tickets, one slot per join launch
     unsigned long long max_part_R, max_part_S;
+    unsigned long long out_of_range;  // keys a range-checked histogram found outside its range
     unsigned long long nonempty;  // partitions with both sides non-empty
     unsigned long long heavy_rows_S;
     unsigned long long heavy_keys;
-    unsigned long long pad[4];
+    unsigned long long pad[3];
 };
 
 // Digits per pass of the tile scatter (part_dev.cuh).
@@ -139,7 +140,8 @@ struct PlanArgs {
 
 // ---- launchers (partition.cu, join.cu, gen.cu) ----
 cudaError_t launch_hist_chunks(const Row *in, uint64_t n, uint64_t chunk, int G, uint32_t *hist,
-                               int P_log2, RadixF rf, cudaStream_t st);
+                               int P_log2, RadixF rf, cudaStream_t st,
+                               unsigned long long *out_of_range = nullptr, uint32_t range_max = 0);
 cudaError_t launch_colscan(uint32_t *hist, int G, int P, uint32_t *totals, cudaStream_t st);
 cudaError_t launch_plan(const PlanArgs &a, cudaStream_t st);
 cudaError_t launch_plan_bases(const uint32_t *totals, uint64_t *base, int P_log2, unsigned long long *maxp,

@@ -85,6 +85,9 @@ struct RadixGeom {
     uint64_t n[2];     // rows of R, S
     RadixF rf;         // final partition f of a key (histograms)
     DigitOp d1, d2;    // pass-1 and pass-2 digits: f = d1 << b2 | d2
+    // S's histogram also counts keys with key - rf.sub > s_range_max into
+    // ctrl->out_of_range (S binned by R's key range); 0xFFFFFFFF: no check
+    uint32_t s_range_max = 0xFFFFFFFFu;
 };
 RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int capR, Workspace &w);
 RadixGeom radix_geometry_msd(uint64_t nR, uint64_t nS, uint32_t sub, int B, int lowbits, Workspace &w);

@@ -310,6 +310,31 @@ def test_psm_heavy_key_takes_lsd(tbg, oracle, cuda, materialize):
 
 
 @pytest.mark.parametrize("materialize", [False, True])
+def test_psm_s_keys_outside_r_range(tbg, oracle, cuda, materialize):
+    """PSM first bins both relations by R's key range; S keys below and above
+    it send the sort back to both relations' range.  Count and rows match
+    the oracle."""
+    rng = np.random.default_rng(7)
+    R = np.zeros(200003, dtype=oracle.ROW)
+    S = np.zeros(500009, dtype=oracle.ROW)
+    R["key"] = rng.integers(1 << 20, 1 << 22, len(R)).astype(np.uint32)
+    inside = R["key"][rng.integers(0, len(R), len(S))]
+    anywhere = rng.integers(0, 1 << 24, len(S)).astype(np.uint32)
+    S["key"] = np.where(rng.random(len(S)) < 0.8, inside, anywhere)
+    assert S["key"].min() < R["key"].min() and S["key"].max() > R["key"].max()
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref, ref_rows = oracle.rho(R, S, materialize=True)
+    if materialize:
+        m, rows, _ = run_join(tbg, cuda, "PSM", R, S, materialize=True, cap=ref)
+        assert m == ref
+        assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+    else:
+        m, _, _ = run_join(tbg, cuda, "PSM", R, S)
+        assert m == ref
+
+
+@pytest.mark.parametrize("materialize", [False, True])
 def test_rsm_wide_key_spans(tbg, oracle, cuda, materialize):
     """Full-range 32-bit keys: inside a radix partition the varying key bits
     span more than the 12 a single counting pass sorts, so every tile takes
