@@ -510,22 +510,85 @@ __device__ __forceinline__ uint32_t merge_count(const uint32_t *A, uint32_t na, 
 }
 
 constexpr uint32_t RSM_KEYS = skewed_size<uint32_t>(RSM_STILE);
+// S tiles of the ranged counting sort (below) and the bins it ranks on.
+constexpr uint32_t RSM_SBIG = RSM_STILE * 4;
+constexpr uint32_t RSM_SBIG_KEYS = skewed_size<uint32_t>(RSM_SBIG);
+constexpr uint32_t RSM_BINS = 1u << COUNT_SORT_BITS;
+// the per-tile path reuses the S buffer: 4096 sorted keys, the sort's
+// scratch keys and its 16-bit counters
+static_assert(2 * RSM_KEYS + 256 * (RSM_THREADS / 32) / 2 <= RSM_SBIG_KEYS, "per-tile buffers fit the S buffer");
 
-size_t rsm_count_smem_bytes() { return (size_t)3 * RSM_KEYS * 4 + 256 * (RSM_THREADS / 32) * 2; }
+size_t rsm_count_smem_bytes() { return (size_t)(RSM_KEYS + RSM_SBIG_KEYS + RSM_BINS) * 4; }
 
-// Count-only RSM for items with r_len <= RSM_STILE: the R chunk's keys are
-// sorted once, then S tiles of RSM_STILE keys are sorted and merged against
-// them; tile k + 1's keys load while tile k merges.
+// One read of S rows [off, off + ns) for the ranged counting sort.  Rows whose
+// key lies in [rmin, rmin + rspan] (R's key range) have the digit
+// (key - rmin) >> shift: RANK false counts the digits, RANK true takes each
+// row's slot from its digit's running offset and stores the key there.  Rows
+// outside R's range cannot match and stay out of the sorted tile.  All keys of
+// a work item share their low `shift` bits (the partition's radix), so keys
+// in range have distinct digits for distinct values and the slots sort them;
+// equal keys sit in any order among themselves.  The counting read keeps S in
+// L2 (ld.global.cg) for the ranking read, which streams it (ld.global.cs).
+template <bool RANK>
+__device__ __forceinline__ void rsm_ranged_pass(const Row *__restrict__ S, uint64_t off, uint32_t ns, uint32_t rmin,
+                                                uint32_t rspan, int shift, uint32_t *cnt, uint32_t *Sk) {
+    const uint2 *v = reinterpret_cast<const uint2 *>(S) + off;
+    constexpr uint32_t BATCH = RSM_THREADS * 8;
+    for (uint32_t b0 = 0; b0 < ns; b0 += BATCH) {
+        uint32_t k[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint32_t e = b0 + i * RSM_THREADS + threadIdx.x;
+            k[i] = 0;
+            if (e < ns) k[i] = RANK ? __ldcs(v + e).x : __ldcg(v + e).x;
+        }
+        const bool dup = warp_has_dups((k[0] - rmin) >> shift, b0 + threadIdx.x < ns && k[0] - rmin <= rspan);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint32_t dk = k[i] - rmin;
+            const bool in = b0 + i * RSM_THREADS + threadIdx.x < ns && dk <= rspan;
+            const uint32_t slot = rank_warp(cnt, in ? dk >> shift : 0u, in, dup);
+            if (RANK && in) Sk[skew<uint32_t>(slot)] = k[i];
+        }
+    }
+}
+
+// cnt[0, bins) -> exclusive offsets in place; returns the total.  Ends with
+// the counters written but not yet synchronised.
+__device__ __forceinline__ uint32_t rsm_scan_bins(uint32_t *cnt, uint32_t bins, uint64_t *scratch) {
+    const uint32_t per = (bins + RSM_THREADS - 1) / RSM_THREADS;
+    const uint32_t b0 = min(bins, threadIdx.x * per), b1 = min(bins, b0 + per);
+    uint32_t sum = 0;
+    for (uint32_t b = b0; b < b1; b++) sum += cnt[b];
+    uint64_t tot;
+    uint32_t run = (uint32_t)block_excl_scan<RSM_THREADS>(sum, &tot, scratch);
+    for (uint32_t b = b0; b < b1; b++) {
+        const uint32_t c = cnt[b];
+        cnt[b] = run;
+        run += c;
+    }
+    return (uint32_t)tot;
+}
+
+// Count-only RSM for items with r_len <= RSM_STILE.  The R chunk's keys are
+// sorted once (sort_keys).  When R's keys span at most RSM_BINS digits above
+// the partition's radix bits, S is sorted in tiles of RSM_SBIG rows by the
+// ranged counting sort (a counting read, a scan of the bins, a ranking read
+// that places the keys) and each sorted tile is merged against R.  Otherwise
+// S tiles of RSM_STILE keys are sorted by sort_keys, tile k + 1's keys
+// loading while tile k merges.
 __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t *Rk = reinterpret_cast<uint32_t *>(smem);
     uint32_t *Sk = Rk + RSM_KEYS;
-    uint32_t *tmp = Sk + RSM_KEYS;
+    uint32_t *bins_cnt = Sk + RSM_SBIG_KEYS;
+    uint32_t *tmp = Sk + RSM_KEYS;  // per-tile sorts: scratch keys and counters inside the S buffer
     uint16_t *cnt = reinterpret_cast<uint16_t *>(tmp + RSM_KEYS);
     __shared__ uint32_t s_item;
     __shared__ uint64_t scan_scratch[RSM_THREADS / 32 + 1];
     __shared__ uint32_t red[2];
     const int tid = threadIdx.x;
+    const int shift = a.hash_shift;
     const unsigned nitems = *a.err ? 0u : *a.nitems;  // a planner error leaves the item list unusable
     unsigned long long local = 0;
     uint32_t key[8];
@@ -536,8 +599,28 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
         if (it >= nitems) break;
         const Item m = a.items[it];
         const uint32_t nr = min(m.r_len, (uint32_t)RSM_STILE);  // the planner's capR is RSM_STILE
+        __syncthreads();  // s_item read by every thread before thread 0 rewrites it
+        if (nr == 0 || m.s_len == 0) continue;
         load_keys<RSM_THREADS>(a.R, m.r_off, nr, key);
         sort_keys<RSM_THREADS>(key, nr, Rk, tmp, cnt, scan_scratch, red);
+        const uint32_t rmin = Rk[0], rspan = Rk[skew<uint32_t>(nr - 1)] - rmin;
+        if ((rspan >> shift) < RSM_BINS) {
+            const uint32_t bins = (rspan >> shift) + 1;
+            for (uint64_t s0 = 0; s0 < m.s_len; s0 += RSM_SBIG) {
+                const uint32_t ns = (uint32_t)umin64(RSM_SBIG, m.s_len - s0);
+                for (uint32_t b = tid; b < bins; b += RSM_THREADS) bins_cnt[b] = 0;
+                __syncthreads();
+                rsm_ranged_pass<false>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
+                __syncthreads();
+                const uint32_t nin = rsm_scan_bins(bins_cnt, bins, scan_scratch);
+                __syncthreads();
+                rsm_ranged_pass<true>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
+                __syncthreads();
+                local += merge_count<RSM_THREADS>(Rk, nr, Sk, nin);
+                __syncthreads();  // Sk and the bins are rewritten by the next tile
+            }
+            continue;
+        }
         uint32_t ns = (uint32_t)umin64(RSM_STILE, m.s_len);
         load_keys<RSM_THREADS>(a.S, m.s_off, ns, key);
         for (uint64_t s0 = 0; s0 < m.s_len;) {

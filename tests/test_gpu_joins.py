@@ -357,6 +357,32 @@ def test_rsm_wide_key_spans(tbg, oracle, cuda, materialize):
         assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
 
 
+@pytest.mark.parametrize("case", ["fk_half_outside", "zipf_s", "dup_r"])
+def test_rsm_ranged_counting_sort(tbg, oracle, cuda, case):
+    """Count-only RSM's ranged counting sort: R's keys in a partition span at
+    most 4096 digits above the radix bits, so S is sorted in tiles of 16384
+    rows ranked against R's key range.  Partitions hold about 32K S rows (two
+    tiles and a ragged one); S keys outside R's range (below and above it)
+    drop out of the sorted tiles; a Zipf S puts runs of one key in a warp;
+    duplicate R keys make runs on both sides."""
+    rng = np.random.default_rng(41)
+    nR, nS = 1 << 20, (1 << 23) + 4099
+    R = np.zeros(nR, dtype=oracle.ROW)
+    S = np.zeros(nS, dtype=oracle.ROW)
+    R["key"] = rng.permutation(np.arange(1, nR + 1, dtype=np.uint32)) + 1000
+    if case == "dup_r":
+        R["key"][: nR // 4] = R["key"][nR // 4: nR // 2]
+    if case == "zipf_s":
+        S["key"] = np.minimum(rng.zipf(1.3, nS), nR).astype(np.uint32) + 1000
+    else:
+        S["key"] = rng.integers(0, 2 * nR, nS).astype(np.uint32)
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    ref = oracle.rho(R, S)
+    m, _, _ = run_join(tbg, cuda, "RSM", R, S)
+    assert m == ref
+
+
 @pytest.mark.parametrize("algo", ["RSM", "PSM"])
 def test_sortmerge_duplicates_both_sides(tbg, oracle, cuda, algo):
     """Runs of equal keys on both sides, spanning merge tiles and partitions."""
