@@ -470,8 +470,12 @@ __device__ void sort_keys(const uint32_t (&key)[8], uint32_t n, uint32_t *out, u
     __syncthreads();
 }
 
-// Matches of this thread's share of the merge path of sorted keys A (na)
-// and B (nb), skewed 4-byte layout: B's rows count the run of equal A keys.
+// Matches of this thread's share of the merge path of sorted keys A (na, the
+// R chunk) and B (nb, an S tile), skewed 4-byte layout.  Here the merged
+// order takes A[i] before B[j] iff A[i] <= B[j], so when B[j] is taken every
+// A key equal to it is behind: `run` counts the A keys equal to the last A
+// key taken (`pk`), and B[j] matches run of them when its key is pk.  No
+// step walks a run of equal keys, so the steps cost the same under skew.
 template <int THREADS>
 __device__ __forceinline__ uint32_t merge_count(const uint32_t *A, uint32_t na, const uint32_t *B, uint32_t nb) {
     const uint32_t L = na + nb;
@@ -482,27 +486,39 @@ __device__ __forceinline__ uint32_t merge_count(const uint32_t *A, uint32_t na, 
     uint32_t lo = d0 > nb ? d0 - nb : 0, hi = min(d0, na);
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (ka(mid) < kb(d0 - mid - 1)) lo = mid + 1;
+        if (ka(mid) <= kb(d0 - mid - 1)) lo = mid + 1;
         else hi = mid;
+    }
+    uint32_t i = lo, j = d0 - lo;
+    uint32_t pk = 0, run = 0;  // with no A key behind, run 0 matches nothing
+    if (i > 0 && d0 < d1) {
+        // the A keys equal to A[i - 1] end at i - 1: a short walk back, then
+        // a binary search for the first of them
+        pk = ka(i - 1);
+        uint32_t q = i - 1;
+        for (int w = 0; w < 4 && q > 0 && ka(q - 1) == pk; w++) q--;
+        if (q > 0 && ka(q - 1) == pk) {
+            uint32_t l = 0, h = q - 1;
+            while (l < h) {
+                const uint32_t m = (l + h) >> 1;
+                if (ka(m) < pk) l = m + 1;
+                else h = m;
+            }
+            q = l;
+        }
+        run = i - q;
     }
     // the current keys stay in registers; at a side's end they read the
     // padding slot past its last key (inside the buffer, never used)
-    uint32_t i = lo, j = d0 - lo;
     uint32_t ak = ka(i), bk = kb(j);
-    uint32_t cnt = 0, last_key = 0, last_cnt = 0;
-    bool have = false;
+    uint32_t cnt = 0;
     for (uint32_t d = d0; d < d1; d++) {
-        if (i < na && (j >= nb || ak < bk)) {
+        if (i < na && (j >= nb || ak <= bk)) {
+            run = ak == pk ? run + 1 : 1;
+            pk = ak;
             ak = ka(++i);
         } else {
-            if (!have || bk != last_key) {
-                last_cnt = 0;
-                if (i < na && ak == bk)
-                    for (uint32_t q = i; q < na && ka(q) == bk; q++) last_cnt++;
-                last_key = bk;
-                have = true;
-            }
-            cnt += last_cnt;
+            if (bk == pk) cnt += run;
             bk = kb(++j);
         }
     }
@@ -529,24 +545,26 @@ size_t rsm_count_smem_bytes() { return (size_t)(RSM_KEYS + RSM_SBIG_KEYS + RSM_B
 // in range have distinct digits for distinct values and the slots sort them;
 // equal keys sit in any order among themselves.  The counting read keeps S in
 // L2 (ld.global.cg) for the ranking read, which streams it (ld.global.cs).
-template <bool RANK>
+template <bool RANK, bool FULL>
 __device__ __forceinline__ void rsm_ranged_pass(const Row *__restrict__ S, uint64_t off, uint32_t ns, uint32_t rmin,
                                                 uint32_t rspan, int shift, uint32_t *cnt, uint32_t *Sk) {
     const uint2 *v = reinterpret_cast<const uint2 *>(S) + off;
     constexpr uint32_t BATCH = RSM_THREADS * 8;
+    if (FULL) ns = RSM_SBIG;
     for (uint32_t b0 = 0; b0 < ns; b0 += BATCH) {
         uint32_t k[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const uint32_t e = b0 + i * RSM_THREADS + threadIdx.x;
             k[i] = 0;
-            if (e < ns) k[i] = RANK ? __ldcs(v + e).x : __ldcg(v + e).x;
+            if (FULL || e < ns) k[i] = RANK ? __ldcs(v + e).x : __ldcg(v + e).x;
         }
-        const bool dup = warp_has_dups((k[0] - rmin) >> shift, b0 + threadIdx.x < ns && k[0] - rmin <= rspan);
+        const bool dup =
+            warp_has_dups((k[0] - rmin) >> shift, (FULL || b0 + threadIdx.x < ns) && k[0] - rmin <= rspan);
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const uint32_t dk = k[i] - rmin;
-            const bool in = b0 + i * RSM_THREADS + threadIdx.x < ns && dk <= rspan;
+            const bool in = (FULL || b0 + i * RSM_THREADS + threadIdx.x < ns) && dk <= rspan;
             const uint32_t slot = rank_warp(cnt, in ? dk >> shift : 0u, in, dup);
             if (RANK && in) Sk[skew<uint32_t>(slot)] = k[i];
         }
@@ -610,11 +628,13 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
                 const uint32_t ns = (uint32_t)umin64(RSM_SBIG, m.s_len - s0);
                 for (uint32_t b = tid; b < bins; b += RSM_THREADS) bins_cnt[b] = 0;
                 __syncthreads();
-                rsm_ranged_pass<false>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
+                if (ns == RSM_SBIG) rsm_ranged_pass<false, true>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
+                else rsm_ranged_pass<false, false>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
                 __syncthreads();
                 const uint32_t nin = rsm_scan_bins(bins_cnt, bins, scan_scratch);
                 __syncthreads();
-                rsm_ranged_pass<true>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
+                if (ns == RSM_SBIG) rsm_ranged_pass<true, true>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
+                else rsm_ranged_pass<true, false>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
                 __syncthreads();
                 local += merge_count<RSM_THREADS>(Rk, nr, Sk, nin);
                 __syncthreads();  // Sk and the bins are rewritten by the next tile
