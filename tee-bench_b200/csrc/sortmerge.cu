@@ -249,12 +249,13 @@ __device__ uint64_t *load_sorted(const Row *__restrict__ src, uint64_t off, uint
 // Merge-path split of diagonal d over sorted arrays A (na) and B (nb):
 // the number of A elements among the first d of the merged order, where A[i]
 // precedes B[j] iff key(A[i]) < key(B[j]).
-template <class GetA, class GetB>
+// With A_FIRST, A[i] precedes B[j] iff key(A[i]) <= key(B[j]) instead.
+template <bool A_FIRST = false, class GetA, class GetB>
 __device__ __forceinline__ uint64_t merge_split(uint64_t d, uint64_t na, uint64_t nb, GetA ka, GetB kb) {
     uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
     while (lo < hi) {
         const uint64_t mid = (lo + hi) >> 1;
-        if (ka(mid) < kb(d - mid - 1)) lo = mid + 1;
+        if (A_FIRST ? ka(mid) <= kb(d - mid - 1) : ka(mid) < kb(d - mid - 1)) lo = mid + 1;
         else hi = mid;
     }
     return lo;
@@ -761,6 +762,7 @@ constexpr int MERGE_THREADS = TBG_MERGE_THREADS;
 constexpr int MERGE_PER_THREAD = TBG_MERGE_PER_THREAD;
 constexpr int MERGE_TILE = MERGE_THREADS * MERGE_PER_THREAD;
 
+template <bool A_FIRST>
 __global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row *__restrict__ S, uint64_t ns,
                                uint64_t *__restrict__ splits, uint64_t nsplits) {
     const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -768,7 +770,101 @@ __global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row
     const uint64_t d = umin64(nr + ns, c * MERGE_TILE);
     auto kr = [&](uint64_t i) { return R[i].key; };
     auto ks = [&](uint64_t j) { return S[j].key; };
-    splits[c] = merge_split(d, nr, ns, kr, ks);
+    splits[c] = merge_split<A_FIRST>(d, nr, ns, kr, ks);
+}
+
+// Count-only merge join.  The merged order takes R[i] before S[j] iff
+// R[i].key <= S[j].key, so when S[j] is taken every R row of its key is
+// behind it (in this tile or an earlier one): each thread keeps the last R
+// key taken and the number of R rows with that key (`run`), and S[j] adds
+// run when its key is that key.  A thread finds the run it starts inside once,
+// walking back (into global memory before the tile's first R row when the run
+// starts earlier); the steps themselves never walk a run.  Keys sit in shared
+// memory at t + t / 16, so threads whose walks start 16 apart use different
+// banks.
+__device__ __forceinline__ uint32_t mskew(uint32_t t) { return t + (t >> 4); }
+constexpr uint32_t mskew_host(uint32_t t) { return t + (t >> 4); }
+
+__global__ void __launch_bounds__(MERGE_THREADS, 8) k_merge_count(const Row *__restrict__ R, uint64_t nr,
+                                                                const Row *__restrict__ S, uint64_t ns,
+                                                                const uint64_t *__restrict__ splits,
+                                                                unsigned long long *matches) {
+    extern __shared__ __align__(16) uint32_t merge_smem[];
+    uint32_t *K = merge_smem;  // mskew(MERGE_TILE) + 1 keys: R's, then S's, and a spare slot
+    const uint64_t L = nr + ns;
+    const uint64_t c = blockIdx.x;
+    const uint64_t dc0 = c * MERGE_TILE, dc1 = umin64(L, dc0 + MERGE_TILE);
+    const uint64_t ic0 = splits[c], ic1 = splits[c + 1];
+    const uint64_t jc0 = dc0 - ic0, jc1 = dc1 - ic1;
+    const uint32_t nrt = (uint32_t)(ic1 - ic0), nst = (uint32_t)(jc1 - jc0);
+    const uint32_t Lt = nrt + nst;
+    {
+        const uint2 *Rv = reinterpret_cast<const uint2 *>(R) + ic0;
+        const uint2 *Sv = reinterpret_cast<const uint2 *>(S) + jc0;
+        uint32_t x[MERGE_PER_THREAD];
+#pragma unroll
+        for (int q = 0; q < MERGE_PER_THREAD; q++) {
+            const uint32_t t = q * MERGE_THREADS + threadIdx.x;
+            if (t < Lt) x[q] = __ldcs(t < nrt ? Rv + t : Sv + (t - nrt)).x;
+        }
+#pragma unroll
+        for (int q = 0; q < MERGE_PER_THREAD; q++) {
+            const uint32_t t = q * MERGE_THREADS + threadIdx.x;
+            if (t < Lt) K[mskew(t)] = x[q];
+        }
+        if (threadIdx.x == 0) K[mskew(Lt)] = 0;
+    }
+    __syncthreads();
+    auto kr = [&](uint32_t i) { return K[mskew(i)]; };
+    auto ks = [&](uint32_t j) { return K[mskew(nrt + j)]; };
+    const uint32_t d0 = min(Lt, threadIdx.x * MERGE_PER_THREAD), d1 = min(Lt, d0 + MERGE_PER_THREAD);
+    uint32_t i;
+    {
+        uint32_t lo = d0 > nst ? d0 - nst : 0, hi = min(d0, nrt);
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (kr(mid) <= ks(d0 - mid - 1)) lo = mid + 1;
+            else hi = mid;
+        }
+        i = lo;
+    }
+    uint32_t j = d0 - i;
+    uint32_t pk = 0;
+    uint64_t run = 0;  // with no R row behind, run 0 matches nothing
+    const uint64_t gi = ic0 + i;
+    if (gi > 0 && d0 < d1) {
+        // the R rows of key R[gi - 1] end at gi - 1: find the first of them
+        auto rkey = [&](uint64_t g) { return g >= ic0 ? kr((uint32_t)(g - ic0)) : R[g].key; };
+        pk = rkey(gi - 1);
+        uint64_t q = gi - 1;
+        for (int w = 0; w < 4 && q > 0 && rkey(q - 1) == pk; w++) q--;
+        if (q > 0 && rkey(q - 1) == pk) {
+            uint64_t l = 0, h = q - 1;
+            while (l < h) {
+                const uint64_t m = (l + h) >> 1;
+                if (rkey(m) < pk) l = m + 1;
+                else h = m;
+            }
+            q = l;
+        }
+        run = gi - q;
+    }
+    // current keys in registers; past a side's end they read the next slot
+    // (the other side's first key or the spare), which the bounds keep unused
+    uint32_t rk = kr(i), sk = ks(j);
+    unsigned long long cnt = 0;
+    for (uint32_t d = d0; d < d1; d++) {
+        if (i < nrt && (j >= nst || rk <= sk)) {
+            run = rk == pk ? run + 1 : 1;
+            pk = rk;
+            rk = kr(++i);
+        } else {
+            if (sk == pk) cnt += run;
+            sk = ks(++j);
+        }
+    }
+    const unsigned long long ws = warp_sum_u64(cnt);
+    if ((threadIdx.x & 31) == 0 && ws) atomicAdd(matches, ws);
 }
 
 template <bool MAT>
@@ -888,12 +984,20 @@ cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t 
     const uint64_t grid = merge_ctas(nr, ns);
     if (!grid) return cudaSuccess;
     const uint64_t nsplits = grid + 1;
-    k_merge_splits<<<(unsigned)((nsplits + 255) / 256), 256, 0, st>>>(R, nr, S, ns, splits, nsplits);
-    const size_t smem = (size_t)(MERGE_TILE + 1 + (mat ? MERGE_TILE : 0)) * 4;
-    auto kern = mat ? k_merge_join<true> : k_merge_join<false>;
-    cudaError_t e = smem_limit((const void *)kern, smem);
-    if (e != cudaSuccess) return e;
-    kern<<<(unsigned)grid, MERGE_THREADS, smem, st>>>(R, nr, S, ns, splits, matches, rows_ctr, out, cap);
+    const unsigned sgrid = (unsigned)((nsplits + 255) / 256);
+    cudaError_t e;
+    if (!mat) {
+        k_merge_splits<true><<<sgrid, 256, 0, st>>>(R, nr, S, ns, splits, nsplits);
+        const size_t smem = (size_t)(mskew_host(MERGE_TILE) + 1) * 4;
+        if ((e = smem_limit((const void *)k_merge_count, smem)) != cudaSuccess) return e;
+        k_merge_count<<<(unsigned)grid, MERGE_THREADS, smem, st>>>(R, nr, S, ns, splits, matches);
+    } else {
+        k_merge_splits<false><<<sgrid, 256, 0, st>>>(R, nr, S, ns, splits, nsplits);
+        const size_t smem = (size_t)(2 * MERGE_TILE + 1) * 4;
+        if ((e = smem_limit((const void *)k_merge_join<true>, smem)) != cudaSuccess) return e;
+        k_merge_join<true><<<(unsigned)grid, MERGE_THREADS, smem, st>>>(R, nr, S, ns, splits, matches, rows_ctr,
+                                                                        out, cap);
+    }
     count_launch(2);
     return cudaGetLastError();
 }

@@ -204,17 +204,18 @@ cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk
 // per SM walks the buckets.  Per bucket:
 //   1. the bucket's histogram over 2^lowbits bins in shared memory (the one
 //      read from DRAM) and its exclusive scan;
-//   2. the bins are cut into 2^pbits parts of consecutive bins, each small
-//      enough (as the histogram shows) to stage in shared memory: per part,
-//      a re-read of the bucket (from L2) places the part's rows at their
-//      sorted positions in the stage, which is then written out with
-//      coalesced stores (a 32K-row bucket: two parts).  A part too large
-//      for the stage (a heavy key) has its rows written straight to their
-//      sorted positions instead.
-// Staging row indices instead (4 bytes, one part per bucket, the rows
-// gathered back from L2 at the write-out) measured 12.8 against 8.3 ms for
-// 2^30 rows: the gather's scattered 8-byte reads cost more L2 sectors than
-// the second part's stream.
+//   2. one re-read of the bucket (from L2) ranks every row by an atomic on
+//      its bin's running offset: a row whose sorted position is below the
+//      stage's capacity (27K rows) goes to the stage in shared memory, the
+//      others (the bucket's last bins; all but the first 27K rows of a heavy
+//      key's bucket) straight to their place in the output; then the stage
+//      is written out with coalesced stores.
+// Two reads per row.  Before, the bins were cut into parts that each fit
+// the stage, with one re-read of the bucket per part (a 32K-row bucket: two
+// parts, three reads per row): 8.3 ms for 2^30 rows against about 7.2 ms
+// now.  Staging row indices instead (4 bytes, one part per bucket, the rows
+// gathered back from L2 at the write-out) measured 12.8 ms: the gather's
+// scattered 8-byte reads cost more L2 sectors than a part's stream.
 // Rows of equal keys land in any order, which the merge does not need (a
 // join's rows are a multiset).
 // ---------------------------------------------------------------------------
@@ -229,7 +230,7 @@ cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk
 constexpr int BSORT_THREADS = TBG_BSORT_THREADS;
 constexpr int BSORT_CTAS = TBG_BSORT_CTAS;
 constexpr int BSORT_PAIRS = 2;                                   // 16-byte row pairs per thread per round
-constexpr size_t BSORT_SMEM = (BSORT_CTAS == 1 ? 200 : 100) * 1024;  // stage + bins
+constexpr size_t BSORT_SMEM = (BSORT_CTAS == 1 ? 226 : 112) * 1024;  // stage + bins
 
 __device__ __forceinline__ uint32_t bsort_bin(uint32_t key, uint32_t sub, uint32_t mask) { return (key - sub) & mask; }
 
@@ -320,32 +321,21 @@ __global__ void __launch_bounds__(BSORT_THREADS, BSORT_CTAS) k_bucket_sort(const
             }
         }
         __syncthreads();
-        // 2. parts of 2^(lowbits - pbits) bins, an even share of the bucket
-        // each filling at most 7/8 of the stage
-        int pbits = 0;
-        while (pbits < lowbits && ((uint64_t)len >> pbits) > cap - cap / 8) pbits++;
-        const int pshift = lowbits - pbits;
-        for (uint32_t part = 0; part < (1u << pbits); part++) {
-            const uint32_t pb0 = part << pshift, pb1 = (part + 1) << pshift;
-            // the part's sorted rows: [h[pb0], h[pb1]) before any of them is ranked
-            const uint32_t r0 = h[pb0], r1 = pb1 < bins ? h[pb1] : len;
-            __syncthreads();  // every thread has read the part's bounds
-            if (r1 == r0) continue;
-            const bool staged = r1 - r0 <= cap;
-            bsort_stream(src, len, sub, mask, [&](Row r, uint32_t, bool ok, bool dup) {
-                const uint32_t d = bsort_bin(r.key, sub, mask);
-                const bool mine = ok && d >= pb0 && d < pb1;
-                const uint32_t pos = rank_warp(h, mine ? d : 0u, mine, dup);
-                if (mine) {
-                    if (staged) stage[pos - r0] = make_uint2(r.key, r.payload);
-                    else dst[pos] = make_uint2(r.key, r.payload);
-                }
-            });
-            __syncthreads();
-            if (staged)
-                for (uint32_t q = tid; q < r1 - r0; q += BSORT_THREADS) dst[r0 + q] = stage[q];
-            __syncthreads();  // the stage is refilled by the next part
-        }
+        // 2. one re-read of the bucket (from L2) ranks every row: the rows
+        // whose sorted position is below the stage's capacity go to the
+        // stage, the others (the bucket's last bins) straight to their place
+        // in the output; then the stage is written out with coalesced stores
+        const uint32_t nstage = min(len, cap);
+        bsort_stream(src, len, sub, mask, [&](Row r, uint32_t, bool ok, bool dup) {
+            const uint32_t pos = rank_warp(h, ok ? bsort_bin(r.key, sub, mask) : 0u, ok, dup);
+            if (ok) {
+                if (pos < nstage) stage[pos] = make_uint2(r.key, r.payload);
+                else dst[pos] = make_uint2(r.key, r.payload);
+            }
+        });
+        __syncthreads();
+        for (uint32_t q = tid; q < nstage; q += BSORT_THREADS) dst[q] = stage[q];
+        __syncthreads();  // the bins and the stage are reused by the next bucket
     }
 }
 
