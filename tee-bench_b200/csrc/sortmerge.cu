@@ -758,16 +758,25 @@ cudaError_t launch_key_range(const Row *in, uint64_t n, uint32_t *minmax, int ns
 #ifndef TBG_MERGE_PER_THREAD
 #define TBG_MERGE_PER_THREAD 16
 #endif
+#ifndef TBG_MCOUNT_PER_THREAD
+#define TBG_MCOUNT_PER_THREAD 32
+#endif
 constexpr int MERGE_THREADS = TBG_MERGE_THREADS;
 constexpr int MERGE_PER_THREAD = TBG_MERGE_PER_THREAD;
 constexpr int MERGE_TILE = MERGE_THREADS * MERGE_PER_THREAD;
+// the count-only merge walks longer segments (its per-thread search and
+// set-up cost less per row) and loads its tile in batches of 16 rows
+constexpr int MCOUNT_PER_THREAD = TBG_MCOUNT_PER_THREAD;
+constexpr int MCOUNT_TILE = MERGE_THREADS * MCOUNT_PER_THREAD;
+constexpr int MCOUNT_BATCH = 16;
+static_assert(MCOUNT_PER_THREAD % MCOUNT_BATCH == 0 && MCOUNT_TILE >= MERGE_TILE, "batches; the splits buffer");
 
 template <bool A_FIRST>
 __global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row *__restrict__ S, uint64_t ns,
-                               uint64_t *__restrict__ splits, uint64_t nsplits) {
+                               uint64_t *__restrict__ splits, uint64_t nsplits, uint32_t tile) {
     const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nsplits) return;
-    const uint64_t d = umin64(nr + ns, c * MERGE_TILE);
+    const uint64_t d = umin64(nr + ns, c * tile);
     auto kr = [&](uint64_t i) { return R[i].key; };
     auto ks = [&](uint64_t j) { return S[j].key; };
     splits[c] = merge_split<A_FIRST>(d, nr, ns, kr, ks);
@@ -785,15 +794,15 @@ __global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row
 __device__ __forceinline__ uint32_t mskew(uint32_t t) { return t + (t >> 4); }
 constexpr uint32_t mskew_host(uint32_t t) { return t + (t >> 4); }
 
-__global__ void __launch_bounds__(MERGE_THREADS, 8) k_merge_count(const Row *__restrict__ R, uint64_t nr,
+__global__ void __launch_bounds__(MERGE_THREADS, 6) k_merge_count(const Row *__restrict__ R, uint64_t nr,
                                                                 const Row *__restrict__ S, uint64_t ns,
                                                                 const uint64_t *__restrict__ splits,
                                                                 unsigned long long *matches) {
     extern __shared__ __align__(16) uint32_t merge_smem[];
-    uint32_t *K = merge_smem;  // mskew(MERGE_TILE) + 1 keys: R's, then S's, and a spare slot
+    uint32_t *K = merge_smem;  // mskew(MCOUNT_TILE) + 1 keys: R's, then S's, and a spare slot
     const uint64_t L = nr + ns;
     const uint64_t c = blockIdx.x;
-    const uint64_t dc0 = c * MERGE_TILE, dc1 = umin64(L, dc0 + MERGE_TILE);
+    const uint64_t dc0 = c * MCOUNT_TILE, dc1 = umin64(L, dc0 + MCOUNT_TILE);
     const uint64_t ic0 = splits[c], ic1 = splits[c + 1];
     const uint64_t jc0 = dc0 - ic0, jc1 = dc1 - ic1;
     const uint32_t nrt = (uint32_t)(ic1 - ic0), nst = (uint32_t)(jc1 - jc0);
@@ -801,23 +810,26 @@ __global__ void __launch_bounds__(MERGE_THREADS, 8) k_merge_count(const Row *__r
     {
         const uint2 *Rv = reinterpret_cast<const uint2 *>(R) + ic0;
         const uint2 *Sv = reinterpret_cast<const uint2 *>(S) + jc0;
-        uint32_t x[MERGE_PER_THREAD];
 #pragma unroll
-        for (int q = 0; q < MERGE_PER_THREAD; q++) {
-            const uint32_t t = q * MERGE_THREADS + threadIdx.x;
-            if (t < Lt) x[q] = __ldcs(t < nrt ? Rv + t : Sv + (t - nrt)).x;
-        }
+        for (int b = 0; b < MCOUNT_PER_THREAD; b += MCOUNT_BATCH) {
+            uint32_t x[MCOUNT_BATCH];
 #pragma unroll
-        for (int q = 0; q < MERGE_PER_THREAD; q++) {
-            const uint32_t t = q * MERGE_THREADS + threadIdx.x;
-            if (t < Lt) K[mskew(t)] = x[q];
+            for (int q = 0; q < MCOUNT_BATCH; q++) {
+                const uint32_t t = (b + q) * MERGE_THREADS + threadIdx.x;
+                if (t < Lt) x[q] = __ldcs(t < nrt ? Rv + t : Sv + (t - nrt)).x;
+            }
+#pragma unroll
+            for (int q = 0; q < MCOUNT_BATCH; q++) {
+                const uint32_t t = (b + q) * MERGE_THREADS + threadIdx.x;
+                if (t < Lt) K[mskew(t)] = x[q];
+            }
         }
         if (threadIdx.x == 0) K[mskew(Lt)] = 0;
     }
     __syncthreads();
     auto kr = [&](uint32_t i) { return K[mskew(i)]; };
     auto ks = [&](uint32_t j) { return K[mskew(nrt + j)]; };
-    const uint32_t d0 = min(Lt, threadIdx.x * MERGE_PER_THREAD), d1 = min(Lt, d0 + MERGE_PER_THREAD);
+    const uint32_t d0 = min(Lt, threadIdx.x * MCOUNT_PER_THREAD), d1 = min(Lt, d0 + MCOUNT_PER_THREAD);
     uint32_t i;
     {
         uint32_t lo = d0 > nst ? d0 - nst : 0, hi = min(d0, nrt);
@@ -849,18 +861,29 @@ __global__ void __launch_bounds__(MERGE_THREADS, 8) k_merge_count(const Row *__r
         }
         run = gi - q;
     }
-    // current keys in registers; past a side's end they read the next slot
-    // (the other side's first key or the spare), which the bounds keep unused
-    uint32_t rk = kr(i), sk = ks(j);
+    // Current keys in registers.  A step takes R (ta) or S without a
+    // branch: one shared load at the taken side's next position (past a
+    // side's end: the other side's first key or the spare slot, which the
+    // bounds keep unused) and selects.
+    uint32_t jj = nrt + j;  // S's cursor in K
+    uint32_t rk = kr(i), sk = K[mskew(jj)];
+    uint32_t run32 = (uint32_t)run;  // a run of R rows is shorter than 2^32
     unsigned long long cnt = 0;
-    for (uint32_t d = d0; d < d1; d++) {
-        if (i < nrt && (j >= nst || rk <= sk)) {
-            run = rk == pk ? run + 1 : 1;
-            pk = rk;
-            rk = kr(++i);
-        } else {
-            if (sk == pk) cnt += run;
-            sk = ks(++j);
+    const uint32_t steps = d1 - d0;
+#pragma unroll
+    for (uint32_t t = 0; t < (uint32_t)MCOUNT_PER_THREAD; t++) {
+        if (t < steps) {
+            const bool ta = i < nrt && (jj >= Lt || rk <= sk);
+            const uint32_t key = ta ? rk : sk;
+            const bool eq = key == pk;
+            cnt += (!ta && eq) ? run32 : 0u;
+            run32 = ta ? (eq ? run32 + 1 : 1u) : run32;
+            pk = ta ? key : pk;
+            const uint32_t nx = K[mskew((ta ? i : jj) + 1)];
+            i += ta;
+            jj += !ta;
+            rk = ta ? nx : rk;
+            sk = ta ? sk : nx;
         }
     }
     const unsigned long long ws = warp_sum_u64(cnt);
@@ -987,12 +1010,14 @@ cudaError_t launch_merge_join(const Row *R, uint64_t nr, const Row *S, uint64_t 
     const unsigned sgrid = (unsigned)((nsplits + 255) / 256);
     cudaError_t e;
     if (!mat) {
-        k_merge_splits<true><<<sgrid, 256, 0, st>>>(R, nr, S, ns, splits, nsplits);
-        const size_t smem = (size_t)(mskew_host(MERGE_TILE) + 1) * 4;
+        const uint64_t cgrid = (nr + ns + MCOUNT_TILE - 1) / MCOUNT_TILE;
+        k_merge_splits<true><<<(unsigned)((cgrid + 256) / 256), 256, 0, st>>>(R, nr, S, ns, splits, cgrid + 1,
+                                                                              MCOUNT_TILE);
+        const size_t smem = (size_t)(mskew_host(MCOUNT_TILE) + 1) * 4;
         if ((e = smem_limit((const void *)k_merge_count, smem)) != cudaSuccess) return e;
-        k_merge_count<<<(unsigned)grid, MERGE_THREADS, smem, st>>>(R, nr, S, ns, splits, matches);
+        k_merge_count<<<(unsigned)cgrid, MERGE_THREADS, smem, st>>>(R, nr, S, ns, splits, matches);
     } else {
-        k_merge_splits<false><<<sgrid, 256, 0, st>>>(R, nr, S, ns, splits, nsplits);
+        k_merge_splits<false><<<sgrid, 256, 0, st>>>(R, nr, S, ns, splits, nsplits, MERGE_TILE);
         const size_t smem = (size_t)(2 * MERGE_TILE + 1) * 4;
         if ((e = smem_limit((const void *)k_merge_join<true>, smem)) != cudaSuccess) return e;
         k_merge_join<true><<<(unsigned)grid, MERGE_THREADS, smem, st>>>(R, nr, S, ns, splits, matches, rows_ctr,
