@@ -119,8 +119,8 @@ int lsd_sort_chunked(const Row *in, uint64_t n, uint32_t kmin, uint32_t kmax, De
     return TBG_OK;
 }
 
-cudaError_t launch_bucket_sort(const Row *in, Row *out, const uint64_t *base, uint32_t nb, uint32_t sub, int lowbits,
-                               int nsm, cudaStream_t st);
+cudaError_t launch_bucket_sort(const Row *in, Row *out, const uint64_t *base, uint32_t nb, uint64_t n, uint32_t sub,
+                               int lowbits, int nsm, cudaStream_t st);
 
 // MSD sort of both relations: radix partitioning by the top B bits of
 // key - sub (RHO's histogram and passes), then each bucket sorted by the low
@@ -171,7 +171,8 @@ static int msd_sort(const tbg_config &cfg, const Row *dR, uint64_t nR, const Row
             return rc;
         const Row *part = (rel ? w.partS : w.partR).as<Row>();
         const uint64_t *base = (rel ? w.baseS : w.baseR).as<uint64_t>();
-        if ((e = launch_bucket_sort(part, sorted[rel], base, (uint32_t)g.P, sub, lowbits, w.nsm, st)) != cudaSuccess)
+        if ((e = launch_bucket_sort(part, sorted[rel], base, (uint32_t)g.P, rel ? nS : nR, sub, lowbits, w.nsm,
+                                    st)) != cudaSuccess)
             return cuda_error(e, "bucket sort");
         msd_done[rel] = true;
         mark_ev(w, cfg.timing != 0, 2 + rel, st);

@@ -791,7 +791,10 @@ __global__ void k_merge_splits(const Row *__restrict__ R, uint64_t nr, const Row
 // starts earlier); the steps themselves never walk a run.  Keys sit in shared
 // memory at t + t / 16, so threads whose walks start 16 apart use different
 // banks.
-__device__ __forceinline__ uint32_t mskew(uint32_t t) { return t + (t >> 4); }
+#ifndef TBG_MERGE_SKEW
+#define TBG_MERGE_SKEW 1
+#endif
+__device__ __forceinline__ uint32_t mskew(uint32_t t) { return TBG_MERGE_SKEW ? t + (t >> 4) : t; }
 constexpr uint32_t mskew_host(uint32_t t) { return t + (t >> 4); }
 
 __global__ void __launch_bounds__(MERGE_THREADS, 6) k_merge_count(const Row *__restrict__ R, uint64_t nr,

@@ -212,8 +212,8 @@ cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk
 //      is written out with coalesced stores.
 // Two reads per row.  Before, the bins were cut into parts that each fit
 // the stage, with one re-read of the bucket per part (a 32K-row bucket: two
-// parts, three reads per row): 8.3 ms for 2^30 rows against about 7.2 ms
-// now.  Staging row indices instead (4 bytes, one part per bucket, the rows
+// parts, three reads per row): 8.4 ms for 2^30 rows against 7.3 ms now (ncu
+// launch lists).  Staging row indices instead (4 bytes, one part per bucket, the rows
 // gathered back from L2 at the write-out) measured 12.8 ms: the gather's
 // scattered 8-byte reads cost more L2 sectors than a part's stream.
 // Rows of equal keys land in any order, which the merge does not need (a
@@ -229,30 +229,80 @@ cudaError_t launch_sort_pass(const Row *in, Row *out, uint64_t n, uint64_t chunk
 #endif
 constexpr int BSORT_THREADS = TBG_BSORT_THREADS;
 constexpr int BSORT_CTAS = TBG_BSORT_CTAS;
-constexpr int BSORT_PAIRS = 2;                                   // 16-byte row pairs per thread per round
+#ifndef TBG_BSORT_GROUPS
+#define TBG_BSORT_GROUPS 4
+#endif
+#ifndef TBG_BSORT_PAIRS
+#define TBG_BSORT_PAIRS 2
+#endif
+constexpr int BSORT_PAIRS = TBG_BSORT_PAIRS;  // 16-byte row pairs per thread per round
 constexpr size_t BSORT_SMEM = (BSORT_CTAS == 1 ? 226 : 112) * 1024;  // stage + bins
 
 __device__ __forceinline__ uint32_t bsort_bin(uint32_t key, uint32_t sub, uint32_t mask) { return (key - sub) & mask; }
 
+// A bucket is sorted by a group of BSORT_THREADS / G threads with its own
+// bins and stage (G groups per CTA work on G buckets at a time, each at its
+// own pace): small buckets (R's 4K rows at 2^27 keys) take G = 4, which keeps
+// four buckets' phases overlapping where one group would wait on its
+// barriers; large buckets take G = 1 and the whole stage.  The scan of the
+// bins reads them as 16-byte words (strided 4-byte reads of a thread's run
+// of bins conflicted 4-way at G = 1 and 16-way at G = 4): with it PSM's R
+// sort (2^27 rows) took 0.36 ms less at G = 4 than at G = 1.
+template <int G>
+__device__ __forceinline__ void group_bar(int g) {
+    if (G == 1) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(BSORT_THREADS / G) : "memory");
+}
+
+// Exclusive scan of one value per thread over a group (scratch: a word per
+// warp of the group); every thread of the group calls it.
+template <int G>
+__device__ __forceinline__ uint32_t group_excl_scan(uint32_t v, uint32_t *total, uint32_t *scratch, int g) {
+    constexpr int GT = BSORT_THREADS / G, NW = GT / 32;
+    const int lane = threadIdx.x & 31, w = (threadIdx.x % GT) >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) scratch[w] = x;
+    group_bar<G>(g);
+    if (w == 0) {
+        uint32_t t = lane < NW ? scratch[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < NW) scratch[lane] = t;
+    }
+    group_bar<G>(g);
+    const uint32_t before = w ? scratch[w - 1] : 0;
+    *total = scratch[NW - 1];
+    group_bar<G>(g);  // scratch is reused by the next scan
+    return before + x - v;
+}
+
 // Calls fn(row, index, valid, dup) for every row of the bucket (index: its
-// place in the bucket), in block-uniform rounds (so fn may use warp
+// place in the bucket), in group-uniform rounds (so fn may use warp
 // collectives); `dup` says the warp saw repeated bins in the round's first
 // row slot (skew).  The next round's loads are issued before the current
 // round is handed to fn.  The bucket's edge rows (outside the 16-byte
-// aligned body) come in a last round of warp 0.
-template <class Fn>
-__device__ __forceinline__ void bsort_stream(const Row *src, uint32_t len, uint32_t sub, uint32_t mask, Fn fn) {
-    const int tid = threadIdx.x;
+// aligned body) come in a last round of the group's first warp.
+template <int GT, class Fn>
+__device__ __forceinline__ void bsort_stream(const Row *src, uint32_t len, uint32_t sub, uint32_t mask, int gtid,
+                                             Fn fn) {
     const uint32_t head = (reinterpret_cast<uintptr_t>(src) & 15) ? 1u : 0u;
     const uint32_t npairs = (len - head) / 2;
     const bool tail = ((len - head) & 1) != 0;
     const uint4 *v = reinterpret_cast<const uint4 *>(src + head);
-    constexpr uint32_t ROUND = BSORT_PAIRS * BSORT_THREADS;
+    constexpr uint32_t ROUND = BSORT_PAIRS * GT;
     uint4 nx[BSORT_PAIRS];
     auto load = [&](uint32_t p0) {
 #pragma unroll
         for (int u = 0; u < BSORT_PAIRS; u++) {
-            const uint32_t p = p0 + u * BSORT_THREADS + tid;
+            const uint32_t p = p0 + u * GT + gtid;
             nx[u] = p < npairs ? __ldcg(v + p) : make_uint4(0, 0, 0, 0);
         }
     };
@@ -262,17 +312,17 @@ __device__ __forceinline__ void bsort_stream(const Row *src, uint32_t len, uint3
 #pragma unroll
         for (int u = 0; u < BSORT_PAIRS; u++) x[u] = nx[u];
         load(p0 + ROUND);
-        const bool dup = warp_has_dups(bsort_bin(x[0].x, sub, mask), p0 + tid < npairs);
+        const bool dup = warp_has_dups(bsort_bin(x[0].x, sub, mask), p0 + gtid < npairs);
 #pragma unroll
         for (int u = 0; u < BSORT_PAIRS; u++) {
-            const uint32_t p = p0 + u * BSORT_THREADS + tid;
+            const uint32_t p = p0 + u * GT + gtid;
             const bool ok = p < npairs;
             fn(Row{x[u].x, x[u].y}, head + 2 * p, ok, dup);
             fn(Row{x[u].z, x[u].w}, head + 2 * p + 1, ok, dup);
         }
     }
-    if (tid < 32) {
-        const int lane = tid;
+    if (gtid < 32) {
+        const int lane = gtid;
         const bool ok = (lane == 0 && head) || (lane == 1 && tail);
         const uint32_t i = lane == 0 ? 0u : len - 1;
         const Row r = ok ? src[i] : Row{0, 0};
@@ -280,62 +330,93 @@ __device__ __forceinline__ void bsort_stream(const Row *src, uint32_t len, uint3
     }
 }
 
-__global__ void __launch_bounds__(BSORT_THREADS, BSORT_CTAS) k_bucket_sort(const Row *__restrict__ in, Row *__restrict__ out,
-                                                                const uint64_t *__restrict__ base, uint32_t nb,
-                                                                uint32_t sub, int lowbits) {
+// Shared memory of one group: its bins, then its stage.
+template <int G>
+__host__ __device__ constexpr size_t bsort_group_bytes() {
+    return (BSORT_SMEM / G) & ~(size_t)15;
+}
+
+template <int G>
+__global__ void __launch_bounds__(BSORT_THREADS, BSORT_CTAS)
+    k_bucket_sort(const Row *__restrict__ in, Row *__restrict__ out, const uint64_t *__restrict__ base, uint32_t nb,
+                  uint32_t sub, int lowbits) {
     extern __shared__ __align__(16) unsigned char bsmem[];
+    constexpr int GT = BSORT_THREADS / G;
+    const int g = threadIdx.x / GT, gtid = threadIdx.x % GT;
     const uint32_t bins = 1u << lowbits, mask = bins - 1;
-    uint32_t *h = reinterpret_cast<uint32_t *>(bsmem);          // bins
-    uint2 *stage = reinterpret_cast<uint2 *>(bsmem + 4 * bins);  // cap rows
-    const uint32_t cap = (uint32_t)((BSORT_SMEM - 4 * (size_t)bins) / 8);
-    __shared__ uint64_t scratch[BSORT_THREADS / 32 + 1];
-    const int tid = threadIdx.x;
-    const uint32_t per = (bins + BSORT_THREADS - 1) / BSORT_THREADS;
-    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
-        const uint64_t lo = base[b], hi = base[b + 1];  // the same for every thread
+    unsigned char *gm = bsmem + g * bsort_group_bytes<G>();
+    uint32_t *h = reinterpret_cast<uint32_t *>(gm);          // bins
+    uint2 *stage = reinterpret_cast<uint2 *>(gm + 4 * bins);  // cap rows
+    const uint32_t cap = (uint32_t)((bsort_group_bytes<G>() - 4 * (size_t)bins) / 8);
+    __shared__ uint32_t scratch_all[G][GT / 32];
+    uint32_t *scratch = scratch_all[g];
+    const uint32_t per = (bins + GT - 1) / GT;
+    for (uint32_t b = blockIdx.x * G + g; b < nb; b += gridDim.x * G) {
+        const uint64_t lo = base[b], hi = base[b + 1];  // the same for every thread of the group
         if (hi <= lo) continue;
         const Row *src = in + lo;
         uint2 *dst = reinterpret_cast<uint2 *>(out + lo);
         const uint32_t len = (uint32_t)(hi - lo);  // a bucket holds < 2^32 rows
         if (len == 1) {
-            if (tid == 0) dst[0] = make_uint2(src[0].key, src[0].payload);
+            if (gtid == 0) dst[0] = make_uint2(src[0].key, src[0].payload);
             continue;
         }
-        for (uint32_t q = tid; q < bins; q += BSORT_THREADS) h[q] = 0;
-        __syncthreads();
+        for (uint32_t q = gtid; q < bins; q += GT) h[q] = 0;
+        group_bar<G>(g);
         // 1. histogram and exclusive scan
-        bsort_stream(src, len, sub, mask, [&](Row r, uint32_t, bool ok, bool dup) {
+        bsort_stream<GT>(src, len, sub, mask, gtid, [&](Row r, uint32_t, bool ok, bool dup) {
             hist_add_warp(h, ok ? bsort_bin(r.key, sub, mask) : 0u, ok, dup);
         });
-        __syncthreads();
-        {
-            const uint32_t b0 = min(bins, tid * per), b1 = min(bins, b0 + per);
+        group_bar<G>(g);
+        if (per % 4 == 0) {
+            // a thread's bins as 16-byte words: a warp reads consecutive
+            // words (one thread's 4 bins each at 1024 threads: no conflicts)
+            uint4 *h4 = reinterpret_cast<uint4 *>(h) + gtid * (per / 4);
+            uint32_t sum = 0;
+            for (uint32_t q = 0; q < per / 4; q++) {
+                const uint4 c = h4[q];
+                sum += c.x + c.y + c.z + c.w;
+            }
+            uint32_t tot;
+            uint32_t run = group_excl_scan<G>(sum, &tot, scratch, g);
+            for (uint32_t q = 0; q < per / 4; q++) {
+                const uint4 c = h4[q];
+                uint4 o;
+                o.x = run;
+                o.y = o.x + c.x;
+                o.z = o.y + c.y;
+                o.w = o.z + c.z;
+                run = o.w + c.w;
+                h4[q] = o;
+            }
+        } else {
+            const uint32_t b0 = min(bins, gtid * per), b1 = min(bins, b0 + per);
             uint32_t sum = 0;
             for (uint32_t q = b0; q < b1; q++) sum += h[q];
-            uint64_t tot;
-            uint32_t run = (uint32_t)block_excl_scan<BSORT_THREADS>(sum, &tot, scratch);
+            uint32_t tot;
+            uint32_t run = group_excl_scan<G>(sum, &tot, scratch, g);
             for (uint32_t q = b0; q < b1; q++) {
                 const uint32_t c = h[q];
                 h[q] = run;
                 run += c;
             }
         }
-        __syncthreads();
+        group_bar<G>(g);
         // 2. one re-read of the bucket (from L2) ranks every row: the rows
         // whose sorted position is below the stage's capacity go to the
         // stage, the others (the bucket's last bins) straight to their place
         // in the output; then the stage is written out with coalesced stores
         const uint32_t nstage = min(len, cap);
-        bsort_stream(src, len, sub, mask, [&](Row r, uint32_t, bool ok, bool dup) {
+        bsort_stream<GT>(src, len, sub, mask, gtid, [&](Row r, uint32_t, bool ok, bool dup) {
             const uint32_t pos = rank_warp(h, ok ? bsort_bin(r.key, sub, mask) : 0u, ok, dup);
             if (ok) {
                 if (pos < nstage) stage[pos] = make_uint2(r.key, r.payload);
                 else dst[pos] = make_uint2(r.key, r.payload);
             }
         });
-        __syncthreads();
-        for (uint32_t q = tid; q < nstage; q += BSORT_THREADS) dst[q] = stage[q];
-        __syncthreads();  // the bins and the stage are reused by the next bucket
+        group_bar<G>(g);
+        for (uint32_t q = gtid; q < nstage; q += GT) dst[q] = stage[q];
+        group_bar<G>(g);  // the bins and the stage are reused by the next bucket
     }
 }
 
@@ -344,17 +425,24 @@ size_t bucket_sort_smem(int lowbits) {
     return BSORT_SMEM;
 }
 
-cudaError_t launch_bucket_sort(const Row *in, Row *out, const uint64_t *base, uint32_t nb, uint32_t sub, int lowbits,
-                               int nsm, cudaStream_t st) {
+cudaError_t launch_bucket_sort(const Row *in, Row *out, const uint64_t *base, uint32_t nb, uint64_t n, uint32_t sub,
+                               int lowbits, int nsm, cudaStream_t st) {
     if (!nb) return cudaSuccess;
     if (lowbits > 14) return cudaErrorInvalidValue;  // the bins must leave room for a stage
     const size_t smem = bucket_sort_smem(lowbits);
-    cudaError_t e = smem_limit((const void *)k_bucket_sort, smem);
+    // four groups when their stages hold an average bucket
+    constexpr int G4 = BSORT_THREADS >= 1024 ? TBG_BSORT_GROUPS : 1;
+    const size_t bins_bytes = (size_t)4 << lowbits;
+    const bool small = G4 > 1 && bins_bytes * 2 <= bsort_group_bytes<G4>() &&
+                       n / nb <= (bsort_group_bytes<G4>() - bins_bytes) / 8;
+    auto kern = small ? k_bucket_sort<G4> : k_bucket_sort<1>;
+    cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     // one CTA per SM: the buckets in flight (each read from DRAM once and
-    // re-read per part) stay within L2
-    const unsigned g = (unsigned)std::min<uint64_t>(nb, (uint64_t)nsm * BSORT_CTAS);
-    k_bucket_sort<<<g, BSORT_THREADS, smem, st>>>(in, out, base, nb, sub, lowbits);
+    // re-read once) stay within L2
+    const int G = small ? G4 : 1;
+    const unsigned g = (unsigned)std::min<uint64_t>((nb + G - 1) / G, (uint64_t)nsm * BSORT_CTAS);
+    kern<<<g, BSORT_THREADS, smem, st>>>(in, out, base, nb, sub, lowbits);
     count_launch();
     return cudaGetLastError();
 }
