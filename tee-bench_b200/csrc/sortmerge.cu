@@ -531,6 +531,7 @@ constexpr uint32_t RSM_KEYS = skewed_size<uint32_t>(RSM_STILE);
 constexpr uint32_t RSM_SBIG = RSM_STILE * 4;
 constexpr uint32_t RSM_SBIG_KEYS = skewed_size<uint32_t>(RSM_SBIG);
 constexpr uint32_t RSM_BINS = 1u << COUNT_SORT_BITS;
+static_assert(RSM_BINS % (4 * RSM_THREADS) == 0, "the rounded bin count fits");
 // the per-tile path reuses the S buffer: 4096 sorted keys, the sort's
 // scratch keys and its 16-bit counters
 static_assert(2 * RSM_KEYS + 256 * (RSM_THREADS / 32) / 2 <= RSM_SBIG_KEYS, "per-tile buffers fit the S buffer");
@@ -576,6 +577,29 @@ __device__ __forceinline__ void rsm_ranged_pass(const Row *__restrict__ S, uint6
 // the counters written but not yet synchronised.
 __device__ __forceinline__ uint32_t rsm_scan_bins(uint32_t *cnt, uint32_t bins, uint64_t *scratch) {
     const uint32_t per = (bins + RSM_THREADS - 1) / RSM_THREADS;
+    if (per % 4 == 0) {
+        // bins a multiple of 4 * RSM_THREADS: a thread's run of bins as
+        // 16-byte words (strided 4-byte reads of the runs conflict 8-way)
+        uint4 *c4 = reinterpret_cast<uint4 *>(cnt) + threadIdx.x * (per / 4);
+        uint32_t sum = 0;
+        for (uint32_t q = 0; q < per / 4; q++) {
+            const uint4 c = c4[q];
+            sum += c.x + c.y + c.z + c.w;
+        }
+        uint64_t tot;
+        uint32_t run = (uint32_t)block_excl_scan<RSM_THREADS>(sum, &tot, scratch);
+        for (uint32_t q = 0; q < per / 4; q++) {
+            const uint4 c = c4[q];
+            uint4 o;
+            o.x = run;
+            o.y = o.x + c.x;
+            o.z = o.y + c.y;
+            o.w = o.z + c.z;
+            run = o.w + c.w;
+            c4[q] = o;
+        }
+        return (uint32_t)tot;
+    }
     const uint32_t b0 = min(bins, threadIdx.x * per), b1 = min(bins, b0 + per);
     uint32_t sum = 0;
     for (uint32_t b = b0; b < b1; b++) sum += cnt[b];
@@ -598,9 +622,9 @@ __device__ __forceinline__ uint32_t rsm_scan_bins(uint32_t *cnt, uint32_t bins, 
 // loading while tile k merges.
 __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t *Rk = reinterpret_cast<uint32_t *>(smem);
+    uint32_t *bins_cnt = reinterpret_cast<uint32_t *>(smem);  // 16-byte aligned for the scan
+    uint32_t *Rk = bins_cnt + RSM_BINS;
     uint32_t *Sk = Rk + RSM_KEYS;
-    uint32_t *bins_cnt = Sk + RSM_SBIG_KEYS;
     uint32_t *tmp = Sk + RSM_KEYS;  // per-tile sorts: scratch keys and counters inside the S buffer
     uint16_t *cnt = reinterpret_cast<uint16_t *>(tmp + RSM_KEYS);
     __shared__ uint32_t s_item;
@@ -624,7 +648,11 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
         sort_keys<RSM_THREADS>(key, nr, Rk, tmp, cnt, scan_scratch, red);
         const uint32_t rmin = Rk[0], rspan = Rk[skew<uint32_t>(nr - 1)] - rmin;
         if ((rspan >> shift) < RSM_BINS) {
-            const uint32_t bins = (rspan >> shift) + 1;
+            // digits in [0, bins); above 1024 bins the count runs to a
+            // multiple of 4 * RSM_THREADS (the extra bins stay empty) so the
+            // scan reads 16-byte words
+            const uint32_t bins0 = (rspan >> shift) + 1;
+            const uint32_t bins = bins0 > 1024 ? (bins0 + 4 * RSM_THREADS - 1) & ~(4u * RSM_THREADS - 1) : bins0;
             for (uint64_t s0 = 0; s0 < m.s_len; s0 += RSM_SBIG) {
                 const uint32_t ns = (uint32_t)umin64(RSM_SBIG, m.s_len - s0);
                 for (uint32_t b = tid; b < bins; b += RSM_THREADS) bins_cnt[b] = 0;
