@@ -393,13 +393,56 @@ __device__ __forceinline__ void load_keys(const Row *__restrict__ src, uint64_t 
     }
 }
 
-// Sorts the n keys held as load_keys left them into `out` (skewed 4-byte
-// layout): one counting pass when the varying bits span at most
-// COUNT_SORT_BITS, else the stable LSD sort through `tmp`.  `out` and `tmp`
-// hold skewed_size<uint32_t>(THREADS * 8) keys.
+// cnt[0, bins) -> exclusive offsets in place; returns the total.  Ends with
+// the counters written but not yet synchronised.  When bins is a multiple of
+// 4 * THREADS (and cnt 16-byte aligned) a thread's run of bins moves as
+// 16-byte words: strided 4-byte reads of the runs conflict (8-way for runs
+// of 8 bins).
 template <int THREADS>
-__device__ void sort_keys(const uint32_t (&key)[8], uint32_t n, uint32_t *out, uint32_t *tmp, uint16_t *cnt,
-                          uint64_t *scratch, uint32_t *red) {
+__device__ __forceinline__ uint32_t scan_bins(uint32_t *cnt, uint32_t bins, uint64_t *scratch) {
+    const uint32_t per = (bins + THREADS - 1) / THREADS;
+    if (per % 4 == 0) {
+        uint4 *c4 = reinterpret_cast<uint4 *>(cnt) + threadIdx.x * (per / 4);
+        uint32_t sum = 0;
+        for (uint32_t q = 0; q < per / 4; q++) {
+            const uint4 c = c4[q];
+            sum += c.x + c.y + c.z + c.w;
+        }
+        uint64_t tot;
+        uint32_t run = (uint32_t)block_excl_scan<THREADS>(sum, &tot, scratch);
+        for (uint32_t q = 0; q < per / 4; q++) {
+            const uint4 c = c4[q];
+            uint4 o;
+            o.x = run;
+            o.y = o.x + c.x;
+            o.z = o.y + c.y;
+            o.w = o.z + c.z;
+            run = o.w + c.w;
+            c4[q] = o;
+        }
+        return (uint32_t)tot;
+    }
+    const uint32_t b0 = min(bins, threadIdx.x * per), b1 = min(bins, b0 + per);
+    uint32_t sum = 0;
+    for (uint32_t b = b0; b < b1; b++) sum += cnt[b];
+    uint64_t tot;
+    uint32_t run = (uint32_t)block_excl_scan<THREADS>(sum, &tot, scratch);
+    for (uint32_t b = b0; b < b1; b++) {
+        const uint32_t c = cnt[b];
+        cnt[b] = run;
+        run += c;
+    }
+    return (uint32_t)tot;
+}
+
+// Sorts the n keys held as load_keys left them into `out` (skewed 4-byte
+// layout): one counting pass on the 2^COUNT_SORT_BITS counters `c32`
+// (16-byte aligned) when the varying bits span at most COUNT_SORT_BITS, else
+// the stable LSD sort through `tmp`.  `out` and `tmp` hold
+// skewed_size<uint32_t>(THREADS * 8) keys.
+template <int THREADS>
+__device__ void sort_keys(const uint32_t (&key)[8], uint32_t n, uint32_t *out, uint32_t *tmp, uint32_t *c32,
+                          uint16_t *cnt, uint64_t *scratch, uint32_t *red) {
     constexpr int ITEMS = 8;
     const int tid = threadIdx.x, lane = tid & 31;
     if (tid == 0) {
@@ -440,7 +483,6 @@ __device__ void sort_keys(const uint32_t (&key)[8], uint32_t n, uint32_t *out, u
         return;
     }
     const uint32_t bins = 1u << span;
-    uint32_t *c32 = tmp;
     for (uint32_t b = tid; b < bins; b += THREADS) c32[b] = 0;
     __syncthreads();
     uint32_t r[ITEMS];
@@ -451,19 +493,7 @@ __device__ void sort_keys(const uint32_t (&key)[8], uint32_t n, uint32_t *out, u
         r[i] = rank_warp(c32, d, valid, warp_has_dups(d, valid));
     }
     __syncthreads();
-    {
-        const uint32_t per = (bins + THREADS - 1) / THREADS;
-        const uint32_t b0 = min(bins, tid * per), b1 = min(bins, b0 + per);
-        uint32_t sum = 0;
-        for (uint32_t b = b0; b < b1; b++) sum += c32[b];
-        uint64_t tot;
-        uint32_t run = (uint32_t)block_excl_scan<THREADS>(sum, &tot, scratch);
-        for (uint32_t b = b0; b < b1; b++) {
-            const uint32_t c = c32[b];
-            c32[b] = run;
-            run += c;
-        }
-    }
+    scan_bins<THREADS>(c32, bins, scratch);
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < ITEMS; i++)
@@ -573,46 +603,6 @@ __device__ __forceinline__ void rsm_ranged_pass(const Row *__restrict__ S, uint6
     }
 }
 
-// cnt[0, bins) -> exclusive offsets in place; returns the total.  Ends with
-// the counters written but not yet synchronised.
-__device__ __forceinline__ uint32_t rsm_scan_bins(uint32_t *cnt, uint32_t bins, uint64_t *scratch) {
-    const uint32_t per = (bins + RSM_THREADS - 1) / RSM_THREADS;
-    if (per % 4 == 0) {
-        // bins a multiple of 4 * RSM_THREADS: a thread's run of bins as
-        // 16-byte words (strided 4-byte reads of the runs conflict 8-way)
-        uint4 *c4 = reinterpret_cast<uint4 *>(cnt) + threadIdx.x * (per / 4);
-        uint32_t sum = 0;
-        for (uint32_t q = 0; q < per / 4; q++) {
-            const uint4 c = c4[q];
-            sum += c.x + c.y + c.z + c.w;
-        }
-        uint64_t tot;
-        uint32_t run = (uint32_t)block_excl_scan<RSM_THREADS>(sum, &tot, scratch);
-        for (uint32_t q = 0; q < per / 4; q++) {
-            const uint4 c = c4[q];
-            uint4 o;
-            o.x = run;
-            o.y = o.x + c.x;
-            o.z = o.y + c.y;
-            o.w = o.z + c.z;
-            run = o.w + c.w;
-            c4[q] = o;
-        }
-        return (uint32_t)tot;
-    }
-    const uint32_t b0 = min(bins, threadIdx.x * per), b1 = min(bins, b0 + per);
-    uint32_t sum = 0;
-    for (uint32_t b = b0; b < b1; b++) sum += cnt[b];
-    uint64_t tot;
-    uint32_t run = (uint32_t)block_excl_scan<RSM_THREADS>(sum, &tot, scratch);
-    for (uint32_t b = b0; b < b1; b++) {
-        const uint32_t c = cnt[b];
-        cnt[b] = run;
-        run += c;
-    }
-    return (uint32_t)tot;
-}
-
 // Count-only RSM for items with r_len <= RSM_STILE.  The R chunk's keys are
 // sorted once (sort_keys).  When R's keys span at most RSM_BINS digits above
 // the partition's radix bits, S is sorted in tiles of RSM_SBIG rows by the
@@ -645,7 +635,7 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
         __syncthreads();  // s_item read by every thread before thread 0 rewrites it
         if (nr == 0 || m.s_len == 0) continue;
         load_keys<RSM_THREADS>(a.R, m.r_off, nr, key);
-        sort_keys<RSM_THREADS>(key, nr, Rk, tmp, cnt, scan_scratch, red);
+        sort_keys<RSM_THREADS>(key, nr, Rk, tmp, bins_cnt, cnt, scan_scratch, red);
         const uint32_t rmin = Rk[0], rspan = Rk[skew<uint32_t>(nr - 1)] - rmin;
         if ((rspan >> shift) < RSM_BINS) {
             // digits in [0, bins); above 1024 bins the count runs to a
@@ -660,7 +650,7 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
                 if (ns == RSM_SBIG) rsm_ranged_pass<false, true>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
                 else rsm_ranged_pass<false, false>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
                 __syncthreads();
-                const uint32_t nin = rsm_scan_bins(bins_cnt, bins, scan_scratch);
+                const uint32_t nin = scan_bins<RSM_THREADS>(bins_cnt, bins, scan_scratch);
                 __syncthreads();
                 if (ns == RSM_SBIG) rsm_ranged_pass<true, true>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
                 else rsm_ranged_pass<true, false>(a.S, m.s_off + s0, ns, rmin, rspan, shift, bins_cnt, Sk);
@@ -673,7 +663,7 @@ __global__ void __launch_bounds__(RSM_THREADS, 2) k_join_rsm_count(JoinArgs a) {
         uint32_t ns = (uint32_t)umin64(RSM_STILE, m.s_len);
         load_keys<RSM_THREADS>(a.S, m.s_off, ns, key);
         for (uint64_t s0 = 0; s0 < m.s_len;) {
-            sort_keys<RSM_THREADS>(key, ns, Sk, tmp, cnt, scan_scratch, red);
+            sort_keys<RSM_THREADS>(key, ns, Sk, tmp, bins_cnt, cnt, scan_scratch, red);
             const uint64_t s1 = s0 + ns;
             const uint32_t ns_next = (uint32_t)umin64(RSM_STILE, m.s_len - s1);
             if (ns_next) load_keys<RSM_THREADS>(a.S, m.s_off + s1, ns_next, key);  // in flight during the merge
