@@ -168,7 +168,12 @@ __device__ void build_table(Table &t, const Row *__restrict__ R, uint64_t r_off,
 }
 
 // Matches of S rows [0, len) (row pointer s, any 8-byte alignment) against
-// the table, this thread's share: 16-byte loads, four in flight.
+// the table, this thread's share: 16-byte loads, four in flight, and with
+// TBG_PROBE_AHEAD the next group of four issued before the current group is
+// probed (the loads of one group then overlap the probes of the previous).
+#ifndef TBG_PROBE_AHEAD
+#define TBG_PROBE_AHEAD 1
+#endif
 template <int THREADS, bool CG = false>
 __device__ __forceinline__ unsigned long long probe_count(const Table &t, const Row *s, uint64_t len) {
     unsigned long long local = 0;
@@ -181,6 +186,24 @@ __device__ __forceinline__ unsigned long long probe_count(const Table &t, const 
     if (head && tid == 0) local += t.count(ld_row<CG>(s, 0).x);
     if (tail && tid == THREADS - 1) local += t.count(ld_row<CG>(s, len - 1).x);
     uint64_t i = tid;
+    if (TBG_PROBE_AHEAD && i + 3 * THREADS < nv) {
+        uint4 n0 = ld_pair<CG>(v + i), n1 = ld_pair<CG>(v + i + THREADS);
+        uint4 n2 = ld_pair<CG>(v + i + 2 * THREADS), n3 = ld_pair<CG>(v + i + 3 * THREADS);
+        for (;;) {
+            const uint4 x0 = n0, x1 = n1, x2 = n2, x3 = n3;
+            i += 4 * THREADS;
+            const bool more = i + 3 * THREADS < nv;
+            if (more) {
+                n0 = ld_pair<CG>(v + i);
+                n1 = ld_pair<CG>(v + i + THREADS);
+                n2 = ld_pair<CG>(v + i + 2 * THREADS);
+                n3 = ld_pair<CG>(v + i + 3 * THREADS);
+            }
+            local += t.count(x0.x) + t.count(x0.z) + t.count(x1.x) + t.count(x1.z);
+            local += t.count(x2.x) + t.count(x2.z) + t.count(x3.x) + t.count(x3.z);
+            if (!more) break;
+        }
+    }
     for (; i + 3 * THREADS < nv; i += 4 * THREADS) {
         uint4 x0 = ld_pair<CG>(v + i), x1 = ld_pair<CG>(v + i + THREADS);
         uint4 x2 = ld_pair<CG>(v + i + 2 * THREADS), x3 = ld_pair<CG>(v + i + 3 * THREADS);
