@@ -677,7 +677,9 @@ def main():
             bypass = algo == "LRN" and not st.used_fallback
             part_rows = rows - heavy
             alg = 8 * rows + (16 * passes + 8) * part_rows
-            model = (f"histogram read 8 B/row of R and S; {passes} passes x 16 + build/probe 8 B/row of the "
+            # RSM's per-partition sort reads an S tile twice, the second time from L2
+            step = "sort + merge" if algo == "RSM" else "build/probe"
+            model = (f"histogram read 8 B/row of R and S; {passes} passes x 16 + {step} 8 B/row of the "
                      f"rows that are partitioned ({part_rows}" + (f", {heavy} heavy S rows joined in the "
                                                                    f"histogram read" if heavy else "") + ")")
             if bypass:  # the kept S rows written compacted, R read once more for its heavy rows
