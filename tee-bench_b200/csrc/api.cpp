@@ -205,7 +205,7 @@ RadixGeom radix_geometry(const tbg_config &cfg, uint64_t nR, uint64_t nS, int ca
     g.P = 1ull << g.B;
     g.F1 = 1ull << g.b1;
     g.capR = capR;
-    g.join_grid = w.nsm * join_ctas_per_sm(capR, !cfg.materialize && cfg.algo != TBG_RHT);
+    g.join_grid = w.nsm * join_ctas_per_sm(capR, cfg.materialize != 0, cfg.algo == TBG_RHT ? 1 : 0);
     g.capS = 0;
     if (cfg.skew_split) {
         g.capS = nS / ((uint64_t)g.join_grid * 4);
@@ -545,7 +545,7 @@ int radix_join_phase(const tbg_config &cfg, tbg_row_out *d_rows, uint64_t cap, W
         small.gate = &ctrl->max_part_R;
         small.gate_max = (unsigned long long)small_cap;
         small.gate_le = 1;
-        if ((e = launch_join(small, false, w.nsm * join_ctas_per_sm(small_cap, ja.layout == 0), st)) != cudaSuccess)
+        if ((e = launch_join(small, false, w.nsm * join_ctas_per_sm(small_cap, false, ja.layout), st)) != cudaSuccess)
             return cuda_error(e, "join");
         ja.gate = small.gate;
         ja.gate_max = (unsigned long long)small_cap;

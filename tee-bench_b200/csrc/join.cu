@@ -12,6 +12,7 @@
 // JOIN_THREADS * 8 probe rows) and places them in (row slot, lane) order, so
 // consecutive lanes store consecutive rows (the reference's insert_output,
 // Include/util.c:20-29, mallocs one node per row).
+#include <algorithm>
 #include <map>
 #include <mutex>
 
@@ -39,6 +40,10 @@ __global__ void __launch_bounds__(JOIN_THREADS) k_join(JoinArgs a) {
         t.hcap = count_head_slots(a.capR);
         t.head64 = reinterpret_cast<uint64_t *>(t.key + a.capR);
         t.next = reinterpret_cast<uint16_t *>(t.head64 + t.hcap);
+    }
+    if (!MAT && a.layout == 1) {  // count only: keys, then bucket starts and cursors (no payloads)
+        t.pay = nullptr;
+        t.heads = t.key + a.capR;
     }
     t.hs = a.hash_shift;
     t.layout = a.layout;
@@ -136,25 +141,31 @@ size_t join_smem_bytes(int capR) {
 }
 // Shared memory of a k_join launch: counting bucket-chain tables hold keys,
 // packed heads and links only.
+// Counting histogram tables (RHT) hold keys, the bucket starts and cursors.
 size_t join_launch_smem(int capR, bool materialize, int layout) {
     if (!materialize && layout == 0)
         return (size_t)capR * 4 + (size_t)count_head_slots(capR) * 8 + (size_t)capR * 2 + 16;
+    if (!materialize && layout == 1) {
+        uint32_t p = 1;
+        while (p < (uint32_t)capR) p <<= 1;
+        const size_t nb = std::max<uint32_t>(p >> 2, 4);  // buckets of the largest partition
+        return (size_t)capR * 4 + (2 * nb + 1) * 4 + 16;
+    }
     return join_smem_bytes(capR);
 }
 
-// Resident CTAs per SM at a table of capR rows (counting: the bucket-chain
-// table of a counting join), cached per (device, capR, counting): the
-// occupancy query runs once per size.
-int join_ctas_per_sm(int capR, bool counting) {
+// Resident CTAs per SM of a k_join launch at a table of capR rows, cached per
+// (device, capR, materialize, layout): the occupancy query runs once per size.
+int join_ctas_per_sm(int capR, bool materialize, int layout) {
     static std::mutex mu;
     static std::map<std::pair<int, int>, int> cache;
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> g(mu);
-    const int key = counting ? -capR : capR;
+    const int key = capR * 4 + (materialize ? 2 : 0) + (layout ? 1 : 0);
     auto it = cache.find(std::make_pair(dev, key));
     if (it != cache.end()) return it->second;
-    const size_t smem = join_launch_smem(capR, !counting, 0);
+    const size_t smem = join_launch_smem(capR, materialize, layout);
     int n = 0;
     if (smem_limit((const void *)k_join<false>, smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_join<false>, JOIN_THREADS, smem) != cudaSuccess) {

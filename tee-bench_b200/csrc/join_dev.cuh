@@ -161,7 +161,7 @@ __device__ void build_table(Table &t, const Row *__restrict__ R, uint64_t r_off,
             uint2 x = ld_row<CG>(R, r_off + i);
             uint32_t pos = atomicAdd(&cur[t.bucket(x.x)], 1u);
             t.key[pos] = x.x;
-            t.pay[pos] = x.y;
+            if (t.pay) t.pay[pos] = x.y;  // counting tables keep keys only
         }
         __syncthreads();
     }

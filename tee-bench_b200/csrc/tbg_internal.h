@@ -151,7 +151,7 @@ cudaError_t launch_part_pass2(const PartArgs &a, cudaStream_t st);
 cudaError_t launch_join(const JoinArgs &a, bool materialize, int grid, cudaStream_t st);
 size_t join_smem_bytes(int capR);
 size_t join_launch_smem(int capR, bool materialize, int layout);
-int join_ctas_per_sm(int capR, bool counting = false);
+int join_ctas_per_sm(int capR, bool materialize, int layout);
 
 cudaError_t launch_gen_pk(Row *d, uint64_t n, uint64_t seed, cudaStream_t st);
 cudaError_t launch_gen_fk(Row *d, uint64_t n, uint64_t maxid, uint64_t seed, cudaStream_t st);
