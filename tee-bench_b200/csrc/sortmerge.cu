@@ -1,21 +1,26 @@
 // Sort-merge joins for sm_100a.
 //
 // RSM (Joins/radix_sortmerge_join.c:74-100): the radix partitions of RHO,
-// then per partition pair both sides are sorted in shared memory over the
-// key bits that vary inside the tile (one counting pass, or a stable LSD
-// radix sort of packed (key, payload) words when they span more than 12
-// bits) and merged.  PSM
+// then per work item R's chunk is sorted in shared memory over the key bits
+// that vary in it (one counting pass, or a stable LSD radix sort when they
+// span more than 12 bits) and S is sorted in tiles and merged against it.
+// Count-only joins sort S in 16384-row tiles by a counting sort ranked
+// against R's key range (k_join_rsm_count); materialising joins sort packed
+// (key, payload) words in 4096-row tiles (k_join_rsm).  PSM
 // (Joins/psm/parallel_sortmerge_join.h:61-111): R and S are sorted globally
-// (LSD radix sort with the chunked stable passes of sortpass.cu) and merged.
+// (the MSD bucket sort or the LSD passes of sortpass.cu) and merged
+// (k_merge_count, k_merge_join).
 //
-// The merge is a merge path (Green, McColl, Bader 2012): the merged order
-// takes R[i] before S[j] iff R[i].key < S[j].key, so when S[j] is taken every
-// R row with a smaller key is behind and its matches are the run of equal
-// keys starting at the current R position.  Diagonals split the path evenly
-// over threads (and, for PSM, over CTAs).  The reference's merge()
+// The merges are merge paths (Green, McColl, Bader 2012); diagonals split the
+// path evenly over threads (and, for PSM, over CTAs).  The count-only merges
+// take R[i] before S[j] iff R[i].key <= S[j].key, so when S[j] is taken every
+// R row of its key is behind it and a running count of the last R key's rows
+// gives its matches.  The materialising merges take R[i] first iff
+// R[i].key < S[j].key, so S[j]'s matches are the run of equal R keys from the
+// current R position, which it emits.  The reference's merge()
 // (Joins/radix_sortmerge_join.c:40-71, parallel_sortmerge_join.h:18-51) has
 // unbounded inner loops and a stale S cursor that miscount duplicates and
-// misses; this merge counts exactly the equi-join.
+// misses; these merges count exactly the equi-join.
 #include <algorithm>
 
 #include "part_dev.cuh"
@@ -765,11 +770,12 @@ cudaError_t launch_key_range(const Row *in, uint64_t n, uint32_t *minmax, int ns
 // Merge join of sorted R (nr) and sorted S (ns).  k_merge_splits finds, for
 // every CTA boundary c * D, the merge-path split (one thread per boundary);
 // CTA c then loads R[i_c, i_c+1) and S[j_c, j_c+1) (D rows together) into
-// one shared array, each thread issuing all of its loads before its first
+// one shared array, each thread issuing a batch of loads before its first
 // shared store, splits its D diagonals evenly over threads and walks them.
-// A run of equal R keys that continues past the tile is finished in global
-// memory.
-// Merge tile shape (build options for A/B timing).
+// Materialising (k_merge_join<true>): a run of equal R keys that continues
+// past the tile is finished in global memory.  Count-only (k_merge_count): a
+// run of equal R keys that starts before the tile is found by walking back.
+// Merge tile shapes (build options for A/B timing).
 #ifndef TBG_MERGE_THREADS
 #define TBG_MERGE_THREADS 256
 #endif
