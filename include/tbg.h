@@ -175,7 +175,7 @@ typedef struct tbg_config {
     int model;              /* LRN: TBG_MODEL_*                                */
     int train_steps;        /* LRN: training steps (<= 500)                    */
     int heavy_bypass;       /* LRN: join flagged heavy keys during partitioning */
-    double sample_rate;     /* LRN: sampled fraction of R and S (0.01)         */
+    double sample_rate;     /* LRN: sampled fraction of S (0: 0.01)            */
     double imbalance_limit; /* LRN: predicted max/mean above which radix is used */
     uint64_t seed;          /* LRN sampling / init seed                        */
     int timing;             /* record per-phase device times into tbg_stats    */
