@@ -33,6 +33,12 @@ __device__ __forceinline__ uint64_t pack_head(uint32_t key, uint32_t row1, uint3
     return ((uint64_t)key << 32) | (row1 << 16) | next1;
 }
 
+// Histogram-table probes read the bucket's keys four at a time (a build
+// option for A/B timing).
+#ifndef TBG_RHT_VEC_PROBE
+#define TBG_RHT_VEC_PROBE 1
+#endif
+
 struct Table {
     uint32_t *key;    // [capR]
     uint32_t *pay;    // [capR] (unused with head64)
@@ -66,6 +72,17 @@ struct Table {
             for (uint32_t h = (uint32_t)x & 0xFFFF; h; h = next[h - 1]) c += (key[h - 1] == k);
         } else if (layout == 0) {
             for (uint32_t h = heads[b]; h; h = next[h - 1]) c += (key[h - 1] == k);
+        } else if (TBG_RHT_VEC_PROBE) {
+            // the bucket's keys read as 16-byte words (key[] starts 16-byte
+            // aligned): a word's slots before the bucket hold keys of other
+            // buckets, which differ from k; slots at or past its end are
+            // masked (past the table they may hold stale keys)
+            const uint32_t j = heads[b], e = heads[b + 1];
+            const uint4 *k4 = reinterpret_cast<const uint4 *>(key);
+            for (uint32_t a4 = j & ~3u; a4 < e; a4 += 4) {
+                const uint4 q = k4[a4 >> 2];
+                c += (q.x == k) + (q.y == k && a4 + 1 < e) + (q.z == k && a4 + 2 < e) + (q.w == k && a4 + 3 < e);
+            }
         } else {
             for (uint32_t j = heads[b], e = heads[b + 1]; j < e; j++) c += (key[j] == k);
         }
