@@ -310,6 +310,34 @@ def test_psm_heavy_key_takes_lsd(tbg, oracle, cuda, materialize):
 
 
 @pytest.mark.parametrize("materialize", [False, True])
+def test_psm_bucket_past_group_stage(tbg, oracle, cuda, materialize):
+    """MSD buckets averaging 4K rows are sorted four per CTA, each group with a
+    5K-row stage; a key repeated tens of thousands of times in R (and another
+    in S) makes one bucket of each relation outgrow its group's stage, so most
+    of its rows go straight to their sorted place.  Count and rows match the
+    oracle."""
+    rng = np.random.default_rng(43)
+    n = 1 << 22
+    R = np.zeros(n, dtype=oracle.ROW)
+    S = np.zeros(n, dtype=oracle.ROW)
+    R["key"] = rng.permutation(np.arange(1, n + 1, dtype=np.uint32))
+    S["key"] = rng.integers(1, n + 1, n).astype(np.uint32)
+    R["key"][:30000] = 777
+    S["key"][:40000] = 888
+    oracle.fill_payloads(R, 0)
+    oracle.fill_payloads(S, 1)
+    if materialize:
+        ref, ref_rows = oracle.rho(R, S, materialize=True)
+        m, rows, _ = run_join(tbg, cuda, "PSM", R, S, materialize=True, cap=ref)
+        assert m == ref
+        assert np.array_equal(oracle.sort_rows(rows), oracle.sort_rows(ref_rows))
+    else:
+        ref = oracle.rho(R, S)
+        m, _, _ = run_join(tbg, cuda, "PSM", R, S)
+        assert m == ref
+
+
+@pytest.mark.parametrize("materialize", [False, True])
 def test_psm_s_keys_outside_r_range(tbg, oracle, cuda, materialize):
     """PSM first bins both relations by R's key range; S keys below and above
     it send the sort back to both relations' range.  Count and rows match
